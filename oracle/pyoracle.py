@@ -1,0 +1,285 @@
+"""ctypes wrappers for the oracle libraries -- TEST INFRASTRUCTURE.
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this module.
+
+``Oracle``     drives oracle/liboracle.so (the C restatement, always built).
+``Reference``  drives oracle/_ref/libnadia_ref*.so (the reference's own sources
+               compiled against the FFTW shim), when that directory was built.
+Both expose the same methods, named after the reference API
+(NADIA/include/BaseCDI.h, PlanarCDI.h, FresnelCDI.h, PolyCDI.h).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+_D = ctypes.POINTER(ctypes.c_double)
+_V = ctypes.c_void_p
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_D)
+
+
+def _cplx_in(a, nx, ny):
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    assert a.shape == (nx, ny), a.shape
+    return a
+
+
+def _real_in(a, nx, ny):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    assert a.shape == (nx, ny), a.shape
+    return a
+
+
+_PROTOS = {
+    "planar_create": (_V, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "fresnel_create": (_V, [ctypes.c_int, ctypes.c_int, _D, ctypes.c_double, ctypes.c_double,
+                            ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
+    "poly_create": (_V, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+    "destroy": (None, [_V]),
+    "set_support": (None, [_V, _D, ctypes.c_int]),
+    "set_intensity": (None, [_V, _D]),
+    "set_beam_stop": (None, [_V, _D]),
+    "set_algorithm": (None, [_V, ctypes.c_int]),
+    "set_custom_algorithm": (None, [_V, _D]),
+    "set_relaxation_parameter": (None, [_V, ctypes.c_double]),
+    "initialise_estimate": (None, [_V, ctypes.c_int]),
+    "set_esw": (None, [_V, _D]),
+    "get_esw": (None, [_V, _D]),
+    "iterate": (None, [_V]),
+    "get_error": (ctypes.c_double, [_V]),
+    "apply_shrinkwrap": (None, [_V, ctypes.c_double, ctypes.c_double]),
+    "get_support": (None, [_V, _D]),
+    "get_transmission": (None, [_V, _D]),
+    "set_transmission": (None, [_V, _D]),
+    "get_illumination_at_sample": (None, [_V, _D]),
+    "fresnel_auto_set_norm": (None, [_V]),
+    "fresnel_set_norm": (None, [_V, ctypes.c_double]),
+    "poly_set_spectrum": (None, [_V, _D, ctypes.c_int]),
+    "get_best_result": (ctypes.c_int, [_V, ctypes.c_int, _D, _D]),
+    "reset_best": (None, [_V]),
+    "propagate_to_detector": (None, [_V, _D]),
+    "propagate_from_detector": (None, [_V, _D]),
+    "scale_intensity": (None, [_V, _D]),
+    "apply_support": (None, [_V, _D]),
+    "project_intensity": (None, [_V, _D]),
+    "get_intensity_autocorrelation": (None, [_V, _D]),
+}
+
+
+class _Lib:
+    def __init__(self, path, prefix):
+        self.lib = ctypes.CDLL(path)
+        self.prefix = prefix
+        for name, (res, args) in _PROTOS.items():
+            f = getattr(self.lib, prefix + name)
+            f.restype = res
+            f.argtypes = args
+            setattr(self, name, f)
+
+
+def oracle_lib_path():
+    return os.path.join(HERE, "liboracle.so")
+
+
+_ORACLE = None
+_REFS = {}
+
+
+def oracle_lib():
+    global _ORACLE
+    if _ORACLE is None:
+        path = oracle_lib_path()
+        if not os.path.exists(path):
+            import importlib.util
+            spec = importlib.util.spec_from_file_location(
+                "build_oracle", os.path.join(HERE, "build_oracle.py"))
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            mod.build_oracle()
+        _ORACLE = _Lib(path, "orc_")
+        _ORACLE.lib.orc_fft2d.argtypes = [_D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        _ORACLE.lib.orc_fft2d.restype = ctypes.c_int
+        _ORACLE.lib.orc_read_spec.argtypes = [ctypes.c_char_p, _D, ctypes.c_int]
+        _ORACLE.lib.orc_read_spec.restype = ctypes.c_int
+        _ORACLE.lib.orc_padding.argtypes = [_V, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]
+    return _ORACLE
+
+
+def reference_available(variant="64"):
+    return os.path.exists(os.path.join(REF_DIR, "libnadia_ref%s.so" % variant))
+
+
+def reference_lib(variant="64"):
+    """variant: '64' (parity build), '64_fast' or '32_fast' (timing builds)."""
+    if variant not in _REFS:
+        _REFS[variant] = _Lib(os.path.join(REF_DIR, "libnadia_ref%s.so" % variant), "ref_")
+    return _REFS[variant]
+
+
+def canon_fft2d(a, forward=True):
+    """The oracle's canonical unnormalised 2-D DFT of a complex array."""
+    a = np.array(a, dtype=np.complex128, order="C", copy=True)
+    rc = oracle_lib().lib.orc_fft2d(_ptr(a), a.shape[0], a.shape[1], 1 if forward else 0)
+    if rc != 0:
+        raise ValueError("unsupported FFT size %s" % (a.shape,))
+    return a
+
+
+def read_spec(path, capacity=4096):
+    out = np.zeros((capacity, 2), dtype=np.float64)
+    n = oracle_lib().lib.orc_read_spec(path.encode(), _ptr(out), capacity)
+    if n < 0:
+        raise IOError(path)
+    return out[:n].copy()
+
+
+class _Solver:
+    """One reconstruction (PlanarCDI / FresnelCDI / PolyCDI) on a CPU library."""
+
+    def __init__(self, lib, kind, nx, ny, n_best=0, white_field=None, wavelength=None,
+                 focal_detector_length=None, focal_sample_length=None, pixel_size=None,
+                 normalisation=1.0, beta=0.9):
+        self.L = lib
+        self.kind = kind
+        self.nx, self.ny = nx, ny
+        if kind == "planar":
+            self.h = lib.planar_create(nx, ny, n_best)
+        elif kind == "fresnel":
+            wf = _cplx_in(white_field, nx, ny)
+            self.h = lib.fresnel_create(nx, ny, _ptr(wf), wavelength, focal_detector_length,
+                                        focal_sample_length, pixel_size, normalisation, n_best)
+        elif kind == "poly":
+            self.h = lib.poly_create(nx, ny, beta, n_best)
+        else:
+            raise ValueError(kind)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.destroy(self.h)
+            self.h = None
+
+    def set_support(self, s, soften=False):
+        s = _real_in(s, self.nx, self.ny)
+        self.L.set_support(self.h, _ptr(s), int(bool(soften)))
+
+    def set_intensity(self, i):
+        i = _real_in(i, self.nx, self.ny)
+        self.L.set_intensity(self.h, _ptr(i))
+
+    def set_beam_stop(self, b):
+        b = _real_in(b, self.nx, self.ny)
+        self.L.set_beam_stop(self.h, _ptr(b))
+
+    def set_algorithm(self, alg):
+        self.L.set_algorithm(self.h, int(alg))
+
+    def set_custom_algorithm(self, m):
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        assert m.shape == (10,)
+        self.L.set_custom_algorithm(self.h, _ptr(m))
+
+    def set_relaxation_parameter(self, b):
+        self.L.set_relaxation_parameter(self.h, float(b))
+
+    def initialise_estimate(self, seed=0):
+        self.L.initialise_estimate(self.h, int(seed))
+
+    def set_exit_surface_wave(self, e):
+        e = _cplx_in(e, self.nx, self.ny)
+        self.L.set_esw(self.h, _ptr(e))
+
+    def get_exit_surface_wave(self):
+        out = np.empty((self.nx, self.ny), dtype=np.complex128)
+        self.L.get_esw(self.h, _ptr(out))
+        return out
+
+    def iterate(self, n=1):
+        for _ in range(n):
+            self.L.iterate(self.h)
+
+    def get_error(self):
+        return self.L.get_error(self.h)
+
+    def apply_shrinkwrap(self, gauss_width=1.5, threshold=0.1):
+        self.L.apply_shrinkwrap(self.h, gauss_width, threshold)
+
+    def get_support(self):
+        out = np.empty((self.nx, self.ny), dtype=np.float64)
+        self.L.get_support(self.h, _ptr(out))
+        return out
+
+    def get_transmission(self):
+        out = np.empty((self.nx, self.ny), dtype=np.complex128)
+        self.L.get_transmission(self.h, _ptr(out))
+        return out
+
+    def set_transmission(self, t):
+        t = _cplx_in(t, self.nx, self.ny)
+        self.L.set_transmission(self.h, _ptr(t))
+
+    def get_illumination_at_sample(self):
+        out = np.zeros((self.nx, self.ny), dtype=np.complex128)
+        self.L.get_illumination_at_sample(self.h, _ptr(out))
+        return out
+
+    def auto_set_norm(self):
+        self.L.fresnel_auto_set_norm(self.h)
+
+    def set_norm(self, n):
+        self.L.fresnel_set_norm(self.h, float(n))
+
+    def set_spectrum(self, spec):
+        spec = np.ascontiguousarray(spec, dtype=np.float64)
+        assert spec.ndim == 2 and spec.shape[1] == 2
+        self.L.poly_set_spectrum(self.h, _ptr(spec), spec.shape[0])
+
+    def get_best_result(self, index=0):
+        err = ctypes.c_double(0)
+        out = np.empty((self.nx, self.ny), dtype=np.complex128)
+        ok = self.L.get_best_result(self.h, index, ctypes.byref(err), _ptr(out))
+        return (err.value, out) if ok else (None, None)
+
+    def reset_best(self):
+        self.L.reset_best(self.h)
+
+    def _op(self, f, c):
+        c = np.array(c, dtype=np.complex128, order="C", copy=True)
+        assert c.shape == (self.nx, self.ny)
+        f(self.h, _ptr(c))
+        return c
+
+    def propagate_to_detector(self, c):
+        return self._op(self.L.propagate_to_detector, c)
+
+    def propagate_from_detector(self, c):
+        return self._op(self.L.propagate_from_detector, c)
+
+    def scale_intensity(self, c):
+        return self._op(self.L.scale_intensity, c)
+
+    def apply_support(self, c):
+        return self._op(self.L.apply_support, c)
+
+    def project_intensity(self, c):
+        return self._op(self.L.project_intensity, c)
+
+    def get_intensity_autocorrelation(self):
+        out = np.empty((self.nx, self.ny), dtype=np.float64)
+        self.L.get_intensity_autocorrelation(self.h, _ptr(out))
+        return out
+
+
+def Oracle(kind, nx, ny, **kw):
+    return _Solver(oracle_lib(), kind, nx, ny, **kw)
+
+
+def Reference(kind, nx, ny, variant="64", **kw):
+    return _Solver(reference_lib(variant), kind, nx, ny, **kw)
