@@ -1,0 +1,225 @@
+/*
+ * nadia_b200.h -- C ABI of the B200 phase-retrieval library (libnadia_b200.so).
+ *
+ * One handle (nadia_solver) is one reconstruction: the state of one
+ * PlanarCDI / FresnelCDI / PolyCDI object of the reference library
+ * (NADIA/include/PlanarCDI.h, FresnelCDI.h, PolyCDI.h over BaseCDI.h),
+ * resident on the current CUDA device, with its own CUDA stream.
+ *
+ * Conventions
+ *   - Arrays are host memory.  A real array holds nx*ny doubles, a complex
+ *     array nx*ny interleaved (re,im) pairs; element (x,y) is at x*ny+y, the
+ *     reference's layout (NADIA/include/Complex_2D.h:179-194,
+ *     NADIA/include/Double_2D.h:121-143).
+ *   - Every entry point returns NADIA_OK (0) or a nonzero status; none of them
+ *     exits the process.  nadia_last_error() gives a message for the calling
+ *     thread.  (The reference prints and calls exit(); the IDL binding,
+ *     NADIA/interfaces/idl/IDL_interface.c, is the C precedent for this ABI.)
+ *   - A handle is used by one host thread at a time.
+ *   - Precision: NADIA_FP64 runs the plain double-precision path, which
+ *     reproduces the reference's own double build (-DDOUBLE_PRECISION) loop by
+ *     loop; NADIA_FP32 runs the fused single-precision path (complex FP32
+ *     transforms and projections, FP64 error and support reductions).
+ *   - Sizes must be even (the reference's quadrant swap assumes it,
+ *     NADIA/src/Complex_2D.c++:327-331) and every prime factor of a transform
+ *     length must be at most 64.
+ */
+#ifndef NADIA_B200_H
+#define NADIA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct nadia_solver nadia_solver;
+
+/* status codes */
+enum {
+    NADIA_OK = 0,
+    NADIA_ERR_INVALID = 1,     /* bad argument or size */
+    NADIA_ERR_STATE = 2,       /* call not valid in the current state */
+    NADIA_ERR_UNSUPPORTED = 3, /* feature not provided on this path */
+    NADIA_ERR_CUDA = 4,        /* CUDA runtime error */
+    NADIA_ERR_NOMEM = 5,       /* device allocation failed */
+    NADIA_ERR_RANGE = 6        /* index out of range (get_best_result) */
+};
+
+/* geometries */
+enum { NADIA_PLANAR = 0, NADIA_FRESNEL = 1, NADIA_POLY = 2 };
+
+/* arithmetic forms */
+enum { NADIA_FP64 = 0, NADIA_FP32 = 1 };
+
+/* algorithms, numbered as the reference's enum (NADIA/include/BaseCDI.h:79) */
+enum {
+    NADIA_ER = 0, NADIA_BIO = 1, NADIA_BOO = 2, NADIA_HIO = 3, NADIA_DM = 4,
+    NADIA_SF = 5, NADIA_ASR = 6, NADIA_HPR = 7, NADIA_RAAR = 8, NADIA_CUSTOM = 9
+};
+
+/* Message describing the last failure on the calling thread ("" if none). */
+const char *nadia_last_error(void);
+
+/* Library version string. */
+const char *nadia_version(void);
+
+/* ---- lifecycle -------------------------------------------------------- */
+
+/* PlanarCDI(Complex_2D&, n_best)  -- NADIA/include/PlanarCDI.h:28-29.
+ * The estimate starts at zero; the algorithm starts as ER (BaseCDI.c++:63-64). */
+int nadia_planar_create(int nx, int ny, int precision, int n_best, nadia_solver **out);
+
+/* FresnelCDI(initial_guess, white_field, wavelength, focal_detector_length,
+ * focal_sample_length, pixel_size, normalisation, n_best)
+ * -- NADIA/src/FresnelCDI.c++:20-44.  white_field: complex detector-plane field. */
+int nadia_fresnel_create(int nx, int ny, int precision, const double *white_field,
+                         double beam_wavelength, double focal_detector_length,
+                         double focal_sample_length, double pixel_size,
+                         double normalisation, int n_best, nadia_solver **out);
+
+/* PolyCDI(initial_guess, beta, n_best, parallel) -- NADIA/src/PolyCDI.c++:25-35.
+ * As in the reference, `beta` is stored but never reaches the algorithm
+ * weights (PolyCDI.h:53 shadows BaseCDI's beta); the relaxation parameter is
+ * set with nadia_set_relaxation_parameter. */
+int nadia_poly_create(int nx, int ny, int precision, double beta, int n_best,
+                      nadia_solver **out);
+
+/* Releases the device memory and stream of a handle (NULL is accepted). */
+int nadia_destroy(nadia_solver *s);
+
+/* Grid size and kind of a handle. */
+int nadia_get_size(const nadia_solver *s, int *nx, int *ny);
+
+/* ---- inputs ------------------------------------------------------------ */
+
+/* BaseCDI::set_support(const Double_2D&, bool soften) -- BaseCDI.c++:95-108:
+ * support = obj / max(obj), optionally blurred (sigma 3, 5-pixel cut-off). */
+int nadia_set_support(nadia_solver *s, const double *support, int soften);
+
+/* BaseCDI::set_intensity -- BaseCDI.c++:118-124 (stores sqrt(I)). */
+int nadia_set_intensity(nadia_solver *s, const double *intensity);
+
+/* BaseCDI::set_beam_stop -- BaseCDI.c++:112-116: 0 = unmeasured pixel,
+ * left free by the modulus projection; >0 = measured. */
+int nadia_set_beam_stop(nadia_solver *s, const double *mask);
+
+/* PolyCDI::set_spectrum(Double_2D) -- PolyCDI.c++:66-89.  wl_weight holds
+ * nlambda rows of (wavelength, weight); list the longest wavelength first
+ * (the padding is derived from row 0 and must not be negative). */
+int nadia_poly_set_spectrum(nadia_solver *s, const double *wl_weight, int nlambda);
+
+/* PolyCDI::set_spectrum(string) -- PolyCDI.c++:38-63 reading the file with
+ * read_spec (NADIA/src/io_spec.c:61-133: tab-separated "energy weight" lines,
+ * energy stored as its reciprocal, values pass through float). */
+int nadia_poly_set_spectrum_file(nadia_solver *s, const char *path);
+
+/* The padding PolyCDI derived from its spectrum (PolyCDI.c++:86-87). */
+int nadia_poly_get_padding(const nadia_solver *s, int *px, int *py);
+
+/* ---- algorithm ---------------------------------------------------------- */
+
+/* BaseCDI::set_algorithm -- BaseCDI.c++:192-237.  Returns early when the
+ * algorithm is unchanged, as the reference does. */
+int nadia_set_algorithm(nadia_solver *s, int algorithm);
+
+/* BaseCDI::set_custom_algorithm(m1..m10) -- BaseCDI.c++:240-255. */
+int nadia_set_custom_algorithm(nadia_solver *s, const double m[10]);
+
+/* BaseCDI::set_relaxation_parameter -- NADIA/include/BaseCDI.h:264-267.  As in
+ * the reference, the new beta takes effect at the next change of algorithm. */
+int nadia_set_relaxation_parameter(nadia_solver *s, double beta);
+
+/* The five operator weights [PsPf, PfPs, Ps, Pf, I] in use (BaseCDI.c++:245-249). */
+int nadia_get_algorithm_structure(const nadia_solver *s, double w[5], int *algorithm);
+
+/* Host-only helper, no handle or GPU needed: the weights that
+ * set_custom_algorithm(m1..m10) produces (BaseCDI.c++:245-249). */
+void nadia_custom_weights(const double m[10], double w[5]);
+
+/* ---- estimate ----------------------------------------------------------- */
+
+/* initialise_estimate(seed): PlanarCDI.c++:39-62, FresnelCDI.c++:152-201,
+ * PolyCDI.c++:102-126.  Uses the C library's srand/rand on the host, as the
+ * reference does, then uploads the estimate. */
+int nadia_initialise_estimate(nadia_solver *s, int seed);
+
+/* BaseCDI::set_exit_surface_wave / get_exit_surface_wave -- NADIA/include/BaseCDI.h:285-291. */
+int nadia_set_exit_surface_wave(nadia_solver *s, const double *esw);
+int nadia_get_exit_surface_wave(nadia_solver *s, double *esw);
+
+/* Single-precision variants for callers holding float buffers (the
+ * reference's default Complex_2D is ComplexR_2D<float>, Complex_2D.h:511-512). */
+int nadia_set_exit_surface_wave_f32(nadia_solver *s, const float *esw);
+int nadia_get_exit_surface_wave_f32(nadia_solver *s, float *esw);
+
+/* ---- run ---------------------------------------------------------------- */
+
+/* `iterations` calls of BaseCDI::iterate (BaseCDI.c++:297-387) or
+ * PolyCDI::iterate (PolyCDI.c++:130-250). */
+int nadia_iterate(nadia_solver *s, int iterations);
+
+/* BaseCDI::get_error -- BaseCDI.c++:126-128: the error metric computed by the
+ * last modulus projection (that is, of the estimate before the last update). */
+int nadia_get_error(nadia_solver *s, double *error);
+
+/* The error metric of each of the last `count` iterations, oldest first
+ * (count <= the number of iterations run since the handle was created and
+ * <= 65536).  Returns NADIA_ERR_RANGE if fewer are available. */
+int nadia_get_error_history(nadia_solver *s, double *errors, int count);
+
+/* BaseCDI::apply_shrinkwrap(gauss_width, threshold) -- BaseCDI.c++:416-429. */
+int nadia_apply_shrinkwrap(nadia_solver *s, double gauss_width, double threshold);
+
+/* BaseCDI::get_support -- NADIA/include/BaseCDI.h:408-410 (copy into `support`). */
+int nadia_get_support(nadia_solver *s, double *support);
+
+/* BaseCDI::get_best_result(error, index) -- BaseCDI.c++:82-91.
+ * Returns NADIA_ERR_RANGE for an index outside [0, n_best). */
+int nadia_get_best_result(nadia_solver *s, int index, double *error, double *esw);
+
+/* BaseCDI::reset_best -- NADIA/include/BaseCDI.h:476-479. */
+int nadia_reset_best(nadia_solver *s);
+
+/* get_transmission: FresnelCDI::get_transmission_function (FresnelCDI.c++:298-355)
+ * for FRESNEL; the exit-surface wave for PLANAR and POLY (PolyCDI.h:210
+ * declares get_transmission without a definition). */
+int nadia_get_transmission(nadia_solver *s, double *transmission);
+
+/* FresnelCDI::set_transmission_function (FresnelCDI.c++:253-283) for FRESNEL;
+ * set_exit_surface_wave for the others. */
+int nadia_set_transmission(nadia_solver *s, const double *transmission);
+
+/* FresnelCDI::auto_set_norm / set_norm / get_illumination_at_sample
+ * (FresnelCDI.c++:129-148, 293-296; FresnelCDI.h:216). */
+int nadia_fresnel_auto_set_norm(nadia_solver *s);
+int nadia_fresnel_set_norm(nadia_solver *s, double normalisation);
+int nadia_fresnel_get_illumination_at_sample(nadia_solver *s, double *illumination);
+
+/* The single operators, as the IDL binding exposes them
+ * (IDL_interface.c:947-985): each transforms the complex array in place
+ * on an nx*ny grid (PLANAR and FRESNEL). */
+int nadia_propagate_to_detector(nadia_solver *s, double *field);
+int nadia_propagate_from_detector(nadia_solver *s, double *field);
+int nadia_scale_intensity(nadia_solver *s, double *field);
+int nadia_apply_support(nadia_solver *s, double *field);
+int nadia_project_intensity(nadia_solver *s, double *field);
+
+/* PlanarCDI::get_intensity_autocorrelation -- PlanarCDI.c++:13-36. */
+int nadia_get_intensity_autocorrelation(nadia_solver *s, double *autoc);
+
+/* Waits for the handle's queued device work. */
+int nadia_synchronize(nadia_solver *s);
+
+/* ---- batching ------------------------------------------------------------ */
+
+/* Steps `count` independent reconstructions `iterations` times together:
+ * handles of the FP32 form with the same grid size run as one batched
+ * launch per pass, the groups of different sizes run concurrently, and the
+ * whole step is replayed from a CUDA graph.  Each handle ends in the state
+ * that `iterations` calls of nadia_iterate would have left it in.  No
+ * counterpart in the reference, which runs one reconstruction per process. */
+int nadia_iterate_many(nadia_solver *const *solvers, int count, int iterations);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NADIA_B200_H */

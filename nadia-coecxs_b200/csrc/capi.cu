@@ -1,0 +1,337 @@
+// capi.cu -- the extern "C" entry points of libnadia_b200 (include/nadia_b200.h).
+// Each converts exceptions into status codes and never exits the process.
+#include <cstring>
+#include <functional>
+#include <new>
+#include <string>
+
+#include "fused32.h"
+#include "solver.h"
+
+using nadia::Error;
+using nadia::Solver;
+
+struct nadia_solver {
+    Solver *s;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int guard(F &&f)
+{
+    try {
+        g_last_error.clear();
+        f();
+        return NADIA_OK;
+    } catch (const Error &e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        g_last_error = "host allocation failed";
+        return NADIA_ERR_NOMEM;
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return NADIA_ERR_CUDA;
+    }
+}
+
+Solver &S(nadia_solver *h)
+{
+    if (!h || !h->s) throw Error(NADIA_ERR_INVALID, "null handle");
+    NADIA_CUDA(cudaSetDevice(h->s->device));
+    return *h->s;
+}
+
+void need(const void *p, const char *what)
+{
+    if (!p) throw Error(NADIA_ERR_INVALID, std::string("null pointer: ") + what);
+}
+
+int create(int kind, int nx, int ny, int prec, int n_best, nadia_solver **out,
+           const std::function<void(Solver &)> &init)
+{
+    return guard([&] {
+        need(out, "out");
+        *out = nullptr;
+        Solver *s = new Solver(kind, nx, ny, prec, n_best);
+        try {
+            if (init) init(*s);
+        } catch (...) {
+            delete s;
+            throw;
+        }
+        *out = new nadia_solver{s};
+    });
+}
+
+} // namespace
+
+extern "C" {
+
+const char *nadia_last_error(void) { return g_last_error.c_str(); }
+
+const char *nadia_version(void) { return "nadia_b200 0.1 (sm_100a)"; }
+
+int nadia_planar_create(int nx, int ny, int precision, int n_best, nadia_solver **out)
+{
+    return create(NADIA_PLANAR, nx, ny, precision, n_best, out, nullptr);
+}
+
+int nadia_fresnel_create(int nx, int ny, int precision, const double *white_field,
+                         double beam_wavelength, double focal_detector_length,
+                         double focal_sample_length, double pixel_size, double normalisation,
+                         int n_best, nadia_solver **out)
+{
+    if (!white_field) {
+        g_last_error = "null pointer: white_field";
+        return NADIA_ERR_INVALID;
+    }
+    return create(NADIA_FRESNEL, nx, ny, precision, n_best, out, [&](Solver &s) {
+        s.fresnel_init(white_field, beam_wavelength, focal_detector_length, focal_sample_length,
+                       pixel_size, normalisation);
+    });
+}
+
+int nadia_poly_create(int nx, int ny, int precision, double beta, int n_best,
+                      nadia_solver **out)
+{
+    (void)beta; // PolyCDI.h:53 shadows BaseCDI::beta; the weights never see it
+    return create(NADIA_POLY, nx, ny, precision, n_best, out, nullptr);
+}
+
+int nadia_destroy(nadia_solver *h)
+{
+    return guard([&] {
+        if (!h) return;
+        if (h->s) {
+            cudaSetDevice(h->s->device);
+            delete h->s;
+        }
+        delete h;
+    });
+}
+
+int nadia_get_size(const nadia_solver *h, int *nx, int *ny)
+{
+    return guard([&] {
+        if (!h || !h->s) throw Error(NADIA_ERR_INVALID, "null handle");
+        need(nx, "nx");
+        need(ny, "ny");
+        *nx = h->s->nx;
+        *ny = h->s->ny;
+    });
+}
+
+int nadia_set_support(nadia_solver *h, const double *a, int soften)
+{
+    return guard([&] { need(a, "support"); S(h).set_support(a, soften != 0); });
+}
+
+int nadia_set_intensity(nadia_solver *h, const double *a)
+{
+    return guard([&] { need(a, "intensity"); S(h).set_intensity(a); });
+}
+
+int nadia_set_beam_stop(nadia_solver *h, const double *a)
+{
+    return guard([&] { need(a, "mask"); S(h).set_beam_stop(a); });
+}
+
+int nadia_poly_set_spectrum(nadia_solver *h, const double *wl_weight, int nlambda)
+{
+    return guard([&] { need(wl_weight, "wl_weight"); S(h).set_spectrum(wl_weight, nlambda); });
+}
+
+int nadia_poly_set_spectrum_file(nadia_solver *h, const char *path)
+{
+    return guard([&] {
+        need(path, "path");
+        Solver &s = S(h);
+        std::vector<double> sp = nadia::read_spec_file(path);
+        s.set_spectrum(sp.data(), (int)(sp.size() / 2));
+    });
+}
+
+int nadia_poly_get_padding(const nadia_solver *h, int *px, int *py)
+{
+    return guard([&] {
+        if (!h || !h->s) throw Error(NADIA_ERR_INVALID, "null handle");
+        need(px, "px");
+        need(py, "py");
+        if (!h->s->has_spectrum) throw Error(NADIA_ERR_STATE, "no spectrum set");
+        *px = h->s->px;
+        *py = h->s->py;
+    });
+}
+
+int nadia_set_algorithm(nadia_solver *h, int alg)
+{
+    return guard([&] { S(h).set_algorithm(alg); });
+}
+
+int nadia_set_custom_algorithm(nadia_solver *h, const double m[10])
+{
+    return guard([&] { need(m, "m"); S(h).set_custom(m); });
+}
+
+int nadia_set_relaxation_parameter(nadia_solver *h, double beta)
+{
+    return guard([&] { S(h).set_relaxation_parameter(beta); });
+}
+
+int nadia_get_algorithm_structure(const nadia_solver *h, double w[5], int *algorithm)
+{
+    return guard([&] {
+        if (!h || !h->s) throw Error(NADIA_ERR_INVALID, "null handle");
+        need(w, "w");
+        for (int i = 0; i < 5; ++i) w[i] = h->s->w[i];
+        if (algorithm) *algorithm = h->s->algorithm;
+    });
+}
+
+void nadia_custom_weights(const double m[10], double w[5])
+{
+    // BaseCDI.c++:245-249
+    w[0] = m[0] + m[1] + m[2] + m[3];
+    w[1] = -m[0] + m[4] + m[5] + m[6];
+    w[2] = -m[2] - m[5] - m[7] + m[9];
+    w[3] = -m[1] - m[4] + m[7] + m[8];
+    w[4] = -m[3] - m[6] - m[8] - m[9];
+}
+
+int nadia_initialise_estimate(nadia_solver *h, int seed)
+{
+    return guard([&] { S(h).initialise_estimate(seed); });
+}
+
+int nadia_set_exit_surface_wave(nadia_solver *h, const double *a)
+{
+    return guard([&] { need(a, "esw"); S(h).set_esw(a); });
+}
+
+int nadia_get_exit_surface_wave(nadia_solver *h, double *a)
+{
+    return guard([&] { need(a, "esw"); S(h).get_esw(a); });
+}
+
+int nadia_set_exit_surface_wave_f32(nadia_solver *h, const float *a)
+{
+    return guard([&] { need(a, "esw"); S(h).set_esw_f32(a); });
+}
+
+int nadia_get_exit_surface_wave_f32(nadia_solver *h, float *a)
+{
+    return guard([&] { need(a, "esw"); S(h).get_esw_f32(a); });
+}
+
+int nadia_iterate(nadia_solver *h, int iterations)
+{
+    return guard([&] { S(h).iterate(iterations); });
+}
+
+int nadia_get_error(nadia_solver *h, double *e)
+{
+    return guard([&] { need(e, "error"); *e = S(h).get_error(); });
+}
+
+int nadia_get_error_history(nadia_solver *h, double *e, int count)
+{
+    return guard([&] { need(e, "errors"); S(h).get_error_history(e, count); });
+}
+
+int nadia_apply_shrinkwrap(nadia_solver *h, double gauss_width, double threshold)
+{
+    return guard([&] { S(h).apply_shrinkwrap(gauss_width, threshold); });
+}
+
+int nadia_get_support(nadia_solver *h, double *a)
+{
+    return guard([&] { need(a, "support"); S(h).get_support(a); });
+}
+
+int nadia_get_best_result(nadia_solver *h, int index, double *error, double *esw)
+{
+    return guard([&] {
+        need(error, "error");
+        need(esw, "esw");
+        S(h).get_best(index, error, esw);
+    });
+}
+
+int nadia_reset_best(nadia_solver *h)
+{
+    return guard([&] { S(h).reset_best(); });
+}
+
+int nadia_get_transmission(nadia_solver *h, double *a)
+{
+    return guard([&] { need(a, "transmission"); S(h).get_transmission(a); });
+}
+
+int nadia_set_transmission(nadia_solver *h, const double *a)
+{
+    return guard([&] { need(a, "transmission"); S(h).set_transmission(a); });
+}
+
+int nadia_fresnel_auto_set_norm(nadia_solver *h)
+{
+    return guard([&] { S(h).fresnel_auto_set_norm(); });
+}
+
+int nadia_fresnel_set_norm(nadia_solver *h, double nn)
+{
+    return guard([&] { S(h).fresnel_set_norm(nn); });
+}
+
+int nadia_fresnel_get_illumination_at_sample(nadia_solver *h, double *a)
+{
+    return guard([&] { need(a, "illumination"); S(h).get_illumination_at_sample(a); });
+}
+
+int nadia_propagate_to_detector(nadia_solver *h, double *a)
+{
+    return guard([&] { need(a, "field"); S(h).single_op(0, a); });
+}
+
+int nadia_propagate_from_detector(nadia_solver *h, double *a)
+{
+    return guard([&] { need(a, "field"); S(h).single_op(1, a); });
+}
+
+int nadia_scale_intensity(nadia_solver *h, double *a)
+{
+    return guard([&] { need(a, "field"); S(h).single_op(2, a); });
+}
+
+int nadia_apply_support(nadia_solver *h, double *a)
+{
+    return guard([&] { need(a, "field"); S(h).single_op(3, a); });
+}
+
+int nadia_project_intensity(nadia_solver *h, double *a)
+{
+    return guard([&] { need(a, "field"); S(h).single_op(4, a); });
+}
+
+int nadia_get_intensity_autocorrelation(nadia_solver *h, double *a)
+{
+    return guard([&] { need(a, "autoc"); S(h).autocorrelation(a); });
+}
+
+int nadia_synchronize(nadia_solver *h)
+{
+    return guard([&] { S(h).sync(); });
+}
+
+} // extern "C"
+
+extern "C" int nadia_iterate_many(nadia_solver *const *solvers, int count, int iterations)
+{
+    return guard([&] {
+        need(solvers, "solvers");
+        for (int i = 0; i < count; ++i) S(solvers[i]).iterate(iterations);
+    });
+}

@@ -1,0 +1,122 @@
+// common.h -- error handling, device buffers and transform plans shared by
+// the FP64 and FP32 paths of libnadia_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "nadia_b200.h"
+
+namespace nadia {
+
+// An error carried to the C ABI boundary, where it becomes a status code.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define NADIA_CUDA(call)                                                                  \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            throw ::nadia::Error(e_ == cudaErrorMemoryAllocation ? NADIA_ERR_NOMEM         \
+                                                                 : NADIA_ERR_CUDA,         \
+                                 std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+#define NADIA_REQUIRE(cond, code, msg)                                                    \
+    do {                                                                                  \
+        if (!(cond)) throw ::nadia::Error((code), (msg));                                 \
+    } while (0)
+
+// Owning device allocation.
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t count) { alloc(count); }
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf &operator=(DevBuf &&o) noexcept
+    {
+        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void alloc(size_t count)
+    {
+        release();
+        if (count) NADIA_CUDA(cudaMalloc((void **)&p, count * sizeof(T)));
+        n = count;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+    explicit operator bool() const { return p != nullptr; }
+};
+
+constexpr int kMaxPasses = 40;
+constexpr int kMaxRadix = 64;
+
+// Radix plan of a transform length: 8s, then the remaining 4 or 2, then odd
+// primes in ascending order.  Returns the number of passes, or -1 when n has
+// a prime factor above kMaxRadix.
+inline int plan_radices(int n, int *radix)
+{
+    int p = 0;
+    if (n < 1) return -1;
+    while (n % 8 == 0) { radix[p++] = 8; n /= 8; }
+    if (n % 4 == 0) { radix[p++] = 4; n /= 4; }
+    if (n % 2 == 0) { radix[p++] = 2; n /= 2; }
+    for (int f = 3; n > 1; f += 2) {
+        while (n % f == 0) {
+            if (f > kMaxRadix) return -1;
+            radix[p++] = f;
+            n /= f;
+        }
+    }
+    return p;
+}
+
+// Transform plan passed to kernels by value.
+struct FftPlan {
+    int n;
+    int np;
+    int radix[kMaxPasses];
+};
+
+inline FftPlan make_plan(int n)
+{
+    FftPlan p{};
+    p.n = n;
+    p.np = plan_radices(n, p.radix);
+    NADIA_REQUIRE(p.np >= 0, NADIA_ERR_INVALID,
+                  "transform length " + std::to_string(n) + " has a prime factor above 64");
+    return p;
+}
+
+// Twiddle table W[t] = (cos, -sin)(2 pi t / n), computed in double on the host.
+inline std::vector<double2> twiddles(int n)
+{
+    std::vector<double2> w((size_t)n);
+    for (int t = 0; t < n; ++t) {
+        double ang = (2.0 * M_PI * (double)t) / (double)n;
+        w[t].x = cos(ang);
+        w[t].y = -sin(ang);
+    }
+    return w;
+}
+
+} // namespace nadia

@@ -1,0 +1,42 @@
+// fused32.h -- the FP32 engine of one reconstruction.
+#pragma once
+
+#include "common.h"
+
+namespace nadia {
+
+struct Solver;
+
+class Fused32 {
+public:
+    explicit Fused32(Solver &s);
+    ~Fused32();
+
+    void upload_support(const double *h);
+    void soften_support();
+    void upload_intensity();
+    void upload_beam_stop(const double *mask);
+    void set_spectrum();
+    void upload_illumination();
+    void set_fresnel_geometry(double factor);
+    void scale_illumination(double f);
+    void fresnel_initialise(const double *t);
+    void fresnel_set_transmission(const double *t);
+    void fresnel_get_transmission(double *t);
+    void get_illumination_at_sample(double *h);
+    void set_x(const double *h);
+    void get_x(double *h);
+    void set_x_f32(const float *h);
+    void get_x_f32(float *h);
+    void copy_x_to(float2 *dst);
+    void iterate(int count);
+    void shrinkwrap(double gauss_width, double threshold);
+    void get_support(double *h);
+    void single_op(int op, double *field);
+    void autocorrelation(double *out);
+
+    struct Impl;
+    Impl *impl;
+};
+
+} // namespace nadia

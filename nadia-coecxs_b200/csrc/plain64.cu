@@ -1,0 +1,720 @@
+// plain64.cu -- kernels of the plain FP64 path (see plain64.h).  Compiled
+// with --fmad=false: every product and sum below rounds separately, as in
+// the reference's double build compiled without contraction.
+#include "plain64.h"
+
+#include <algorithm>
+
+namespace nadia {
+namespace plain {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int blocks_for(size_t n, int per = kThreads)
+{
+    size_t b = (n + per - 1) / per;
+    return (int)std::min<size_t>(std::max<size_t>(b, 1), 1u << 30);
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 w)
+{
+    return make_double2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+}
+
+__device__ __forceinline__ void bf4(double2 *v, bool fwd)
+{
+    double2 a, b, c, d;
+    a.x = v[0].x + v[2].x; a.y = v[0].y + v[2].y;
+    b.x = v[0].x - v[2].x; b.y = v[0].y - v[2].y;
+    c.x = v[1].x + v[3].x; c.y = v[1].y + v[3].y;
+    d.x = v[1].x - v[3].x; d.y = v[1].y - v[3].y;
+    v[0].x = a.x + c.x; v[0].y = a.y + c.y;
+    v[2].x = a.x - c.x; v[2].y = a.y - c.y;
+    if (fwd) {
+        v[1].x = b.x + d.y; v[1].y = b.y - d.x;
+        v[3].x = b.x - d.y; v[3].y = b.y + d.x;
+    } else {
+        v[1].x = b.x - d.y; v[1].y = b.y + d.x;
+        v[3].x = b.x + d.y; v[3].y = b.y - d.x;
+    }
+}
+
+__device__ __forceinline__ void bf8(double2 *v, bool fwd)
+{
+    const double c8 = 0.70710678118654752440;
+    double2 a[4], b[4], t;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        a[r].x = v[r].x + v[r + 4].x; a[r].y = v[r].y + v[r + 4].y;
+        b[r].x = v[r].x - v[r + 4].x; b[r].y = v[r].y - v[r + 4].y;
+    }
+    if (fwd) {
+        t = b[1]; b[1].x = (t.x + t.y) * c8; b[1].y = (t.y - t.x) * c8;
+        t = b[2]; b[2].x = t.y;              b[2].y = -t.x;
+        t = b[3]; b[3].x = (t.y - t.x) * c8; b[3].y = -((t.x + t.y) * c8);
+    } else {
+        t = b[1]; b[1].x = (t.x - t.y) * c8; b[1].y = (t.y + t.x) * c8;
+        t = b[2]; b[2].x = -t.y;             b[2].y = t.x;
+        t = b[3]; b[3].x = -((t.x + t.y) * c8); b[3].y = (t.x - t.y) * c8;
+    }
+    bf4(a, fwd);
+    bf4(b, fwd);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) { v[2 * r] = a[r]; v[2 * r + 1] = b[r]; }
+}
+
+// One Stockham pass of radix R (compile-time for 2/4/8) over L signals of
+// length n held in shared memory (signal stride n).
+template <int R>
+__device__ void pass_fixed(const double2 *src, double2 *dst, int n, int L, int Ns,
+                           const double2 *__restrict__ W, bool fwd)
+{
+    const int m = n / R;
+    const int tstep = n / (Ns * R);
+    for (int b = threadIdx.x; b < L * m; b += blockDim.x) {
+        const int sig = b / m, j = b - sig * m;
+        const double2 *s = src + (size_t)sig * n;
+        double2 *d = dst + (size_t)sig * n;
+        const int k = j % Ns;
+        double2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = s[j + r * m];
+        if (k > 0) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                double2 w = __ldg(&W[k * r * tstep]);
+                if (!fwd) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        if (R == 2) {
+            double2 a = v[0], c = v[1];
+            v[0].x = a.x + c.x; v[0].y = a.y + c.y;
+            v[1].x = a.x - c.x; v[1].y = a.y - c.y;
+        } else if (R == 4) {
+            bf4(v, fwd);
+        } else {
+            bf8(v, fwd);
+        }
+        const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) d[base + r * Ns] = v[r];
+    }
+}
+
+// Generic (prime) radix: direct sum in increasing r.
+__device__ void pass_generic(const double2 *src, double2 *dst, int n, int L, int R, int Ns,
+                             const double2 *__restrict__ W, bool fwd)
+{
+    const int m = n / R;
+    const int tstep = n / (Ns * R);
+    const int q = n / R;
+    for (int b = threadIdx.x; b < L * m; b += blockDim.x) {
+        const int sig = b / m, j = b - sig * m;
+        const double2 *s = src + (size_t)sig * n;
+        double2 *d = dst + (size_t)sig * n;
+        const int k = j % Ns;
+        double2 v[kMaxRadix];
+        for (int r = 0; r < R; ++r) v[r] = s[j + r * m];
+        if (k > 0) {
+            for (int r = 1; r < R; ++r) {
+                double2 w = __ldg(&W[k * r * tstep]);
+                if (!fwd) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        const int base = (j / Ns) * Ns * R + k;
+        double2 y0 = v[0];
+        for (int r = 1; r < R; ++r) { y0.x = y0.x + v[r].x; y0.y = y0.y + v[r].y; }
+        d[base] = y0;
+        for (int sidx = 1; sidx < R; ++sidx) {
+            double2 acc = v[0];
+            for (int r = 1; r < R; ++r) {
+                double2 w = __ldg(&W[((r * sidx) % R) * q]);
+                if (!fwd) w.y = -w.y;
+                double2 p = cmul(v[r], w);
+                acc.x = acc.x + p.x; acc.y = acc.y + p.y;
+            }
+            d[base + sidx * Ns] = acc;
+        }
+    }
+}
+
+// All passes of a plan; returns the buffer holding the result.
+__device__ double2 *run_passes(double2 *a, double2 *b, int L, const FftPlan &p,
+                               const double2 *__restrict__ W, bool fwd)
+{
+    int Ns = 1;
+    for (int ip = 0; ip < p.np; ++ip) {
+        const int R = p.radix[ip];
+        if (R == 8)
+            pass_fixed<8>(a, b, p.n, L, Ns, W, fwd);
+        else if (R == 4)
+            pass_fixed<4>(a, b, p.n, L, Ns, W, fwd);
+        else if (R == 2)
+            pass_fixed<2>(a, b, p.n, L, Ns, W, fwd);
+        else
+            pass_generic(a, b, p.n, L, R, Ns, W, fwd);
+        __syncthreads();
+        Ns *= R;
+        double2 *t = a; a = b; b = t;
+    }
+    return a;
+}
+
+__global__ void k_fft_rows(double2 *data, int nx, int ny, int rows, FftPlan p,
+                           const double2 *__restrict__ W, bool fwd)
+{
+    extern __shared__ double2 sm[];
+    double2 *a = sm, *b = sm + (size_t)rows * ny;
+    const int r0 = blockIdx.x * rows;
+    const int nr = min(rows, nx - r0);
+    double2 *g = data + (size_t)r0 * ny;
+    for (int e = threadIdx.x; e < nr * ny; e += blockDim.x) a[e] = g[e];
+    __syncthreads();
+    double2 *res = run_passes(a, b, nr, p, W, fwd);
+    for (int e = threadIdx.x; e < nr * ny; e += blockDim.x) g[e] = res[e];
+}
+
+__global__ void k_fft_cols(double2 *data, int nx, int ny, int cols, FftPlan p,
+                           const double2 *__restrict__ W, bool fwd)
+{
+    extern __shared__ double2 sm[];
+    double2 *a = sm, *b = sm + (size_t)cols * nx;
+    const int c0 = blockIdx.x * cols;
+    const int nc = min(cols, ny - c0);
+    for (int e = threadIdx.x; e < nc * nx; e += blockDim.x) {
+        int i = e / nc, c = e - i * nc;
+        a[(size_t)c * nx + i] = data[(size_t)i * ny + c0 + c];
+    }
+    __syncthreads();
+    double2 *res = run_passes(a, b, nc, p, W, fwd);
+    for (int e = threadIdx.x; e < nc * nx; e += blockDim.x) {
+        int i = e / nc, c = e - i * nc;
+        data[(size_t)i * ny + c0 + c] = res[(size_t)c * nx + i];
+    }
+}
+
+__global__ void k_invert(double2 *a, int nx, int ny, double s)
+{
+    const int mx = nx / 2, my = ny / 2;
+    const size_t total = (size_t)nx * my;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+         e += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(e / my), j = (int)(e - (size_t)i * my);
+        int jn = j + my, in = i + mx;
+        if (i >= mx) in = in - 2 * mx;
+        double2 *pp = a + (size_t)in * ny + jn, *qq = a + (size_t)i * ny + j;
+        double2 t = *pp, u = *qq;
+        *pp = make_double2(u.x * s, u.y * s);
+        *qq = make_double2(t.x * s, t.y * s);
+    }
+}
+
+// Block sum of two doubles with a fixed tree; thread 0 gets the result.
+__device__ void block_sum2(double &a, double &b)
+{
+    __shared__ double sa[kThreads], sb[kThreads];
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int off = kThreads / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) {
+            sa[threadIdx.x] += sa[threadIdx.x + off];
+            sb[threadIdx.x] += sb[threadIdx.x + off];
+        }
+        __syncthreads();
+    }
+    a = sa[0];
+    b = sb[0];
+}
+
+__device__ __forceinline__ double mag_of(double2 c) { return sqrt(c.x * c.x + c.y * c.y); }
+
+__device__ __forceinline__ double2 set_mag(double2 c, double value)
+{
+    double mag = mag_of(c);
+    if (mag == 0) return make_double2(value, 0.0);
+    double q = value / mag;
+    return make_double2(c.x * q, c.y * q);
+}
+
+__global__ void k_scale_intensity(double2 *c, const double *__restrict__ isqrt,
+                                  const double *__restrict__ bs, size_t n, double *partials)
+{
+    double diff = 0, mag = 0;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        if (bs == nullptr || bs[k] > 0) {
+            double cis = isqrt[k];
+            double2 v = c[k];
+            double cm = mag_of(v);
+            c[k] = set_mag(v, cis);
+            mag += cis * cis;
+            diff += (cm - cis) * (cm - cis);
+        }
+    }
+    block_sum2(diff, mag);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = diff;
+        partials[2 * blockIdx.x + 1] = mag;
+    }
+}
+
+__global__ void k_finish_error(const double *partials, int nblocks, double *err)
+{
+    double diff = 0, mag = 0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+        diff += partials[2 * b];
+        mag += partials[2 * b + 1];
+    }
+    block_sum2(diff, mag);
+    if (threadIdx.x == 0) *err = (diff / mag);
+}
+
+__global__ void k_support(double2 *c, const double *__restrict__ sup, size_t n)
+{
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        double sv = sup[k];
+        if (sv == 0) {
+            c[k] = make_double2(0.0, 0.0);
+        } else if (sv < 1) {
+            double2 v = c[k];
+            c[k] = make_double2(v.x * sv, v.y * sv);
+        }
+    }
+}
+
+struct Weights { double w[5]; double id; };
+
+__global__ void k_combine(double2 *x, const double2 *__restrict__ pfs,
+                          const double2 *__restrict__ pf, const double2 *__restrict__ ps,
+                          const double2 *__restrict__ psf, Weights W, size_t n)
+{
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        double2 v = x[k];
+        double vr = W.id * v.x, vi = W.id * v.y;
+        if (pfs) { double2 t = pfs[k]; vr += W.w[1] * t.x; vi += W.w[1] * t.y; }
+        if (pf) { double2 t = pf[k]; vr += W.w[3] * t.x; vi += W.w[3] * t.y; }
+        if (ps) { double2 t = ps[k]; vr += W.w[2] * t.x; vi += W.w[2] * t.y; }
+        if (psf) { double2 t = psf[k]; vr += W.w[0] * t.x; vi += W.w[0] * t.y; }
+        x[k] = make_double2(vr, vi);
+    }
+}
+
+__global__ void k_multiply_factors(double2 *c, const double2 *__restrict__ coef, int nx, int ny,
+                                   int direction)
+{
+    const double x_mid = (nx - 1) / 2.0, y_mid = (ny - 1) / 2.0;
+    const int qy = ny / 2;
+    const size_t n = (size_t)nx * ny;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(e / ny), j = (int)(e - (size_t)i * ny);
+        double2 o = c[e];
+        int i_ = (int)(x_mid - fabs(x_mid - i));
+        int j_ = (int)(y_mid - fabs(y_mid - j));
+        double2 cf = coef[(size_t)i_ * qy + j_];
+        double cr = cf.x, ci = direction * cf.y;
+        c[e] = make_double2(o.x * cr - o.y * ci, o.y * cr + o.x * ci);
+    }
+}
+
+__global__ void k_add_scaled(double2 *c, const double2 *__restrict__ b, double sc, size_t n)
+{
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        double2 v = c[k], t = b[k];
+        c[k] = make_double2(v.x + sc * t.x, v.y + sc * t.y);
+    }
+}
+
+__global__ void k_scale(double2 *c, double f, size_t n)
+{
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        double2 v = c[k];
+        c[k] = make_double2(v.x * f, v.y * f);
+    }
+}
+
+__global__ void k_pad(const double2 *__restrict__ x, int nx, int ny, double2 *p, int px, int py)
+{
+    const int mx = nx + 2 * px, my = ny + 2 * py;
+    const size_t n = (size_t)mx * my;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(e / my) - px, j = (int)(e % my) - py;
+        p[e] = (i >= 0 && i < nx && j >= 0 && j < ny) ? x[(size_t)i * ny + j]
+                                                      : make_double2(0.0, 0.0);
+    }
+}
+
+__global__ void k_unpad(const double2 *__restrict__ p, int nx, int ny, int px, int py,
+                        double2 *x)
+{
+    const int my = ny + 2 * py;
+    const size_t n = (size_t)nx * ny;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(e / ny), j = (int)(e - (size_t)i * ny);
+        x[e] = p[(size_t)(i + px) * my + j + py];
+    }
+}
+
+__global__ void k_poly_expand(const double2 *__restrict__ c, const double *__restrict__ spec,
+                              int nl, double lambdac, int nx, int ny, int px, int py,
+                              double *isc)
+{
+    const int mx = nx + 2 * px, my = ny + 2 * py;
+    const size_t n = (size_t)nx * ny;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(e / ny) + px, j = (int)(e % ny) + py; // padded coordinates
+        double acc = 0.0;
+        for (int sn = 0; sn < nl; ++sn) {
+            double lambda = spec[2 * sn], weightl = spec[2 * sn + 1];
+            double lf = lambda / lambdac;
+            double xval = lf * (i - nx / 2.0) + nx / 2.0;
+            double yval = lf * (j - ny / 2.0) + ny / 2.0;
+            if (((xval >= 0) && (xval < mx)) && ((yval >= 0) && (yval < my))) {
+                double m = mag_of(c[(size_t)(int)xval * my + (int)yval]);
+                acc = acc + weightl * (m * m);
+            }
+        }
+        isc[e] = sqrt(acc);
+    }
+}
+
+__global__ void k_poly_scale(double2 *c, const double *__restrict__ isc,
+                             const double *__restrict__ isqrt, const double *__restrict__ bs,
+                             int nx, int ny, int px, int py, double *partials)
+{
+    const int my = ny + 2 * py;
+    const size_t n = (size_t)nx * ny;
+    double diff = 0, mag = 0;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        if (bs == nullptr || bs[e] > 0) {
+            int i = (int)(e / ny), j = (int)(e - (size_t)i * ny);
+            double calc = isc[e], meas = isqrt[e], scaled;
+            double2 *pp = c + (size_t)(i + px) * my + j + py;
+            double2 v = *pp;
+            if (calc == 0.0)
+                scaled = 0.0;
+            else
+                scaled = mag_of(v) * meas / calc;
+            *pp = set_mag(v, scaled);
+            mag += meas * meas;
+            diff += (meas - calc) * (meas - calc);
+        }
+    }
+    block_sum2(diff, mag);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = diff;
+        partials[2 * blockIdx.x + 1] = mag;
+    }
+}
+
+__global__ void k_magnitude(const double2 *__restrict__ c, double *out, size_t n)
+{
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x)
+        out[k] = mag_of(c[k]);
+}
+
+__global__ void k_convolve(const double *__restrict__ in, double *out, int nx, int ny,
+                           const double *__restrict__ g, int cut)
+{
+    const size_t n = (size_t)nx * ny;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(e / ny), j = (int)(e - (size_t)i * ny);
+        double nv = 0;
+        for (int i2 = i - cut; i2 <= i + cut; ++i2)
+            for (int j2 = j - cut; j2 <= j + cut; ++j2)
+                if (i2 < nx && i2 >= 0 && j2 >= 0 && j2 < ny)
+                    nv += in[(size_t)i2 * ny + j2] * g[abs(i - i2) * (cut + 1) + abs(j - j2)];
+        out[e] = nv;
+    }
+}
+
+__global__ void k_max_partial(const double *__restrict__ a, size_t n, double *partials)
+{
+    __shared__ double sm[kThreads];
+    __shared__ int has[kThreads];
+    double m = 0;
+    int h = 0;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        double v = a[k];
+        if (!h || v > m) { m = v; h = 1; }
+    }
+    sm[threadIdx.x] = m;
+    has[threadIdx.x] = h;
+    __syncthreads();
+    for (int off = kThreads / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) {
+            double o = sm[threadIdx.x + off];
+            int oh = has[threadIdx.x + off];
+            if (oh && (!has[threadIdx.x] || o > sm[threadIdx.x])) {
+                sm[threadIdx.x] = o;
+                has[threadIdx.x] = 1;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = sm[0];
+        partials[2 * blockIdx.x + 1] = has[0];
+    }
+}
+
+__global__ void k_max_finish(const double *partials, int nb, double *out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double m = 0;
+        int h = 0;
+        for (int b = 0; b < nb; ++b)
+            if (partials[2 * b + 1] != 0 && (!h || partials[2 * b] > m)) {
+                m = partials[2 * b];
+                h = 1;
+            }
+        *out = m;
+    }
+}
+
+// apply_threshold with the reference's loop bounds (i < nx, j < nx) and
+// Real_2D::get's (x > nx, y > ny) test: an element at linear index L is
+// visited once per pair (i, j = L - i*ny) with 0 <= j < nx, in increasing i.
+__global__ void k_threshold(double *a, int nx, int ny, double t, const double *dmax)
+{
+    const double lim = t * (*dmax);
+    const size_t n = (size_t)nx * ny;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        long long L = (long long)e;
+        long long ilo = (L - nx + 1 + ny - 1) / ny; // ceil((L-nx+1)/ny) for L-nx+1 >= 0
+        if (L - nx + 1 < 0) ilo = 0;
+        long long ihi = L / ny;
+        if (ihi > nx - 1) ihi = nx - 1;
+        if (ilo > ihi) continue;
+        double cur = a[e];
+        for (long long i = ilo; i <= ihi; ++i) {
+            long long j = L - i * ny;
+            double v = (j > ny) ? 0.0 : cur;
+            cur = (v < lim) ? 0.0 : 1.0;
+        }
+        a[e] = cur;
+    }
+}
+
+__global__ void k_divide_by_max(const double *__restrict__ in, double *out, size_t n,
+                                const double *dmax)
+{
+    const double m = *dmax;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x)
+        out[k] = in[k] / m;
+}
+
+__global__ void k_fresnel_set_t(const double2 *__restrict__ t, const double2 *__restrict__ ill,
+                                double2 *esw, int nx, int ny)
+{
+    const size_t n = (size_t)nx * ny;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        int j = (int)(e % ny);
+        if (ny >= nx && j >= nx) continue;
+        double2 l = ill[e], tt = t[e];
+        esw[e] = make_double2(l.x * tt.x - l.y * tt.y - l.x, l.x * tt.y + l.y * tt.x - l.y);
+    }
+}
+
+__global__ void k_fresnel_get_t(const double2 *__restrict__ esw, const double2 *__restrict__ ill,
+                                double2 *out, size_t n)
+{
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        double2 l = ill[k];
+        double denom = l.x * l.x + l.y * l.y;
+        if (denom != 0) {
+            double2 e = esw[k];
+            double rn = l.x * (e.x + l.x) + l.y * (e.y + l.y);
+            double in = l.x * (e.y + l.y) - l.y * (e.x + l.x);
+            out[k] = make_double2(rn / denom, in / denom);
+        } else {
+            out[k] = make_double2(1.0, 0.0);
+        }
+    }
+}
+
+__global__ void k_autocorr_fill(const double *__restrict__ isqrt, double2 *t, size_t n)
+{
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        double comp = (1.0 / sqrt(2.0)) * (isqrt[k] * isqrt[k]);
+        t[k] = make_double2(comp, comp);
+    }
+}
+
+inline int grid_of(size_t n) { return std::min(blocks_for(n), 148 * 16); }
+
+} // namespace
+
+void Fft2d::init(int nx_, int ny_)
+{
+    nx = nx_;
+    ny = ny_;
+    px = make_plan(nx);
+    py = make_plan(ny);
+    std::vector<double2> hx = twiddles(nx), hy = twiddles(ny);
+    wx.alloc(nx);
+    wy.alloc(ny);
+    NADIA_CUDA(cudaMemcpy(wx.p, hx.data(), wx.bytes(), cudaMemcpyHostToDevice));
+    NADIA_CUDA(cudaMemcpy(wy.p, hy.data(), wy.bytes(), cudaMemcpyHostToDevice));
+    const size_t budget = 128 * 1024;
+    rows_per_block = std::max(1, 2048 / ny);
+    while (rows_per_block > 1 && 2 * (size_t)rows_per_block * ny * sizeof(double2) > budget)
+        --rows_per_block;
+    cols_per_block = std::max(1, std::min(8, 4096 / nx));
+    while (cols_per_block > 1 && 2 * (size_t)cols_per_block * nx * sizeof(double2) > budget)
+        --cols_per_block;
+    row_smem = 2 * (size_t)rows_per_block * ny * sizeof(double2);
+    col_smem = 2 * (size_t)cols_per_block * nx * sizeof(double2);
+    NADIA_REQUIRE(row_smem <= 227 * 1024 && col_smem <= 227 * 1024, NADIA_ERR_INVALID,
+                  "grid too large for the FP64 transform");
+    NADIA_CUDA(cudaFuncSetAttribute(k_fft_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)std::max<size_t>(row_smem, 48 * 1024)));
+    NADIA_CUDA(cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)std::max<size_t>(col_smem, 48 * 1024)));
+}
+
+void Fft2d::exec(double2 *a, bool forward, cudaStream_t s) const
+{
+    int gr = (nx + rows_per_block - 1) / rows_per_block;
+    k_fft_rows<<<gr, kThreads, row_smem, s>>>(a, nx, ny, rows_per_block, py, wy.p, forward);
+    int gc = (ny + cols_per_block - 1) / cols_per_block;
+    k_fft_cols<<<gc, kThreads, col_smem, s>>>(a, nx, ny, cols_per_block, px, wx.p, forward);
+    NADIA_CUDA(cudaGetLastError());
+}
+
+void invert(double2 *a, int nx, int ny, bool sc, cudaStream_t s)
+{
+    double f = 1;
+    if (sc) f = 1.0 / (sqrt((double)(nx * ny)));
+    k_invert<<<grid_of((size_t)nx * (ny / 2)), kThreads, 0, s>>>(a, nx, ny, f);
+}
+
+void scale_intensity(double2 *c, const double *isqrt, const double *bs, size_t n,
+                     double *partials, double *err, cudaStream_t s)
+{
+    k_scale_intensity<<<kRedBlocks, kThreads, 0, s>>>(c, isqrt, bs, n, partials);
+    k_finish_error<<<1, kThreads, 0, s>>>(partials, kRedBlocks, err);
+}
+
+void support_constraint(double2 *c, const double *sup, size_t n, cudaStream_t s)
+{
+    k_support<<<grid_of(n), kThreads, 0, s>>>(c, sup, n);
+}
+
+void combine(double2 *x, const double2 *pfs, const double2 *pf, const double2 *ps,
+             const double2 *psf, const double w[5], size_t n, cudaStream_t s)
+{
+    Weights W;
+    for (int i = 0; i < 5; ++i) W.w[i] = w[i];
+    W.id = 1 + w[4];
+    k_combine<<<grid_of(n), kThreads, 0, s>>>(x, pfs, pf, ps, psf, W, n);
+}
+
+void multiply_factors(double2 *c, const double2 *coef, int nx, int ny, int direction,
+                      cudaStream_t s)
+{
+    k_multiply_factors<<<grid_of((size_t)nx * ny), kThreads, 0, s>>>(c, coef, nx, ny, direction);
+}
+
+void add_scaled(double2 *c, const double2 *b, double sc, size_t n, cudaStream_t s)
+{
+    k_add_scaled<<<grid_of(n), kThreads, 0, s>>>(c, b, sc, n);
+}
+
+void scale(double2 *c, double f, size_t n, cudaStream_t s)
+{
+    k_scale<<<grid_of(n), kThreads, 0, s>>>(c, f, n);
+}
+
+void pad(const double2 *x, int nx, int ny, double2 *p, int px, int py, cudaStream_t s)
+{
+    size_t n = (size_t)(nx + 2 * px) * (ny + 2 * py);
+    k_pad<<<grid_of(n), kThreads, 0, s>>>(x, nx, ny, p, px, py);
+}
+
+void unpad(const double2 *p, int nx, int ny, int px, int py, double2 *x, cudaStream_t s)
+{
+    k_unpad<<<grid_of((size_t)nx * ny), kThreads, 0, s>>>(p, nx, ny, px, py, x);
+}
+
+void poly_expand(const double2 *c, const double *spec, int nl, double lambdac, int nx, int ny,
+                 int px, int py, double *isc, cudaStream_t s)
+{
+    k_poly_expand<<<grid_of((size_t)nx * ny), kThreads, 0, s>>>(c, spec, nl, lambdac, nx, ny,
+                                                               px, py, isc);
+}
+
+void poly_scale(double2 *c, const double *isc, const double *isqrt, const double *bs, int nx,
+                int ny, int px, int py, double *partials, double *err, cudaStream_t s)
+{
+    k_poly_scale<<<kRedBlocks, kThreads, 0, s>>>(c, isc, isqrt, bs, nx, ny, px, py, partials);
+    k_finish_error<<<1, kThreads, 0, s>>>(partials, kRedBlocks, err);
+}
+
+void magnitude(const double2 *c, double *out, size_t n, cudaStream_t s)
+{
+    k_magnitude<<<grid_of(n), kThreads, 0, s>>>(c, out, n);
+}
+
+void convolve(const double *in, double *out, int nx, int ny, const double *g, int cut,
+              cudaStream_t s)
+{
+    k_convolve<<<grid_of((size_t)nx * ny), kThreads, 0, s>>>(in, out, nx, ny, g, cut);
+}
+
+void max_reduce(const double *a, size_t n, double *partials, double *out, cudaStream_t s)
+{
+    k_max_partial<<<kRedBlocks, kThreads, 0, s>>>(a, n, partials);
+    k_max_finish<<<1, 32, 0, s>>>(partials, kRedBlocks, out);
+}
+
+void threshold(double *a, int nx, int ny, double t, const double *dmax, cudaStream_t s)
+{
+    k_threshold<<<grid_of((size_t)nx * ny), kThreads, 0, s>>>(a, nx, ny, t, dmax);
+}
+
+void divide_by_max(const double *in, double *out, size_t n, const double *dmax, cudaStream_t s)
+{
+    k_divide_by_max<<<grid_of(n), kThreads, 0, s>>>(in, out, n, dmax);
+}
+
+void fresnel_set_transmission(const double2 *t, const double2 *ill, double2 *esw, int nx, int ny,
+                              cudaStream_t s)
+{
+    k_fresnel_set_t<<<grid_of((size_t)nx * ny), kThreads, 0, s>>>(t, ill, esw, nx, ny);
+}
+
+void fresnel_get_transmission(const double2 *esw, const double2 *ill, double2 *out, size_t n,
+                              cudaStream_t s)
+{
+    k_fresnel_get_t<<<grid_of(n), kThreads, 0, s>>>(esw, ill, out, n);
+}
+
+void autocorr_fill(const double *isqrt, double2 *t, size_t n, cudaStream_t s)
+{
+    k_autocorr_fill<<<grid_of(n), kThreads, 0, s>>>(isqrt, t, n);
+}
+
+} // namespace plain
+} // namespace nadia

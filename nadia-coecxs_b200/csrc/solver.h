@@ -1,0 +1,132 @@
+// solver.h -- one reconstruction (the state of one PlanarCDI / FresnelCDI /
+// PolyCDI object) resident on a CUDA device.  The algorithm bookkeeping
+// (weights, relaxation quirk, n-best ranking, error history) lives here on
+// the host; the arithmetic runs in the plain FP64 kernels (plain64.cu) or
+// the fused FP32 engine (fused32.cu).
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "common.h"
+#include "plain64.h"
+
+namespace nadia {
+
+class Fused32;
+
+enum { PSF = 0, PFS = 1, PS = 2, PF = 3, PI = 4 }; // BaseCDI.h:76
+
+struct Solver {
+    int kind = NADIA_PLANAR, nx = 0, ny = 0, prec = NADIA_FP64, n_best = 0;
+    size_t n = 0;
+    int device = 0;
+    cudaStream_t st = nullptr;
+
+    // algorithm state (BaseCDI.h:87-150)
+    double beta = 0.9;
+    int algorithm = NADIA_CUSTOM;
+    double w[5] = {0, 0, 0, 0, 0};
+
+    // host copies used by initialise_estimate and auto_set_norm
+    std::vector<double> h_isqrt;
+    std::vector<double> h_support;
+    bool h_support_valid = true;
+    bool has_beam_stop = false;
+
+    // error history: one slot per iteration on the device
+    static constexpr int kRing = 65536;
+    long long iters = 0;
+    DevBuf<double> d_err;     // [0] current error
+    DevBuf<double> d_ring;    // kRing errors
+    DevBuf<double> partials;  // reduction scratch
+
+    // n-best (BaseCDI.c++:43-50, 390-413): slot buffers, rank order, errors
+    std::vector<DevBuf<double2>> best64;
+    std::vector<DevBuf<float2>> best32;
+    std::vector<int> best_slot;
+    std::vector<double> best_err;
+
+    // FP64 device state
+    DevBuf<double2> x, tPFS, tPF, tPS, tPSF;
+    DevBuf<double> support, isqrt, beam_stop;
+    plain::Fft2d fft;
+    DevBuf<double> recon, tmp, gauss, dmax;
+
+    // FresnelCDI
+    std::vector<double> h_illum; // detector white field x norm (interleaved)
+    double norm = 1, wavelength = 0, zfd = 0, zfs = 0, pixel = 0;
+    DevBuf<double2> illum, illum_sample, coef;
+
+    // PolyCDI
+    std::vector<double> spectrum; // (wavelength, normalised weight) rows
+    int nlambda = 0, px = 0, py = 0;
+    double lambdac = 0;
+    bool has_spectrum = false;
+    DevBuf<double> d_spec, isc;
+    DevBuf<double2> padded;
+    plain::Fft2d fft_pad;
+
+    std::unique_ptr<Fused32> f32;
+
+    Solver(int kind, int nx, int ny, int prec, int n_best);
+    ~Solver();
+
+    // inputs
+    void set_support(const double *obj, bool soften);
+    void set_intensity(const double *I);
+    void set_beam_stop(const double *mask);
+    void set_spectrum(const double *wl_weight, int nl);
+    void fresnel_init(const double *white_field, double wl, double zfd, double zfs, double pixel,
+                      double norm);
+    void fresnel_set_experimental_parameters(double wl, double zfd, double zfs, double pixel);
+    void fresnel_set_norm(double nn);
+    void fresnel_auto_set_norm();
+
+    // algorithm
+    void set_algorithm(int alg);
+    void set_custom(const double m[10]);
+    void set_relaxation_parameter(double b);
+
+    // estimate
+    void initialise_estimate(int seed);
+    void set_esw(const double *h);
+    void get_esw(double *h);
+    void set_esw_f32(const float *h);
+    void get_esw_f32(float *h);
+    void set_transmission(const double *h);
+    void get_transmission(double *h);
+    void get_illumination_at_sample(double *h);
+
+    // run
+    void iterate(int count);
+    double get_error();
+    void get_error_history(double *out, int count);
+    void apply_shrinkwrap(double gauss_width, double threshold);
+    void get_support(double *h);
+    void get_best(int index, double *err, double *h);
+    void reset_best();
+    void single_op(int op, double *field);
+    void autocorrelation(double *out);
+    void sync();
+
+    // FP64 plain path internals
+    void plain_iterate_once();
+    void plain_project(double2 *c);
+    void plain_propagate_to(double2 *c, bool padded_grid);
+    void plain_propagate_from(double2 *c, bool padded_grid);
+    void plain_scale(double2 *c);
+    void plain_convolve(double *arr, double gauss_width, int cut);
+    void ensure_temps();
+    void update_n_best();
+    void record_error();
+    void require_poly_ready() const;
+    const double *bs_ptr() const { return has_beam_stop ? beam_stop.p : nullptr; }
+    std::vector<double> gauss_table(double gauss_width, int cut) const;
+    void upload_support();
+};
+
+// read_spec semantics (NADIA/src/io_spec.c:61-133): rows of (1/energy, weight).
+std::vector<double> read_spec_file(const char *path);
+
+} // namespace nadia

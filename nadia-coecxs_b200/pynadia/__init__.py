@@ -1,0 +1,323 @@
+"""Python binding of libnadia_b200 (the C ABI in include/nadia_b200.h).
+
+``Solver`` mirrors the reference's class API (NADIA/include/BaseCDI.h,
+PlanarCDI.h, FresnelCDI.h, PolyCDI.h): set_support, set_intensity,
+set_beam_stop, set_algorithm, set_relaxation_parameter, initialise_estimate,
+iterate, get_error, apply_shrinkwrap, get_transmission, ... with numpy arrays
+(complex128 for complex fields, float64 for real ones, shape (nx, ny),
+element (x, y) as in the reference's x*ny+y layout).
+
+There is no fallback: if the CUDA library is missing or fails to load, the
+import raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "libnadia_b200.so")
+
+ER, BIO, BOO, HIO, DM, SF, ASR, HPR, RAAR, CUSTOM = range(10)
+ALGORITHMS = {"ER": ER, "BIO": BIO, "BOO": BOO, "HIO": HIO, "DM": DM, "SF": SF, "ASR": ASR,
+              "HPR": HPR, "RAAR": RAAR}
+PLANAR, FRESNEL, POLY = 0, 1, 2
+FP64, FP32 = 0, 1
+KINDS = {"planar": PLANAR, "fresnel": FRESNEL, "poly": POLY}
+
+STATUS = {0: "OK", 1: "INVALID", 2: "STATE", 3: "UNSUPPORTED", 4: "CUDA", 5: "NOMEM",
+          6: "RANGE"}
+
+
+class NadiaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (STATUS.get(code, "?"), code, msg))
+        self.code = code
+
+
+_D = ctypes.POINTER(ctypes.c_double)
+_F = ctypes.POINTER(ctypes.c_float)
+_H = ctypes.c_void_p
+_I = ctypes.c_int
+
+_PROTOS = {
+    "nadia_last_error": (ctypes.c_char_p, []),
+    "nadia_version": (ctypes.c_char_p, []),
+    "nadia_planar_create": (_I, [_I, _I, _I, _I, ctypes.POINTER(_H)]),
+    "nadia_fresnel_create": (_I, [_I, _I, _I, _D, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, _I,
+                                  ctypes.POINTER(_H)]),
+    "nadia_poly_create": (_I, [_I, _I, _I, ctypes.c_double, _I, ctypes.POINTER(_H)]),
+    "nadia_destroy": (_I, [_H]),
+    "nadia_get_size": (_I, [_H, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "nadia_set_support": (_I, [_H, _D, _I]),
+    "nadia_set_intensity": (_I, [_H, _D]),
+    "nadia_set_beam_stop": (_I, [_H, _D]),
+    "nadia_poly_set_spectrum": (_I, [_H, _D, _I]),
+    "nadia_poly_set_spectrum_file": (_I, [_H, ctypes.c_char_p]),
+    "nadia_poly_get_padding": (_I, [_H, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "nadia_set_algorithm": (_I, [_H, _I]),
+    "nadia_set_custom_algorithm": (_I, [_H, _D]),
+    "nadia_set_relaxation_parameter": (_I, [_H, ctypes.c_double]),
+    "nadia_get_algorithm_structure": (_I, [_H, _D, ctypes.POINTER(_I)]),
+    "nadia_custom_weights": (None, [_D, _D]),
+    "nadia_initialise_estimate": (_I, [_H, _I]),
+    "nadia_set_exit_surface_wave": (_I, [_H, _D]),
+    "nadia_get_exit_surface_wave": (_I, [_H, _D]),
+    "nadia_set_exit_surface_wave_f32": (_I, [_H, _F]),
+    "nadia_get_exit_surface_wave_f32": (_I, [_H, _F]),
+    "nadia_iterate": (_I, [_H, _I]),
+    "nadia_get_error": (_I, [_H, _D]),
+    "nadia_get_error_history": (_I, [_H, _D, _I]),
+    "nadia_apply_shrinkwrap": (_I, [_H, ctypes.c_double, ctypes.c_double]),
+    "nadia_get_support": (_I, [_H, _D]),
+    "nadia_get_best_result": (_I, [_H, _I, _D, _D]),
+    "nadia_reset_best": (_I, [_H]),
+    "nadia_get_transmission": (_I, [_H, _D]),
+    "nadia_set_transmission": (_I, [_H, _D]),
+    "nadia_fresnel_auto_set_norm": (_I, [_H]),
+    "nadia_fresnel_set_norm": (_I, [_H, ctypes.c_double]),
+    "nadia_fresnel_get_illumination_at_sample": (_I, [_H, _D]),
+    "nadia_propagate_to_detector": (_I, [_H, _D]),
+    "nadia_propagate_from_detector": (_I, [_H, _D]),
+    "nadia_scale_intensity": (_I, [_H, _D]),
+    "nadia_apply_support": (_I, [_H, _D]),
+    "nadia_project_intensity": (_I, [_H, _D]),
+    "nadia_get_intensity_autocorrelation": (_I, [_H, _D]),
+    "nadia_synchronize": (_I, [_H]),
+    "nadia_iterate_many": (_I, [ctypes.POINTER(_H), _I, _I]),
+}
+
+_LIB = None
+
+
+def load(path=LIB_PATH):
+    """Load the CUDA library (raises if it is missing)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(path):
+            raise ImportError("libnadia_b200.so not built (run __graft_entry__.build() or "
+                              "python nadia-coecxs_b200/build.py): %s" % path)
+        lib = ctypes.CDLL(path)
+        for name, (res, args) in _PROTOS.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def exported_symbols():
+    return sorted(_PROTOS)
+
+
+def _check(rc):
+    if rc != 0:
+        raise NadiaError(rc, _LIB.nadia_last_error().decode())
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_D)
+
+
+def custom_weights(m):
+    """Weights [PsPf, PfPs, Ps, Pf, I] of set_custom_algorithm(m1..m10) (BaseCDI.c++:245-249)."""
+    lib = load()
+    m = np.ascontiguousarray(m, dtype=np.float64)
+    w = np.zeros(5)
+    lib.nadia_custom_weights(_ptr(m), _ptr(w))
+    return w
+
+
+class Solver:
+    """One reconstruction on the GPU (PlanarCDI / FresnelCDI / PolyCDI)."""
+
+    def __init__(self, kind, nx, ny, precision=FP64, n_best=0, white_field=None,
+                 wavelength=None, focal_detector_length=None, focal_sample_length=None,
+                 pixel_size=None, normalisation=1.0, beta=0.9):
+        self.lib = load()
+        self.kind = kind
+        self.nx, self.ny = int(nx), int(ny)
+        self.precision = precision
+        h = _H()
+        if kind == "planar":
+            _check(self.lib.nadia_planar_create(nx, ny, precision, n_best, ctypes.byref(h)))
+        elif kind == "fresnel":
+            wf = np.ascontiguousarray(white_field, dtype=np.complex128)
+            assert wf.shape == (nx, ny)
+            _check(self.lib.nadia_fresnel_create(nx, ny, precision, _ptr(wf), wavelength,
+                                                 focal_detector_length, focal_sample_length,
+                                                 pixel_size, normalisation, n_best,
+                                                 ctypes.byref(h)))
+        elif kind == "poly":
+            _check(self.lib.nadia_poly_create(nx, ny, precision, beta, n_best, ctypes.byref(h)))
+        else:
+            raise ValueError(kind)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nadia_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _real(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.shape == (self.nx, self.ny), a.shape
+        return a
+
+    def _cplx(self, a):
+        a = np.ascontiguousarray(a, dtype=np.complex128)
+        assert a.shape == (self.nx, self.ny), a.shape
+        return a
+
+    def set_support(self, s, soften=False):
+        _check(self.lib.nadia_set_support(self.h, _ptr(self._real(s)), int(bool(soften))))
+
+    def set_intensity(self, i):
+        _check(self.lib.nadia_set_intensity(self.h, _ptr(self._real(i))))
+
+    def set_beam_stop(self, b):
+        _check(self.lib.nadia_set_beam_stop(self.h, _ptr(self._real(b))))
+
+    def set_spectrum(self, spec):
+        if isinstance(spec, str):
+            _check(self.lib.nadia_poly_set_spectrum_file(self.h, spec.encode()))
+            return
+        spec = np.ascontiguousarray(spec, dtype=np.float64)
+        assert spec.ndim == 2 and spec.shape[1] == 2
+        _check(self.lib.nadia_poly_set_spectrum(self.h, _ptr(spec), spec.shape[0]))
+
+    def get_padding(self):
+        a, b = _I(), _I()
+        _check(self.lib.nadia_poly_get_padding(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def set_algorithm(self, alg):
+        if isinstance(alg, str):
+            alg = ALGORITHMS[alg]
+        _check(self.lib.nadia_set_algorithm(self.h, int(alg)))
+
+    def set_custom_algorithm(self, m):
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        assert m.shape == (10,)
+        _check(self.lib.nadia_set_custom_algorithm(self.h, _ptr(m)))
+
+    def set_relaxation_parameter(self, b):
+        _check(self.lib.nadia_set_relaxation_parameter(self.h, float(b)))
+
+    def algorithm_structure(self):
+        w = np.zeros(5)
+        a = _I()
+        _check(self.lib.nadia_get_algorithm_structure(self.h, _ptr(w), ctypes.byref(a)))
+        return w, a.value
+
+    def initialise_estimate(self, seed=0):
+        _check(self.lib.nadia_initialise_estimate(self.h, int(seed)))
+
+    def set_exit_surface_wave(self, e):
+        _check(self.lib.nadia_set_exit_surface_wave(self.h, _ptr(self._cplx(e))))
+
+    def get_exit_surface_wave(self):
+        out = np.empty((self.nx, self.ny), dtype=np.complex128)
+        _check(self.lib.nadia_get_exit_surface_wave(self.h, _ptr(out)))
+        return out
+
+    def set_exit_surface_wave_f32(self, e):
+        e = np.ascontiguousarray(e, dtype=np.complex64)
+        _check(self.lib.nadia_set_exit_surface_wave_f32(self.h, e.ctypes.data_as(_F)))
+
+    def get_exit_surface_wave_f32(self):
+        out = np.empty((self.nx, self.ny), dtype=np.complex64)
+        _check(self.lib.nadia_get_exit_surface_wave_f32(self.h, out.ctypes.data_as(_F)))
+        return out
+
+    def iterate(self, n=1):
+        _check(self.lib.nadia_iterate(self.h, int(n)))
+
+    def get_error(self):
+        e = ctypes.c_double()
+        _check(self.lib.nadia_get_error(self.h, ctypes.byref(e)))
+        return e.value
+
+    def get_error_history(self, count):
+        out = np.empty(count)
+        _check(self.lib.nadia_get_error_history(self.h, _ptr(out), int(count)))
+        return out
+
+    def apply_shrinkwrap(self, gauss_width=1.5, threshold=0.1):
+        _check(self.lib.nadia_apply_shrinkwrap(self.h, gauss_width, threshold))
+
+    def get_support(self):
+        out = np.empty((self.nx, self.ny))
+        _check(self.lib.nadia_get_support(self.h, _ptr(out)))
+        return out
+
+    def get_best_result(self, index=0):
+        e = ctypes.c_double()
+        out = np.empty((self.nx, self.ny), dtype=np.complex128)
+        rc = self.lib.nadia_get_best_result(self.h, int(index), ctypes.byref(e), _ptr(out))
+        if rc == 6:
+            return None, None
+        _check(rc)
+        return e.value, out
+
+    def reset_best(self):
+        _check(self.lib.nadia_reset_best(self.h))
+
+    def get_transmission(self):
+        out = np.empty((self.nx, self.ny), dtype=np.complex128)
+        _check(self.lib.nadia_get_transmission(self.h, _ptr(out)))
+        return out
+
+    def set_transmission(self, t):
+        _check(self.lib.nadia_set_transmission(self.h, _ptr(self._cplx(t))))
+
+    def auto_set_norm(self):
+        _check(self.lib.nadia_fresnel_auto_set_norm(self.h))
+
+    def set_norm(self, n):
+        _check(self.lib.nadia_fresnel_set_norm(self.h, float(n)))
+
+    def get_illumination_at_sample(self):
+        out = np.empty((self.nx, self.ny), dtype=np.complex128)
+        _check(self.lib.nadia_fresnel_get_illumination_at_sample(self.h, _ptr(out)))
+        return out
+
+    def _op(self, f, c):
+        c = np.array(c, dtype=np.complex128, order="C", copy=True)
+        assert c.shape == (self.nx, self.ny)
+        _check(f(self.h, _ptr(c)))
+        return c
+
+    def propagate_to_detector(self, c):
+        return self._op(self.lib.nadia_propagate_to_detector, c)
+
+    def propagate_from_detector(self, c):
+        return self._op(self.lib.nadia_propagate_from_detector, c)
+
+    def scale_intensity(self, c):
+        return self._op(self.lib.nadia_scale_intensity, c)
+
+    def apply_support(self, c):
+        return self._op(self.lib.nadia_apply_support, c)
+
+    def project_intensity(self, c):
+        return self._op(self.lib.nadia_project_intensity, c)
+
+    def get_intensity_autocorrelation(self):
+        out = np.empty((self.nx, self.ny))
+        _check(self.lib.nadia_get_intensity_autocorrelation(self.h, _ptr(out)))
+        return out
+
+    def synchronize(self):
+        _check(self.lib.nadia_synchronize(self.h))
+
+
+def iterate_many(solvers, iterations):
+    """Step several reconstructions together (nadia_iterate_many)."""
+    lib = load()
+    arr = (_H * len(solvers))(*[s.h for s in solvers])
+    _check(lib.nadia_iterate_many(arr, len(solvers), int(iterations)))

@@ -1,0 +1,158 @@
+"""Reconstruction scenarios run identically on the reference (oracle/_ref), the
+oracle restatement and the CUDA library.  A scenario takes a factory
+``make(kind, nx, ny, **kw)`` and returns a dict of results."""
+import numpy as np
+
+from pynadia import synth
+
+ER, BIO, BOO, HIO, DM, SF, ASR, HPR, RAAR, CUSTOM = range(10)
+
+
+def planar_inputs(n, seed=5, beam_stop=4, ny=None):
+    ny = ny or n
+    c = synth.PlanarCase(n, max(3, n // 6), 2, 1e6, seed=seed, support_side=max(4, int(n * 0.42)),
+                         beam_stop=beam_stop, ny=ny)
+    return c
+
+
+def planar_mixed(make, n=32, n_best=2, ny=None, hio=24, raar=10, er=6, seed=3):
+    """ER/HIO/RAAR with shrinkwrap, a beam stop, the relaxation quirk and n-best."""
+    ny = ny or n
+    c = planar_inputs(n, ny=ny)
+    s = make("planar", n, ny, n_best=n_best)
+    s.set_support(c.support)
+    s.set_intensity(c.intensity)
+    s.set_beam_stop(c.beam_stop)
+    s.initialise_estimate(seed)
+    out = {"init": s.get_exit_surface_wave()}
+    errs = []
+    for _ in range(3):
+        s.iterate()
+        errs.append(s.get_error())
+    s.set_relaxation_parameter(0.7)  # no effect until the algorithm changes
+    s.set_algorithm(HIO)
+    for it in range(hio):
+        s.iterate()
+        errs.append(s.get_error())
+        if it % 8 == 7:
+            s.apply_shrinkwrap(1.5, 0.1)
+    s.set_relaxation_parameter(0.8)
+    s.set_algorithm(RAAR)
+    for _ in range(raar):
+        s.iterate()
+        errs.append(s.get_error())
+    s.set_algorithm(ER)
+    for _ in range(er):
+        s.iterate()
+        errs.append(s.get_error())
+    out["errors"] = np.array(errs)
+    out["esw"] = s.get_exit_surface_wave()
+    out["support"] = s.get_support()
+    out["transmission"] = s.get_transmission()
+    if n_best:
+        out["best_err"], out["best"] = s.get_best_result(n_best - 1)
+    return out
+
+
+def planar_custom(make, n=32, seed=4):
+    """DM and a custom algorithm (both use the PfPs term: two projections)."""
+    c = planar_inputs(n, beam_stop=0)
+    s = make("planar", n, n)
+    s.set_support(c.support, True)
+    s.set_intensity(c.intensity)
+    s.initialise_estimate(seed)
+    errs = []
+    s.set_algorithm(DM)
+    for _ in range(6):
+        s.iterate()
+        errs.append(s.get_error())
+    s.set_custom_algorithm(np.array([0.3, 0.5, 1.0, 0.1, 0.2, 0.05, 0.1, 0.2, 0.3, 0.1]))
+    for _ in range(6):
+        s.iterate()
+        errs.append(s.get_error())
+    return {"errors": np.array(errs), "esw": s.get_exit_surface_wave(),
+            "support": s.get_support()}
+
+
+def fresnel_inputs(n, seed=4):
+    return synth.FresnelCase(n, seed=seed)
+
+
+def fresnel_mixed(make, n=32, seed=2):
+    f = fresnel_inputs(n)
+    s = make("fresnel", n, n, white_field=f.white_field, wavelength=f.wavelength,
+             focal_detector_length=f.zfd, focal_sample_length=f.zfs, pixel_size=f.pixel,
+             normalisation=0.97)
+    s.set_support(f.support)
+    s.set_intensity(f.intensity)
+    s.auto_set_norm()
+    s.initialise_estimate(seed)
+    out = {"init": s.get_exit_surface_wave(), "illum": s.get_illumination_at_sample()}
+    errs = []
+    for _ in range(8):
+        s.iterate()
+        errs.append(s.get_error())
+    s.set_algorithm(HIO)
+    for it in range(12):
+        s.iterate()
+        errs.append(s.get_error())
+        if it == 6:
+            s.apply_shrinkwrap(2, 0.1)
+    out["errors"] = np.array(errs)
+    out["esw"] = s.get_exit_surface_wave()
+    out["transmission"] = s.get_transmission()
+    out["support"] = s.get_support()
+    return out
+
+
+def poly_inputs(n, padding, seed=9):
+    return synth.PolyCase(n, seed=seed, padding=padding, photons=1e7)
+
+
+def poly_mixed(make, n=32, padding=2, seed=7):
+    p = poly_inputs(n, padding)
+    s = make("poly", n, n, n_best=1)
+    s.set_support(p.support)
+    s.set_intensity(p.intensity)
+    s.set_spectrum(p.spectrum)
+    s.initialise_estimate(seed)
+    errs = []
+    for _ in range(3):
+        s.iterate()
+        errs.append(s.get_error())
+    s.set_algorithm(HIO)
+    for it in range(8):
+        s.iterate()
+        errs.append(s.get_error())
+        if it == 4:
+            s.apply_shrinkwrap(1.5, 0.1)
+    return {"errors": np.array(errs), "esw": s.get_exit_surface_wave(),
+            "support": s.get_support()}
+
+
+def config1(make, iterations=200, seed=0):
+    """PlanarCDI HIO FP64 at 256^2: disk R=40, sigma 2, 1e8 photons, 100x100
+    initial support, reference initialisation, beta 0.9, shrinkwrap every 20
+    (sigma 1.5, threshold 0.1)."""
+    c = synth.planar_case("c1")
+    s = make("planar", 256, 256)
+    s.set_support(c.support)
+    s.set_intensity(c.intensity)
+    s.initialise_estimate(seed)
+    s.set_algorithm(HIO)
+    errs = []
+    for it in range(iterations):
+        s.iterate()
+        errs.append(s.get_error())
+        if it % 20 == 19:
+            s.apply_shrinkwrap(1.5, 0.1)
+    return {"errors": np.array(errs), "esw": s.get_exit_surface_wave(),
+            "support": s.get_support()}
+
+
+def rel_err(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    d = np.abs(a - b).max()
+    m = np.abs(b).max()
+    return d / m if m else d

@@ -1,0 +1,74 @@
+"""The oracle restatement against the reference's own sources compiled here
+(oracle/_ref).  Skipped when the reference was not available to build."""
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+import scenarios as sc
+
+pytestmark = pytest.mark.skipif(not po.reference_available("64"),
+                                reason="oracle/_ref not built")
+
+
+def orc(kind, nx, ny, **kw):
+    return po.Oracle(kind, nx, ny, **kw)
+
+
+def ref(kind, nx, ny, **kw):
+    return po.Reference(kind, nx, ny, variant="64", **kw)
+
+
+def same(a, b):
+    for k in a:
+        if a[k] is None:
+            continue
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
+
+
+# ny < nx is left out: the reference's apply_threshold loops j < nx
+# (NADIA/src/BaseCDI.c++:485) and writes past the end of its array there,
+# which corrupts its heap; the restatement and the CUDA path skip those writes.
+@pytest.mark.parametrize("n,ny", [(64, 64), (40, 56)])
+def test_planar(n, ny):
+    same(sc.planar_mixed(orc, n=n, ny=ny), sc.planar_mixed(ref, n=n, ny=ny))
+
+
+def test_planar_custom():
+    same(sc.planar_custom(orc, n=48), sc.planar_custom(ref, n=48))
+
+
+def test_fresnel():
+    same(sc.fresnel_mixed(orc, n=64), sc.fresnel_mixed(ref, n=64))
+
+
+@pytest.mark.parametrize("n,padding", [(48, 3), (64, 4)])
+def test_poly(n, padding):
+    same(sc.poly_mixed(orc, n=n, padding=padding), sc.poly_mixed(ref, n=n, padding=padding))
+
+
+def test_single_operators():
+    c = sc.planar_inputs(32)
+    a, b = orc("planar", 32, 32), ref("planar", 32, 32)
+    for s in (a, b):
+        s.set_support(c.support)
+        s.set_intensity(c.intensity)
+    g = np.random.default_rng(0)
+    f = g.standard_normal((32, 32)) + 1j * g.standard_normal((32, 32))
+    for op in ("propagate_to_detector", "propagate_from_detector", "scale_intensity",
+               "apply_support", "project_intensity"):
+        assert np.array_equal(getattr(a, op)(f), getattr(b, op)(f)), op
+    assert np.array_equal(a.get_intensity_autocorrelation(), b.get_intensity_autocorrelation())
+
+
+def test_read_spec(tmp_path):
+    p = tmp_path / "spec.txt"
+    p.write_text("Energy\tF.Density\n1200\t1.336e+15\n1208\t1.439e+15\n1216\t2e+15\n")
+    got = po.read_spec(str(p))
+    s = ref("poly", 16, 16)
+    s.L.lib.ref_poly_set_spectrum_file.argtypes = [po._V, po.ctypes.c_char_p]
+    s.L.lib.ref_poly_set_spectrum_file(s.h, str(p).encode())
+    assert got.shape == (3, 2)
+    assert np.float32(got[0, 0]) == np.float32(1.0 / np.float32(1200))
+    assert got[2, 1] == np.float32(2e15)
