@@ -19,7 +19,7 @@ LIB = os.path.join(HERE, "libnadia_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off",
                  "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 PER_FILE = {
     "plain64.cu": ["--fmad=false"],

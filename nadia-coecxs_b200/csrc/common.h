@@ -67,6 +67,15 @@ struct DevBuf {
     explicit operator bool() const { return p != nullptr; }
 };
 
+// Host-to-device copy that has landed when it returns.  A plain cudaMemcpy
+// from pageable memory may return before its DMA completes, and the library's
+// streams do not synchronise with the legacy default stream.
+inline void upload_now(void *dst, const void *src, size_t bytes)
+{
+    NADIA_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    NADIA_CUDA(cudaStreamSynchronize(0));
+}
+
 constexpr int kMaxPasses = 40;
 constexpr int kMaxRadix = 64;
 

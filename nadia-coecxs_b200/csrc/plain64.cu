@@ -575,8 +575,8 @@ void Fft2d::init(int nx_, int ny_)
     std::vector<double2> hx = twiddles(nx), hy = twiddles(ny);
     wx.alloc(nx);
     wy.alloc(ny);
-    NADIA_CUDA(cudaMemcpy(wx.p, hx.data(), wx.bytes(), cudaMemcpyHostToDevice));
-    NADIA_CUDA(cudaMemcpy(wy.p, hy.data(), wy.bytes(), cudaMemcpyHostToDevice));
+    upload_now(wx.p, hx.data(), wx.bytes());
+    upload_now(wy.p, hy.data(), wy.bytes());
     const size_t budget = 128 * 1024;
     rows_per_block = std::max(1, 2048 / ny);
     while (rows_per_block > 1 && 2 * (size_t)rows_per_block * ny * sizeof(double2) > budget)

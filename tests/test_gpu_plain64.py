@@ -178,7 +178,7 @@ def test_errors_are_status_codes():
         p.iterate()
     assert e.value.code == 2
     with pytest.raises(pynadia.NadiaError):
-        p.set_spectrum(np.array([[1.0, 1.0], [2.0, 1.0]]))  # shortest first: negative padding
+        p.set_spectrum(np.array([[1.0, 1.0], [2.0, 3.0]]))  # shortest first: negative padding
     s = gpu("planar", 32, 32, n_best=1)
     assert s.get_best_result(1) == (None, None)
 
