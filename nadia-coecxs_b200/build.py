@@ -7,6 +7,7 @@ with --fmad=false so the FP64 path performs no contracted multiply-adds.  The
 shared library lands next to this file and is what the Python binding and the
 C++ drop-in headers load.
 """
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -47,7 +48,7 @@ def _run(cmd):
 def build(force=False, verbose=False):
     os.makedirs(BUILD, exist_ok=True)
     hdr_time = max(os.path.getmtime(h) for h in headers())
-    objs = []
+    objs, jobs = [], []
     for src in sources():
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src + ".o")
@@ -56,9 +57,11 @@ def build(force=False, verbose=False):
                 and os.path.getmtime(obj) >= hdr_time):
             continue
         lang = [] if src.endswith(".cu") else ["-x", "cu"]
-        out = _run([NVCC, *COMMON, *PER_FILE.get(src, []), *lang, "-c", path, "-o", obj])
-        if verbose and out.strip():
-            print(out)
+        jobs.append([NVCC, *COMMON, *PER_FILE.get(src, []), *lang, "-c", path, "-o", obj])
+    with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
+        for out in pool.map(_run, jobs):
+            if verbose and out.strip():
+                print(out)
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB)
                                                 for o in objs):
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs])

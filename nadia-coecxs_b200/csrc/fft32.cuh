@@ -253,9 +253,22 @@ struct Radices {
 enum { kColMap = 0, kRowMap = 1 };
 constexpr int kPanel = 4; // panel width K
 
-template <int N_, int NT_, int L_, int MAP_, class RL>
+// Shared-memory address swizzle a -> a ^ ((((a >> S1) ^ (a >> S2)) & M) << SH)
+// (S2 = 0: no second term), chosen per tile shape so that every exchange of
+// every pass is free of bank conflicts (checked by simulating the access
+// pattern of each warp).
+template <int S1_, int S2_, int M_, int SH_>
+struct Swizzle {
+    static __host__ __device__ __forceinline__ int apply(int a)
+    {
+        const int t = (a >> S1_) ^ (S2_ ? (a >> S2_) : 0);
+        return a ^ ((t & M_) << SH_);
+    }
+};
+
+template <int N_, int NT_, int L_, int MAP_, class RL, class SW, int MINB_ = 1>
 struct TileCfg {
-    static constexpr int N = N_, NT = NT_, L = L_, MAP = MAP_;
+    static constexpr int N = N_, NT = NT_, L = L_, MAP = MAP_, MINB = MINB_;
     static constexpr int E = N * L / NT;
     static constexpr int P = RL::P;
     using Rad = RL;
@@ -278,13 +291,9 @@ struct TileCfg {
         for (int i = 0; i < p; ++i) s *= radix(i, fwd);
         return s;
     }
-    // shared-memory words (float2) incl. one pad word per 32
-    static constexpr int smem_words() { return N * L + (N * L) / 32 + 1; }
-    static __device__ __forceinline__ int sidx(int s, int pos)
-    {
-        int a = pos * L + s;
-        return a + (a >> 5);
-    }
+    // shared-memory words (float2)
+    static constexpr int smem_words() { return N * L; }
+    static __device__ __forceinline__ int sidx(int s, int pos) { return SW::apply(pos * L + s); }
     // butterfly beta of a pass whose signals hold NR = N/R butterflies
     static __device__ __forceinline__ void map(int beta, int NR, int &s, int &j)
     {
@@ -300,6 +309,13 @@ struct TileCfg {
         }
     }
 };
+
+constexpr int hibit(int r)
+{
+    int h = 1;
+    while (h * 2 <= r) h *= 2;
+    return h;
+}
 
 // twiddle of pass (k, r, N/(Ns*R)): table W[t] = exp(-2 pi i t / N)
 template <bool FWD>
@@ -324,9 +340,26 @@ __device__ __forceinline__ void pass_compute(float2 (&v)[C::E], const float2 *__
         if (Ns > 1) {
             int s, j;
             C::map(threadIdx.x + q * C::NT, NR, s, j);
-            const int k = j % Ns;
+            const int t1 = (j % Ns) * TSTEP;
+            // W^(t1*r) applied as formed: W^t1 is loaded and squared/cubed for
+            // r = 1..3; W^(4a t1) is loaded for each group of four and
+            // multiplied by those (at most two products per twiddle, few
+            // registers live)
+            const float2 w1 = twiddle<FWD>(tw, t1);
+            float2 wb[4];
+            wb[1] = w1;
+            if (R > 2) wb[2] = cmul(w1, w1);
+            if (R > 3) wb[3] = cmul(wb[2], w1);
 #pragma unroll
-            for (int r = 1; r < R; ++r) v[q * R + r] = cmul(v[q * R + r], twiddle<FWD>(tw, k * r * TSTEP));
+            for (int r = 1; r < (R < 4 ? R : 4); ++r) v[q * R + r] = cmul(v[q * R + r], wb[r]);
+#pragma unroll
+            for (int a = 4; a < R; a += 4) {
+                const float2 wa = twiddle<FWD>(tw, t1 * a);
+                v[q * R + a] = cmul(v[q * R + a], wa);
+#pragma unroll
+                for (int b = 1; b < 4; ++b)
+                    if (a + b < R) v[q * R + a + b] = cmul(v[q * R + a + b], cmul(wa, wb[b]));
+            }
         }
         Dft<R, FWD>::run(&v[q * R]);
     }

@@ -26,214 +26,20 @@
 #include "fused32.h"
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <functional>
+#include <tuple>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <vector>
 
-#include "fft32.cuh"
-#include "fused32_impl.h"
+#include "fused32_kernels.cuh"
 #include "solver.h"
 
 namespace nadia {
 namespace f32 {
-
-// ------------------------------------------------------------ tile configs
-
-// Column and row tile shapes per transform length.  K*L >= 16 keeps the row
-// pass's panel segments at 128 bytes or more.
-template <int N> struct Shape;
-template <> struct Shape<256> {
-    using Col = TileCfg<256, 256, 16, kColMap, Radices<16, 16>>;
-    using Row = TileCfg<256, 256, 16, kRowMap, Radices<16, 16>>;
-};
-template <> struct Shape<512> {
-    using Col = TileCfg<512, 256, 8, kColMap, Radices<16, 8, 4>>;
-    using Row = TileCfg<512, 256, 8, kRowMap, Radices<16, 8, 4>>;
-};
-template <> struct Shape<768> {
-    using Col = TileCfg<768, 256, 8, kColMap, Radices<8, 8, 4, 3>>;
-    using Row = TileCfg<768, 256, 8, kRowMap, Radices<8, 8, 4, 3>>;
-};
-template <> struct Shape<1024> {
-    using Col = TileCfg<1024, 256, 4, kColMap, Radices<16, 16, 4>>;
-    using Row = TileCfg<1024, 256, 4, kRowMap, Radices<16, 16, 4>>;
-};
-template <> struct Shape<1536> {
-    using Col = TileCfg<1536, 256, 4, kColMap, Radices<8, 8, 8, 3>>;
-    using Row = TileCfg<1536, 256, 4, kRowMap, Radices<8, 8, 8, 3>>;
-};
-template <> struct Shape<2048> {
-    using Col = TileCfg<2048, 512, 4, kColMap, Radices<16, 16, 8>>;
-    using Row = TileCfg<2048, 512, 4, kRowMap, Radices<16, 16, 8>>;
-};
-template <> struct Shape<4096> {
-    using Col = TileCfg<4096, 1024, 4, kColMap, Radices<16, 16, 16>>;
-    using Row = TileCfg<4096, 1024, 4, kRowMap, Radices<16, 16, 16>>;
-};
-
-__device__ __forceinline__ size_t paddr(int i, int p, int nx)
-{
-    return ((size_t)(p / kPanel) * nx + i) * kPanel + (p % kPanel);
-}
-
-__device__ __forceinline__ float support_factor(float s)
-{
-    return s == 0.f ? 0.f : (s < 1.f ? s : 1.f);
-}
-
-// FP64 block sum; result valid in thread 0
-template <int NT>
-__device__ __forceinline__ double block_sum(double v)
-{
-    __shared__ double red[NT / 32];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    double t = 0;
-    if (threadIdx.x < 32) {
-        t = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.0;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
-    }
-    return t;
-}
-
-// -------------------------------------------------------------- column pass
-
-template <class C, bool FRESNEL>
-__global__ void __launch_bounds__(C::NT) k_col(const Slot *const *slots, int nx, int ny,
-                                               const float2 *__restrict__ tw)
-{
-    extern __shared__ float2 sm[];
-    const Slot &S = *slots[blockIdx.y];
-    float2 *__restrict__ P = S.P;
-    const float *__restrict__ mI = S.mI;
-    const float s0 = S.s0;
-    const int c0 = blockIdx.x * (C::L / kPanel);
-    float2 v[C::E];
-
-    for_each_slot<C, true, true>([&](int e, int s, int pos) {
-        v[e] = P[paddr(pos, c0 * kPanel + s, nx)];
-    });
-    transform<C, true>(v, sm, tw);
-
-    double diff = 0.0;
-    for_each_slot<C, true, false>([&](int e, int s, int kx) {
-        const int ky = c0 * kPanel + s;
-        const size_t a = paddr(kx, ky, nx);
-        const float m = __ldg(&mI[a]);
-        float2 X = v[e];
-        if (!FRESNEL) {
-            if (!(m < 0.f)) {
-                const float a2 = X.x * X.x + X.y * X.y;
-                if (a2 > 0.f) {
-                    const float inv = rsqrtf(a2);
-                    const double d = (double)(a2 * inv * s0) - (double)m;
-                    diff += d * d;
-                    X = cscale(X, m * s0 * inv);
-                } else {
-                    diff += (double)m * (double)m;
-                    X = make_float2(m * s0, 0.f);
-                }
-            } else {
-                X = cscale(X, s0 * s0);
-            }
-        } else {
-            const float2 cf = cmul(__ldg(&S.tx[kx]), __ldg(&S.ty[ky]));
-            const float2 w = S.W[a];
-            float2 u = cadd(cscale(cmul(cf, X), s0), w);
-            if (!(m < 0.f)) {
-                const float a2 = u.x * u.x + u.y * u.y;
-                if (a2 > 0.f) {
-                    const float inv = rsqrtf(a2);
-                    const double d = (double)(a2 * inv) - (double)m;
-                    diff += d * d;
-                    u = cscale(u, m * inv);
-                } else {
-                    diff += (double)m * (double)m;
-                    u = make_float2(m, 0.f);
-                }
-            }
-            X = cscale(cmulc(csub(u, w), cf), s0);
-        }
-        v[e] = X;
-    });
-    const double tot = block_sum<C::NT>(diff);
-    if (threadIdx.x == 0) S.partials[blockIdx.x] = tot;
-
-    transform<C, false>(v, sm, tw);
-    for_each_slot<C, false, false>([&](int e, int s, int pos) {
-        P[paddr(pos, c0 * kPanel + s, nx)] = v[e];
-    });
-}
-
-// ----------------------------------------------------------------- row pass
-
-enum { kRowFull = 0, kRowPrime = 1 };
-
-template <class C, int MODE>
-__global__ void __launch_bounds__(C::NT) k_row(const Slot *const *slots, int nx, int ny,
-                                               const float2 *__restrict__ tw)
-{
-    extern __shared__ float2 sm[];
-    const Slot &S = *slots[blockIdx.y];
-    float2 *__restrict__ P = S.P;
-    float2 *__restrict__ x = S.x;
-    const int i0 = blockIdx.x * C::L;
-    float2 v[C::E];
-
-    if (MODE == kRowFull) {
-        // finish the error metric of the column pass that just ran
-        if (blockIdx.x == 0 && S.project) {
-            double t = 0.0;
-            for (int b = threadIdx.x; b < S.ncol; b += C::NT) t += S.partials[b];
-            t = block_sum<C::NT>(t);
-            if (threadIdx.x == 0) {
-                const double e = t * S.inv_norm2;
-                long long it = *S.iter;
-                *S.err = e;
-                S.ring[it % S.ring_len] = e;
-                *S.iter = it + 1;
-            }
-        } else if (blockIdx.x == 0 && threadIdx.x == 0) {
-            long long it = *S.iter;
-            S.ring[it % S.ring_len] = *S.err;
-            *S.iter = it + 1;
-        }
-        for_each_slot<C, false, true>([&](int e, int s, int pos) {
-            v[e] = P[paddr(i0 + s, pos, nx)];
-        });
-        transform<C, false>(v, sm, tw);
-        const float *__restrict__ sup = S.sup;
-        const float wid = S.w_id, wpf = S.w_pf, wps = S.w_ps, wpsf = S.w_psf;
-        const bool er = S.er;
-        for_each_slot<C, false, false>([&](int e, int s, int pos) {
-            const size_t a = paddr(i0 + s, pos, nx);
-            const float f = support_factor(__ldg(&sup[a]));
-            const float2 y = v[e];
-            float2 xn;
-            if (er) {
-                xn = cscale(y, f);
-            } else {
-                const float2 xk = x[a];
-                xn = make_float2(wid * xk.x + wpf * y.x + wps * (f * xk.x) + wpsf * (f * y.x),
-                                 wid * xk.y + wpf * y.y + wps * (f * xk.y) + wpsf * (f * y.y));
-            }
-            x[a] = xn;
-            v[e] = xn;
-        });
-    } else {
-        for_each_slot<C, true, true>([&](int e, int s, int pos) {
-            v[e] = x[paddr(i0 + s, pos, nx)];
-        });
-    }
-    transform<C, true>(v, sm, tw);
-    for_each_slot<C, true, false>([&](int e, int s, int pos) {
-        P[paddr(i0 + s, pos, nx)] = v[e];
-    });
-}
 
 // ------------------------------------------------------------- shrinkwrap
 
@@ -407,127 +213,6 @@ __global__ void k_scale32(float2 *c, float f, size_t n)
         c[a] = cscale(c[a], f);
 }
 
-// ------------------------------------------------------------ dispatch
-
-template <int N>
-struct Kern {
-    using Col = typename Shape<N>::Col;
-    using Row = typename Shape<N>::Row;
-};
-
-template <class C>
-size_t smem_bytes() { return (size_t)C::smem_words() * sizeof(float2); }
-
-template <class C, class K>
-void set_smem(K kernel)
-{
-    NADIA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem_bytes<C>()));
-}
-
-template <int N>
-void col_prepare_impl()
-{
-    using C = typename Kern<N>::Col;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        set_smem<C>(k_col<C, false>);
-        set_smem<C>(k_col<C, true>);
-    });
-}
-
-template <int N>
-void row_prepare_impl()
-{
-    using C = typename Kern<N>::Row;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        set_smem<C>(k_row<C, kRowFull>);
-        set_smem<C>(k_row<C, kRowPrime>);
-    });
-}
-
-template <int N>
-bool col_launch_impl(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
-                     const float2 *tw, cudaStream_t st)
-{
-    using C = typename Kern<N>::Col;
-    dim3 grid(ny / C::L, nslots);
-    if (fresnel)
-        k_col<C, true><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
-    else
-        k_col<C, false><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
-    return true;
-}
-
-template <int N>
-bool row_launch_impl(int mode, const Slot *const *slots, int nslots, int nx, int ny,
-                     const float2 *tw, cudaStream_t st)
-{
-    using C = typename Kern<N>::Row;
-    dim3 grid(nx / C::L, nslots);
-    if (mode == kRowFull)
-        k_row<C, kRowFull><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
-    else
-        k_row<C, kRowPrime><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
-    return true;
-}
-
-#define NADIA_SIZES(X) X(256) X(512) X(768) X(1024) X(1536) X(2048) X(4096)
-
-bool supported(int n)
-{
-#define X(N) if (n == N) return true;
-    NADIA_SIZES(X)
-#undef X
-    return false;
-}
-
-int col_tile(int n)
-{
-#define X(N) if (n == N) return Kern<N>::Col::L;
-    NADIA_SIZES(X)
-#undef X
-    return 0;
-}
-
-int row_tile(int n)
-{
-#define X(N) if (n == N) return Kern<N>::Row::L;
-    NADIA_SIZES(X)
-#undef X
-    return 0;
-}
-
-// Set the kernels' shared-memory limits (must happen before any stream capture).
-void prepare(int nx, int ny)
-{
-#define X(N) if (nx == N) col_prepare_impl<N>();
-    NADIA_SIZES(X)
-#undef X
-#define X(N) if (ny == N) row_prepare_impl<N>();
-    NADIA_SIZES(X)
-#undef X
-}
-
-void col_launch(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
-                const float2 *tw, cudaStream_t st)
-{
-#define X(N) if (nx == N) { col_launch_impl<N>(fresnel, slots, nslots, nx, ny, tw, st); return; }
-    NADIA_SIZES(X)
-#undef X
-    throw Error(NADIA_ERR_UNSUPPORTED, "FP32 transform length not available");
-}
-
-void row_launch(int mode, const Slot *const *slots, int nslots, int nx, int ny, const float2 *tw,
-                cudaStream_t st)
-{
-#define X(N) if (ny == N) { row_launch_impl<N>(mode, slots, nslots, nx, ny, tw, st); return; }
-    NADIA_SIZES(X)
-#undef X
-    throw Error(NADIA_ERR_UNSUPPORTED, "FP32 transform length not available");
-}
-
 // twiddle tables W[t] = exp(-2 pi i t / N) per device and length
 const float2 *twiddle_table(int n)
 {
@@ -549,6 +234,243 @@ const float2 *twiddle_table(int n)
 }
 
 inline int grid1(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
+
+int sm_count()
+{
+    static int n = [] {
+        int dev = 0, v = 0;
+        NADIA_CUDA(cudaGetDevice(&dev));
+        NADIA_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+        return v;
+    }();
+    return n;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda)
+namespace {
+using EncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                              const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                              const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeFn encode_fn()
+{
+    static EncodeFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        NADIA_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        NADIA_REQUIRE(p && q == cudaDriverEntryPointSuccess, NADIA_ERR_CUDA,
+                      "cuTensorMapEncodeTiled unavailable");
+        return reinterpret_cast<EncodeFn>(p);
+    }();
+    return fn;
+}
+
+// panel-layout array (K, nx, ny/K) of 8- or 4-byte elements, box (K, rows, <=256)
+void encode_one(CUtensorMap *m, void *base, bool complex8, int nx, int ny, int rows)
+{
+    const int npan = ny / kPanel;
+    const cuuint64_t esz = complex8 ? 8 : 4;
+    cuuint64_t dims[3] = {(cuuint64_t)kPanel, (cuuint64_t)nx, (cuuint64_t)npan};
+    cuuint64_t strides[2] = {kPanel * esz, (cuuint64_t)nx * kPanel * esz};
+    cuuint32_t box[3] = {(cuuint32_t)kPanel, (cuuint32_t)rows, (cuuint32_t)box_panels(npan)};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode_fn()(m, complex8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                             3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    NADIA_REQUIRE(r == CUDA_SUCCESS, NADIA_ERR_CUDA,
+                  "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+}
+} // namespace
+
+void encode_tensor_maps(Slot &s, int nx, int ny)
+{
+    const int rows[3] = {4, 8, 16};
+    for (int k = 0; k < 3; ++k) {
+        if (nx % rows[k]) {
+            std::memset(&s.tm[k][0], 0, sizeof(s.tm[k]));
+            continue;
+        }
+        encode_one(&s.tm[k][0], s.P, true, nx, ny, rows[k]);
+        encode_one(&s.tm[k][1], s.x, true, nx, ny, rows[k]);
+        encode_one(&s.tm[k][2], (void *)s.sup, false, nx, ny, rows[k]);
+    }
+}
+
+// ---------------------------------------------------------------- registry
+
+void add_variants_256(std::vector<TileVariant> &);
+void add_variants_512(std::vector<TileVariant> &);
+void add_variants_768(std::vector<TileVariant> &);
+void add_variants_1024(std::vector<TileVariant> &);
+void add_variants_1536(std::vector<TileVariant> &);
+void add_variants_2048(std::vector<TileVariant> &);
+void add_variants_4096(std::vector<TileVariant> &);
+
+const std::vector<TileVariant> &variants(int n)
+{
+    static const std::map<int, std::vector<TileVariant>> reg = [] {
+        std::map<int, std::vector<TileVariant>> m;
+        add_variants_256(m[256]);
+        add_variants_512(m[512]);
+        add_variants_768(m[768]);
+        add_variants_1024(m[1024]);
+        add_variants_1536(m[1536]);
+        add_variants_2048(m[2048]);
+        add_variants_4096(m[4096]);
+        return m;
+    }();
+    static const std::vector<TileVariant> none;
+    auto it = reg.find(n);
+    return it == reg.end() ? none : it->second;
+}
+
+bool supported(int n) { return !variants(n).empty(); }
+
+// ---------------------------------------------------------------- autotuner
+//
+// The first reconstruction of a given grid, kind and batch class times every
+// compiled column variant (transform length nx) and row variant (length ny)
+// on scratch buffers of that shape with CUDA events, and keeps the fastest.
+// The scratch slots hold measured-everywhere data, so the timed work is the
+// full iteration.  NADIA_TUNE=0 in the environment skips the timing and takes
+// the first variant of each length; NADIA_TUNE_VERBOSE=1 prints the timings.
+
+namespace {
+
+struct TuneKey {
+    int dev, nx, ny, fresnel, batch;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(dev, nx, ny, fresnel, batch) < std::tie(o.dev, o.nx, o.ny, o.fresnel, o.batch);
+    }
+};
+
+float time_launches(const std::function<void(cudaStream_t)> &f, cudaStream_t st, int reps)
+{
+    cudaEvent_t a, b;
+    NADIA_CUDA(cudaEventCreate(&a));
+    NADIA_CUDA(cudaEventCreate(&b));
+    f(st);
+    f(st);
+    NADIA_CUDA(cudaEventRecord(a, st));
+    for (int i = 0; i < reps; ++i) f(st);
+    NADIA_CUDA(cudaEventRecord(b, st));
+    NADIA_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    NADIA_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms * 1000.f / reps;
+}
+
+} // namespace
+
+const Choice &choose(int nx, int ny, bool fresnel, int nslots)
+{
+    static std::mutex mu;
+    static std::map<TuneKey, Choice> cache;
+    int dev = 0;
+    NADIA_CUDA(cudaGetDevice(&dev));
+    const int batch = nslots > 1 ? 4 : 1;
+    TuneKey key{dev, nx, ny, fresnel ? 1 : 0, batch};
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+
+    const auto &cv = variants(nx), &rv = variants(ny);
+    NADIA_REQUIRE(!cv.empty() && !rv.empty(), NADIA_ERR_UNSUPPORTED,
+                  "the FP32 form supports 256, 512, 768, 1024, 1536, 2048 and 4096 per axis");
+    for (const auto &v : cv) v.prepare();
+    for (const auto &v : rv) v.prepare();
+    Choice ch;
+    const char *env = getenv("NADIA_TUNE");
+    const bool tune = !(env && env[0] == '0');
+    const bool verbose = getenv("NADIA_TUNE_VERBOSE") != nullptr;
+    // pick the first variant whose tiles divide the grid (and tune among those)
+    std::vector<const TileVariant *> cols, rows;
+    for (const auto &v : cv)
+        if (ny % v.L == 0) cols.push_back(&v);
+    for (const auto &v : rv)
+        if (nx % v.L == 0) rows.push_back(&v);
+    NADIA_REQUIRE(!cols.empty() && !rows.empty(), NADIA_ERR_UNSUPPORTED,
+                  "grid shape does not divide into the FP32 tiles");
+    ch.col = cols[0];
+    ch.row = rows[0];
+    if (tune && (cols.size() > 1 || rows.size() > 1)) {
+        const size_t n = (size_t)nx * ny;
+        const int ns = batch;
+        cudaStream_t st;
+        NADIA_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        std::vector<DevBuf<float2>> P(ns), X(ns);
+        std::vector<DevBuf<float>> sup(ns), mI(ns);
+        DevBuf<float2> W(n), tx(nx), ty(ny);
+        int maxcol = 0;
+        for (auto *v : cols) maxcol = std::max(maxcol, ny / v->L);
+        DevBuf<double> part((size_t)maxcol * ns), err(ns), ring(ns * 4);
+        DevBuf<long long> iter(ns);
+        DevBuf<int> flag(1);
+        NADIA_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+        std::vector<Slot> hs(ns);
+        NADIA_CUDA(cudaMemsetAsync(W.p, 0, W.bytes(), st));
+        NADIA_CUDA(cudaMemsetAsync(tx.p, 0, tx.bytes(), st));
+        NADIA_CUDA(cudaMemsetAsync(ty.p, 0, ty.bytes(), st));
+        NADIA_CUDA(cudaMemsetAsync(iter.p, 0, iter.bytes(), st));
+    NADIA_CUDA(cudaMemsetAsync(flag.p, 0, flag.bytes(), st));
+        for (int i = 0; i < ns; ++i) {
+            P[i].alloc(n); X[i].alloc(n); sup[i].alloc(n); mI[i].alloc(n);
+            NADIA_CUDA(cudaMemsetAsync(P[i].p, 0, P[i].bytes(), st));
+            NADIA_CUDA(cudaMemsetAsync(X[i].p, 0, X[i].bytes(), st));
+            NADIA_CUDA(cudaMemsetAsync(sup[i].p, 0, sup[i].bytes(), st));
+            NADIA_CUDA(cudaMemsetAsync(mI[i].p, 0, mI[i].bytes(), st));
+            Slot &s = hs[i];
+            s = Slot{};
+            s.P = P[i].p; s.x = X[i].p; s.sup = sup[i].p; s.mI = mI[i].p;
+            s.W = fresnel ? W.p : nullptr; s.tx = fresnel ? tx.p : nullptr; s.ty = fresnel ? ty.p : nullptr;
+            s.partials = part.p + (size_t)i * maxcol; s.err = err.p + i; s.ring = ring.p + 4 * i;
+            s.ring_len = 4; s.iter = iter.p + i; s.ncol = 1; s.w_id = 1; s.w_pf = -0.9f;
+            s.w_ps = -1; s.w_psf = 1.9f; s.project = 1; s.s0 = 1.f; s.inv_norm2 = 1.0;
+            s.flag = flag.p;
+            encode_tensor_maps(s, nx, ny);
+        }
+        DevBuf<Slot> dslots(ns);
+        DevBuf<Slot *> dptrs(ns);
+        std::vector<Slot *> hp(ns);
+        for (int i = 0; i < ns; ++i) hp[i] = dslots.p + i;
+        NADIA_CUDA(cudaMemcpyAsync(dslots.p, hs.data(), ns * sizeof(Slot), cudaMemcpyHostToDevice, st));
+        NADIA_CUDA(cudaMemcpyAsync(dptrs.p, hp.data(), ns * sizeof(Slot *), cudaMemcpyHostToDevice, st));
+        NADIA_CUDA(cudaStreamSynchronize(st));
+        const float2 *twx = twiddle_table(nx), *twy = twiddle_table(ny);
+        float best = 1e30f;
+        for (auto *v : cols) {
+            float us = time_launches([&](cudaStream_t s) {
+                v->col(fresnel, dptrs.p, ns, nx, ny, twx, s);
+            }, st, 5);
+            if (verbose)
+                fprintf(stderr, "nadia tune: col n=%d NT=%d L=%d radices=%s%s batch=%d: %.2f us\n",
+                        nx, v->nt, v->L, v->radices, v->persistent ? " persistent" : "", ns, us);
+            if (us < best) { best = us; ch.col = v; ch.col_us = us; }
+        }
+        best = 1e30f;
+        for (auto *v : rows) {
+            float us = time_launches([&](cudaStream_t s) {
+                v->row(kRowFull, dptrs.p, ns, nx, ny, twy, s);
+            }, st, 5);
+            if (verbose)
+                fprintf(stderr, "nadia tune: row n=%d NT=%d L=%d radices=%s%s batch=%d: %.2f us\n",
+                        ny, v->nt, v->L, v->radices, v->persistent ? " persistent" : "", ns, us);
+            if (us < best) { best = us; ch.row = v; ch.row_us = us; }
+        }
+        NADIA_CUDA(cudaGetLastError());
+        NADIA_CUDA(cudaStreamSynchronize(st));
+        int fl = 0;
+        NADIA_CUDA(cudaMemcpy(&fl, flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+        cudaStreamDestroy(st);
+        NADIA_REQUIRE(fl == 0, NADIA_ERR_CUDA, "a device-side wait timed out while tuning");
+    }
+    return cache[key] = ch;
+}
 
 } // namespace f32
 
@@ -576,16 +498,15 @@ Fused32::Impl::Impl(Solver &s) : S(s)
                   "per axis; use NADIA_FP64 for other sizes");
     NADIA_REQUIRE(s.kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
                   "PolyCDI runs in the FP64 form");
-    NADIA_REQUIRE(ny % col_tile(nx) == 0 && nx % row_tile(ny) == 0, NADIA_ERR_UNSUPPORTED,
-                  "grid shape does not divide into the FP32 tiles");
-    prepare(nx, ny);
+    choice = &choose(nx, ny, s.kind == NADIA_FRESNEL, 1);
     P.alloc(n);
     x.alloc(n);
     sup.alloc(n);
     mI.alloc(n);
-    ncol = ny / col_tile(nx);
+    ncol = ny / choice->col->L;
     partials.alloc(ncol);
     iter.alloc(1);
+    flag.alloc(1);
     slot.alloc(1);
     slot_ptr.alloc(1);
     cudaStream_t st = s.st;
@@ -595,6 +516,7 @@ Fused32::Impl::Impl(Solver &s) : S(s)
     NADIA_CUDA(cudaMemsetAsync(mI.p, 0, mI.bytes(), st));
     NADIA_CUDA(cudaMemsetAsync(partials.p, 0, partials.bytes(), st));
     NADIA_CUDA(cudaMemsetAsync(iter.p, 0, iter.bytes(), st));
+    NADIA_CUDA(cudaMemsetAsync(flag.p, 0, flag.bytes(), st));
     twx = twiddle_table(nx);
     twy = twiddle_table(ny);
     h_slot = Slot{};
@@ -610,6 +532,8 @@ Fused32::Impl::Impl(Solver &s) : S(s)
     h_slot.ncol = ncol;
     h_slot.s0 = (float)(1.0 / sqrt((double)nx * (double)ny));
     h_slot.inv_norm2 = 0.0;
+    h_slot.flag = flag.p;
+    encode_tensor_maps(h_slot, nx, ny);
     Slot *sp = slot.p;
     NADIA_CUDA(cudaMemcpyAsync(slot_ptr.p, &sp, sizeof(Slot *), cudaMemcpyHostToDevice, st));
     push_slot();
@@ -890,15 +814,15 @@ void Fused32::Impl::check_algorithm() const
 void Fused32::Impl::prime(cudaStream_t st)
 {
     const Slot *const *sl = slot_ptr.p;
-    row_launch(kRowPrime, sl, 1, nx, ny, twy, st);
+    choice->row->row(kRowPrime, sl, 1, nx, ny, twy, st);
     p_valid = true;
 }
 
 void Fused32::Impl::launch_iteration(cudaStream_t st)
 {
     const Slot *const *sl = slot_ptr.p;
-    col_launch(S.kind == NADIA_FRESNEL, sl, 1, nx, ny, twx, st);
-    row_launch(kRowFull, sl, 1, nx, ny, twy, st);
+    choice->col->col(S.kind == NADIA_FRESNEL, sl, 1, nx, ny, twx, st);
+    choice->row->row(kRowFull, sl, 1, nx, ny, twy, st);
 }
 
 void Fused32::iterate(int count)
@@ -958,6 +882,17 @@ void Fused32::shrinkwrap(double gauss_width, double threshold)
     k_max_final<<<1, 256, 0, I.S.st>>>(I.maxpart.p, gb);
     k_divide<<<gb, 256, 0, I.S.st>>>(I.tmp2.p, I.sup.p, I.n, I.maxpart.p + gb);
     NADIA_CUDA(cudaGetLastError());
+}
+
+void Fused32::check_device_flag()
+{
+    int fl = 0;
+    NADIA_CUDA(cudaMemcpyAsync(&fl, impl->flag.p, sizeof(int), cudaMemcpyDeviceToHost, impl->S.st));
+    NADIA_CUDA(cudaStreamSynchronize(impl->S.st));
+    if (fl) {
+        NADIA_CUDA(cudaMemsetAsync(impl->flag.p, 0, sizeof(int), impl->S.st));
+        throw Error(NADIA_ERR_CUDA, "a device-side wait timed out; the estimate is not valid");
+    }
 }
 
 void Fused32::get_support(double *h)

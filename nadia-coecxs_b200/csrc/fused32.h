@@ -34,6 +34,8 @@ public:
     void get_support(double *h);
     void single_op(int op, double *field);
     void autocorrelation(double *out);
+    // raise NADIA_ERR_CUDA if a device-side wait of this reconstruction gave up
+    void check_device_flag();
 
     struct Impl;
     Impl *impl;

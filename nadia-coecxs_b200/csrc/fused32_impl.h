@@ -2,6 +2,9 @@
 #pragma once
 
 #include <vector>
+#include <string>
+
+#include <cuda.h>
 
 #include "common.h"
 #include "fused32.h"
@@ -14,7 +17,10 @@ namespace f32 {
 
 // One reconstruction as the fused kernels see it.  It lives in device
 // memory, so graphs captured once keep working when the algorithm changes.
-struct Slot {
+struct alignas(64) Slot {
+    // tensor maps over P, x and the support for row tiles of 4, 8 and 16 rows
+    // (persistent row pass); box (K, rows, <= 256 panels)
+    CUtensorMap tm[3][3];
     float2 *P;              // work array (row transforms of x / column-pass output)
     float2 *x;              // estimate
     const float *sup;       // support
@@ -32,6 +38,7 @@ struct Slot {
     int project;            // the algorithm projects (else the error is carried over)
     float s0;               // 1/sqrt(nx*ny)
     double inv_norm2;       // 1 / sum of sqrt(I)^2 over measured pixels
+    int *flag;              // raised when a device-side wait gives up
 };
 
 struct Gauss {
@@ -39,20 +46,54 @@ struct Gauss {
     int cut;
 };
 
+// panels per tensor box: the largest divisor of the panel count that is at
+// most 256 (the TMA box limit), so the boxes tile a row tile exactly
+__host__ __device__ inline int box_panels(int npan)
+{
+    for (int d = npan < 256 ? npan : 256; d > 1; --d)
+        if (npan % d == 0) return d;
+    return 1;
+}
+
 __host__ __device__ inline size_t panel_index_dev(int x, int y, int nx)
 {
     return ((size_t)(y / 4) * nx + x) * 4 + (y % 4);
 }
 
+enum { kRowFull = 0, kRowPrime = 1 };
+
+using ColLaunch = void (*)(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
+                           const float2 *tw, cudaStream_t st);
+using RowLaunch = void (*)(int mode, const Slot *const *slots, int nslots, int nx, int ny,
+                           const float2 *tw, cudaStream_t st);
+
+// One compiled tile shape of a transform length, usable as column pass
+// (length nx) and as row pass (length ny).
+struct TileVariant {
+    int n = 0, nt = 0, L = 0, minb = 0;
+    bool persistent = false;
+    const char *radices = "";
+    void (*prepare)() = nullptr;
+    ColLaunch col = nullptr;
+    RowLaunch row = nullptr;
+};
+
+// the variants of a transform length (empty when the length has none)
+const std::vector<TileVariant> &variants(int n);
 bool supported(int n);
-void prepare(int nx, int ny);
-int col_tile(int n);
-int row_tile(int n);
-void col_launch(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
-                const float2 *tw, cudaStream_t st);
-void row_launch(int mode, const Slot *const *slots, int nslots, int nx, int ny, const float2 *tw,
-                cudaStream_t st);
+
+// The column- and row-pass variants the autotuner picked for a grid, kind and
+// batch class (one reconstruction, or several per launch).
+struct Choice {
+    const TileVariant *col = nullptr, *row = nullptr;
+    float col_us = 0, row_us = 0;
+};
+const Choice &choose(int nx, int ny, bool fresnel, int nslots);
+
 const float2 *twiddle_table(int n);
+int sm_count();
+// tensor maps of a slot's P, x and support (needs P, x, sup set)
+void encode_tensor_maps(Slot &s, int nx, int ny);
 
 } // namespace f32
 
@@ -67,10 +108,12 @@ struct Fused32::Impl {
     DevBuf<float> sup, mI, tmp1, tmp2, maxpart;
     DevBuf<double> partials;
     DevBuf<long long> iter;
+    DevBuf<int> flag;
     DevBuf<f32::Slot> slot;
     DevBuf<f32::Slot *> slot_ptr;
     f32::Slot h_slot{};
     const float2 *twx = nullptr, *twy = nullptr;
+    const f32::Choice *choice = nullptr;
     std::vector<double> h_bs;
     bool p_valid = false;
     cudaGraphExec_t graph_exec = nullptr;

@@ -1,0 +1,314 @@
+// fused32_kernels.cuh -- the column and row passes of the fused FP32
+// iteration, templated on the tile shape (see fused32.cu for the design), and
+// the glue that turns one tile shape into a launchable variant.
+#pragma once
+
+#include "fft32.cuh"
+#include "fused32_impl.h"
+
+namespace nadia {
+namespace f32 {
+
+__device__ __forceinline__ size_t paddr(int i, int p, int nx)
+{
+    return ((size_t)(p / kPanel) * nx + i) * kPanel + (p % kPanel);
+}
+
+__device__ __forceinline__ float support_factor(float s)
+{
+    return s == 0.f ? 0.f : (s < 1.f ? s : 1.f);
+}
+
+// FP64 block sum; result valid in thread 0
+template <int NT>
+__device__ __forceinline__ double block_sum(double v)
+{
+    __shared__ double red[NT / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0;
+    if (threadIdx.x < 32) {
+        t = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+    }
+    return t;
+}
+
+// -------------------------------------------------------------- column pass
+
+template <class C, bool FRESNEL>
+__global__ void __launch_bounds__(C::NT, C::MINB) k_col(const Slot *const *slots, int nx, int ny,
+                                               const float2 *__restrict__ tw)
+{
+    extern __shared__ float2 sm[];
+    const Slot &S = *slots[blockIdx.y];
+    float2 *__restrict__ P = S.P;
+    const float *__restrict__ mI = S.mI;
+    const float s0 = S.s0;
+    const int c0 = blockIdx.x * (C::L / kPanel);
+    float2 v[C::E];
+
+    for_each_slot<C, true, true>([&](int e, int s, int pos) {
+        v[e] = P[paddr(pos, c0 * kPanel + s, nx)];
+    });
+    transform<C, true>(v, sm, tw);
+
+    double diff = 0.0;
+    for_each_slot<C, true, false>([&](int e, int s, int kx) {
+        const int ky = c0 * kPanel + s;
+        const size_t a = paddr(kx, ky, nx);
+        const float m = __ldg(&mI[a]);
+        float2 X = v[e];
+        if (!FRESNEL) {
+            if (!(m < 0.f)) {
+                const float a2 = X.x * X.x + X.y * X.y;
+                if (a2 > 0.f) {
+                    const float inv = rsqrtf(a2);
+                    const double d = (double)(a2 * inv * s0) - (double)m;
+                    diff += d * d;
+                    X = cscale(X, m * s0 * inv);
+                } else {
+                    diff += (double)m * (double)m;
+                    X = make_float2(m * s0, 0.f);
+                }
+            } else {
+                X = cscale(X, s0 * s0);
+            }
+        } else {
+            const float2 cf = cmul(__ldg(&S.tx[kx]), __ldg(&S.ty[ky]));
+            const float2 w = S.W[a];
+            float2 u = cadd(cscale(cmul(cf, X), s0), w);
+            if (!(m < 0.f)) {
+                const float a2 = u.x * u.x + u.y * u.y;
+                if (a2 > 0.f) {
+                    const float inv = rsqrtf(a2);
+                    const double d = (double)(a2 * inv) - (double)m;
+                    diff += d * d;
+                    u = cscale(u, m * inv);
+                } else {
+                    diff += (double)m * (double)m;
+                    u = make_float2(m, 0.f);
+                }
+            }
+            X = cscale(cmulc(csub(u, w), cf), s0);
+        }
+        v[e] = X;
+    });
+    const double tot = block_sum<C::NT>(diff);
+    if (threadIdx.x == 0) S.partials[blockIdx.x] = tot;
+
+    transform<C, false>(v, sm, tw);
+    for_each_slot<C, false, false>([&](int e, int s, int pos) {
+        P[paddr(pos, c0 * kPanel + s, nx)] = v[e];
+    });
+}
+
+// ----------------------------------------------------------------- row pass
+
+
+template <class C, int MODE>
+__global__ void __launch_bounds__(C::NT, C::MINB) k_row(const Slot *const *slots, int nx, int ny,
+                                               const float2 *__restrict__ tw)
+{
+    extern __shared__ float2 sm[];
+    const Slot &S = *slots[blockIdx.y];
+    float2 *__restrict__ P = S.P;
+    float2 *__restrict__ x = S.x;
+    const int i0 = blockIdx.x * C::L;
+    float2 v[C::E];
+
+    if (MODE == kRowFull) {
+        // finish the error metric of the column pass that just ran
+        if (blockIdx.x == 0 && S.project) {
+            double t = 0.0;
+            for (int b = threadIdx.x; b < S.ncol; b += C::NT) t += S.partials[b];
+            t = block_sum<C::NT>(t);
+            if (threadIdx.x == 0) {
+                const double e = t * S.inv_norm2;
+                long long it = *S.iter;
+                *S.err = e;
+                S.ring[it % S.ring_len] = e;
+                *S.iter = it + 1;
+            }
+        } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+            long long it = *S.iter;
+            S.ring[it % S.ring_len] = *S.err;
+            *S.iter = it + 1;
+        }
+        for_each_slot<C, false, true>([&](int e, int s, int pos) {
+            v[e] = P[paddr(i0 + s, pos, nx)];
+        });
+        transform<C, false>(v, sm, tw);
+        const float *__restrict__ sup = S.sup;
+        const float wid = S.w_id, wpf = S.w_pf, wps = S.w_ps, wpsf = S.w_psf;
+        const bool er = S.er;
+        for_each_slot<C, false, false>([&](int e, int s, int pos) {
+            const size_t a = paddr(i0 + s, pos, nx);
+            const float f = support_factor(__ldg(&sup[a]));
+            const float2 y = v[e];
+            float2 xn;
+            if (er) {
+                xn = cscale(y, f);
+            } else {
+                const float2 xk = x[a];
+                xn = make_float2(wid * xk.x + wpf * y.x + wps * (f * xk.x) + wpsf * (f * y.x),
+                                 wid * xk.y + wpf * y.y + wps * (f * xk.y) + wpsf * (f * y.y));
+            }
+            x[a] = xn;
+            v[e] = xn;
+        });
+    } else {
+        for_each_slot<C, true, true>([&](int e, int s, int pos) {
+            v[e] = x[paddr(i0 + s, pos, nx)];
+        });
+    }
+    transform<C, true>(v, sm, tw);
+    for_each_slot<C, true, false>([&](int e, int s, int pos) {
+        P[paddr(i0 + s, pos, nx)] = v[e];
+    });
+}
+
+
+} // namespace f32
+} // namespace nadia
+
+#include "fused32_persist.cuh"
+
+namespace nadia {
+namespace f32 {
+
+// --------------------------------------------------------------- variants
+
+template <class C>
+size_t smem_bytes()
+{
+    return (size_t)C::smem_words() * sizeof(float2);
+}
+
+template <class C, class K>
+void set_smem(K kernel)
+{
+    NADIA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_bytes<C>()));
+}
+
+template <class CC, class CR>
+void prepare_variant()
+{
+    set_smem<CC>(k_col<CC, false>);
+    set_smem<CC>(k_col<CC, true>);
+    set_smem<CR>(k_row<CR, kRowFull>);
+    set_smem<CR>(k_row<CR, kRowPrime>);
+}
+
+template <class C>
+void launch_col(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
+                const float2 *tw, cudaStream_t st)
+{
+    dim3 grid(ny / C::L, nslots);
+    if (fresnel)
+        k_col<C, true><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
+    else
+        k_col<C, false><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
+}
+
+template <class C>
+void launch_row(int mode, const Slot *const *slots, int nslots, int nx, int ny, const float2 *tw,
+                cudaStream_t st)
+{
+    dim3 grid(nx / C::L, nslots);
+    if (mode == kRowFull)
+        k_row<C, kRowFull><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
+    else
+        k_row<C, kRowPrime><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
+}
+
+// shared memory of the persistent passes: two stages of P and sqrt(I)
+// (column); two stages of P plus x and the support (row); and mbarriers
+template <class C>
+constexpr size_t persist_col_smem() { return (size_t)C::N * C::L * 24 + 16; }
+template <class C>
+constexpr size_t persist_row_smem() { return (size_t)C::N * C::L * 28 + 24; }
+
+template <class CC, class CR>
+void prepare_persistent()
+{
+    prepare_variant<CC, CR>();
+    NADIA_CUDA(cudaFuncSetAttribute(kp_col<CC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)persist_col_smem<CC>()));
+    NADIA_CUDA(cudaFuncSetAttribute(kp_col<CC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)persist_col_smem<CC>()));
+    NADIA_CUDA(cudaFuncSetAttribute(kp_row<CR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)persist_row_smem<CR>()));
+}
+
+template <class C>
+void launch_col_persistent(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
+                           const float2 *tw, cudaStream_t st)
+{
+    const int ntiles = (ny / C::L) * nslots;
+    const int grid = ntiles < sm_count() ? ntiles : sm_count();
+    if (fresnel)
+        kp_col<C, true><<<grid, C::NT, persist_col_smem<C>(), st>>>(slots, nslots, nx, ny, tw);
+    else
+        kp_col<C, false><<<grid, C::NT, persist_col_smem<C>(), st>>>(slots, nslots, nx, ny, tw);
+}
+
+template <class C>
+void launch_row_persistent(int mode, const Slot *const *slots, int nslots, int nx, int ny,
+                           const float2 *tw, cudaStream_t st)
+{
+    if (mode != kRowFull) {
+        launch_row<C>(mode, slots, nslots, nx, ny, tw, st);
+        return;
+    }
+    const int ntiles = (nx / C::L) * nslots;
+    const int grid = ntiles < sm_count() ? ntiles : sm_count();
+    kp_row<C><<<grid, C::NT, persist_row_smem<C>(), st>>>(slots, nslots, nx, ny, tw);
+}
+
+// One tile shape (N, NT threads, L signals per block, radices, swizzle, min
+// blocks per SM) as a column-pass and a row-pass variant.
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_variant(const char *radices)
+{
+    using CC = TileCfg<N, NT, L, kColMap, Radices<Rs...>, SW, MINB>;
+    using CR = TileCfg<N, NT, L, kRowMap, Radices<Rs...>, SW, MINB>;
+    TileVariant t;
+    t.n = N;
+    t.nt = NT;
+    t.L = L;
+    t.minb = MINB;
+    t.radices = radices;
+    t.prepare = &prepare_variant<CC, CR>;
+    t.col = &launch_col<CC>;
+    t.row = &launch_row<CR>;
+    return t;
+}
+
+// The same tile shape as persistent, TMA-pipelined passes (tiles of at most
+// 8192 elements, so both stages fit in shared memory).
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_persistent(const char *radices)
+{
+    using CC = TileCfg<N, NT, L, kColMap, Radices<Rs...>, SW, MINB>;
+    using CR = TileCfg<N, NT, L, kRowMap, Radices<Rs...>, SW, MINB>;
+    static_assert(persist_row_smem<CR>() <= 227 * 1024, "persistent row tile too large");
+    TileVariant t;
+    t.n = N;
+    t.nt = NT;
+    t.L = L;
+    t.minb = MINB;
+    t.persistent = true;
+    t.radices = radices;
+    t.prepare = &prepare_persistent<CC, CR>;
+    t.col = &launch_col_persistent<CC>;
+    t.row = &launch_row_persistent<CR>;
+    return t;
+}
+
+} // namespace f32
+} // namespace nadia

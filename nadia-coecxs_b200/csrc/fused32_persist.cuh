@@ -1,0 +1,301 @@
+// fused32_persist.cuh -- persistent, TMA-pipelined forms of the column and
+// row passes.
+//
+// One CTA per SM loops over tiles.  While it transforms tile i, the tensor
+// memory accelerator brings tile i+1 into the other shared-memory stage
+// (cp.async.bulk completing on an mbarrier) and writes tile i-1 back
+// (cp.async.bulk bulk-group stores), so HBM traffic overlaps the arithmetic.
+//
+//   column pass: a tile of L columns is one contiguous run of the panel
+//     layout (N*L elements of P plus N*L of sqrt(I)): two plain bulk copies.
+//   row pass: a tile of L rows is ny/K segments of K*L elements spaced nx*K
+//     apart: a 3-D tensor map (K, nx, ny/K) with box (K, L, <=256) fetches it
+//     in a few tensor copies; x and the support arrive the same way, on their
+//     own barrier, while the inverse row transform runs.
+//
+// Every mbarrier wait is bounded; on a timeout the CTA raises the slot's
+// error flag, waits (bounded) for its copies in flight and leaves.
+#pragma once
+
+#include "tma.cuh"
+
+namespace nadia {
+namespace f32 {
+
+constexpr uint32_t kWaitPolls = 1u << 24;
+
+// raw shared-memory index of element (signal s, position pos) as the bulk
+// copies lay a tile out: column tiles [panel][pos][kk], row tiles [panel][row][kk]
+template <class C>
+__device__ __forceinline__ int raw_col(int s, int pos)
+{
+    return ((s / kPanel) * C::N + pos) * kPanel + (s % kPanel);
+}
+template <class C>
+__device__ __forceinline__ int raw_row(int s, int pos)
+{
+    return ((pos / kPanel) * C::L + s) * kPanel + (pos % kPanel);
+}
+
+__device__ __forceinline__ void raise_flag(const Slot &S)
+{
+    if (S.flag) atomicExch(S.flag, 1);
+}
+
+template <class C, bool FRESNEL>
+__global__ void __launch_bounds__(C::NT, 1)
+    kp_col(const Slot *const *slots, int nslots, int nx, int ny, const float2 *__restrict__ tw)
+{
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    constexpr int TW = C::N * C::L;
+    float2 *Pb0 = reinterpret_cast<float2 *>(smraw);
+    float2 *Pb1 = Pb0 + TW;
+    float *Mb0 = reinterpret_cast<float *>(Pb1 + TW);
+    float *Mb1 = Mb0 + TW;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Mb1 + TW);
+    const int tps = ny / C::L;
+    const int ntiles = tps * nslots;
+
+    if (threadIdx.x == 0) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+
+    auto issue = [&](int tile, int b) {
+        const Slot &S = *slots[tile / tps];
+        const size_t off = (size_t)(tile % tps) * C::L * nx;
+        tma::mbar_arrive_expect_tx(&bar[b], TW * 12);
+        tma::bulk_load(b ? (void *)Pb1 : (void *)Pb0, S.P + off, TW * 8, &bar[b]);
+        tma::bulk_load(b ? (void *)Mb1 : (void *)Mb0, S.mI + off, TW * 4, &bar[b]);
+    };
+    int t = blockIdx.x;
+    if (threadIdx.x == 0 && t < ntiles) issue(t, 0);
+
+    for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
+        const int b = it & 1;
+        float2 *Pb = b ? Pb1 : Pb0;
+        const float *Mb = b ? Mb1 : Mb0;
+        const Slot &S = *slots[t / tps];
+        const int c0 = (t % tps) * (C::L / kPanel);
+        const int tn = t + gridDim.x;
+        if (threadIdx.x == 0 && tn < ntiles) {
+            tma::bulk_wait_read_all();
+            issue(tn, b ^ 1);
+        }
+        const bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, kWaitPolls);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                raise_flag(S);
+                tma::mbar_wait(&bar[b], (it >> 1) & 1, kWaitPolls);
+                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, kWaitPolls);
+            }
+            break;
+        }
+        float2 v[C::E];
+        for_each_slot<C, true, true>([&](int e, int s, int pos) { v[e] = Pb[raw_col<C>(s, pos)]; });
+        __syncthreads();
+        transform<C, true>(v, Pb, tw);
+
+        const float s0 = S.s0;
+        double diff = 0.0;
+        for_each_slot<C, true, false>([&](int e, int s, int kx) {
+            const float m = Mb[raw_col<C>(s, kx)];
+            float2 X = v[e];
+            if (!FRESNEL) {
+                if (!(m < 0.f)) {
+                    const float a2 = X.x * X.x + X.y * X.y;
+                    if (a2 > 0.f) {
+                        const float inv = rsqrtf(a2);
+                        const double d = (double)(a2 * inv * s0) - (double)m;
+                        diff += d * d;
+                        X = cscale(X, m * s0 * inv);
+                    } else {
+                        diff += (double)m * (double)m;
+                        X = make_float2(m * s0, 0.f);
+                    }
+                } else {
+                    X = cscale(X, s0 * s0);
+                }
+            } else {
+                const int ky = c0 * kPanel + s;
+                const float2 cf = cmul(__ldg(&S.tx[kx]), __ldg(&S.ty[ky]));
+                const float2 w = __ldg(&S.W[paddr(kx, ky, nx)]);
+                float2 u = cadd(cscale(cmul(cf, X), s0), w);
+                if (!(m < 0.f)) {
+                    const float a2 = u.x * u.x + u.y * u.y;
+                    if (a2 > 0.f) {
+                        const float inv = rsqrtf(a2);
+                        const double d = (double)(a2 * inv) - (double)m;
+                        diff += d * d;
+                        u = cscale(u, m * inv);
+                    } else {
+                        diff += (double)m * (double)m;
+                        u = make_float2(m, 0.f);
+                    }
+                }
+                X = cscale(cmulc(csub(u, w), cf), s0);
+            }
+            v[e] = X;
+        });
+        const double tot = block_sum<C::NT>(diff);
+        if (threadIdx.x == 0) S.partials[t % tps] = tot;
+
+        transform<C, false>(v, Pb, tw);
+        for_each_slot<C, false, false>([&](int e, int s, int pos) { Pb[raw_col<C>(s, pos)] = v[e]; });
+        tma::fence_async_shared();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tma::bulk_store(S.P + (size_t)(t % tps) * C::L * nx, Pb, TW * 8);
+            tma::bulk_commit();
+        }
+    }
+    if (threadIdx.x == 0) tma::bulk_wait_all();
+}
+
+// finish the error metric of the column pass for one slot (all threads)
+template <int NT>
+__device__ __forceinline__ void finish_error(const Slot &S)
+{
+    if (S.project) {
+        double t = 0.0;
+        for (int b = threadIdx.x; b < S.ncol; b += NT) t += S.partials[b];
+        t = block_sum<NT>(t);
+        if (threadIdx.x == 0) {
+            const double e = t * S.inv_norm2;
+            const long long it = *S.iter;
+            *S.err = e;
+            S.ring[it % S.ring_len] = e;
+            *S.iter = it + 1;
+        }
+    } else if (threadIdx.x == 0) {
+        const long long it = *S.iter;
+        S.ring[it % S.ring_len] = *S.err;
+        *S.iter = it + 1;
+    }
+    __syncthreads();
+}
+
+template <int L>
+__host__ __device__ constexpr int tmap_index()
+{
+    return L == 4 ? 0 : (L == 8 ? 1 : 2);
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::NT, 1)
+    kp_row(const Slot *const *slots, int nslots, int nx, int ny, const float2 *__restrict__ tw)
+{
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    constexpr int TW = C::N * C::L;
+    constexpr int TM = tmap_index<C::L>();
+    float2 *Pb0 = reinterpret_cast<float2 *>(smraw);
+    float2 *Pb1 = Pb0 + TW;
+    float2 *Xb = Pb1 + TW;
+    float *Sb = reinterpret_cast<float *>(Xb + TW);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Sb + TW);
+    const int tps = nx / C::L;
+    const int ntiles = tps * nslots;
+    const int npan = ny / kPanel;
+    const int boxp = box_panels(npan);
+
+    if (threadIdx.x == 0) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::mbar_init(&bar[2], 1);
+        tma::fence_barrier_init();
+    }
+    // slots whose error this CTA finishes (the column pass ran before)
+    for (int sl = blockIdx.x; sl < nslots; sl += gridDim.x) finish_error<C::NT>(*slots[sl]);
+    __syncthreads();
+
+    auto issue_p = [&](int tile, int b) {
+        const Slot &S = *slots[tile / tps];
+        const int i0 = (tile % tps) * C::L;
+        float2 *dst = b ? Pb1 : Pb0;
+        tma::mbar_arrive_expect_tx(&bar[b], TW * 8);
+        for (int c = 0; c < npan; c += boxp)
+            tma::tensor_load_3d(dst + (size_t)c * C::L * kPanel, &S.tm[TM][0], 0, i0, c, &bar[b]);
+    };
+    auto issue_xs = [&](int tile) {
+        const Slot &S = *slots[tile / tps];
+        const int i0 = (tile % tps) * C::L;
+        tma::mbar_arrive_expect_tx(&bar[2], TW * 12);
+        for (int c = 0; c < npan; c += boxp) {
+            tma::tensor_load_3d(Xb + (size_t)c * C::L * kPanel, &S.tm[TM][1], 0, i0, c, &bar[2]);
+            tma::tensor_load_3d(Sb + (size_t)c * C::L * kPanel, &S.tm[TM][2], 0, i0, c, &bar[2]);
+        }
+    };
+    int t = blockIdx.x;
+    if (threadIdx.x == 0 && t < ntiles) issue_p(t, 0);
+
+    for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
+        const int b = it & 1;
+        float2 *Pb = b ? Pb1 : Pb0;
+        const Slot &S = *slots[t / tps];
+        const int i0 = (t % tps) * C::L;
+        const int tn = t + gridDim.x;
+        if (threadIdx.x == 0) {
+            tma::bulk_wait_read_all();
+            issue_xs(t);
+            if (tn < ntiles) issue_p(tn, b ^ 1);
+        }
+        bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, kWaitPolls);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                raise_flag(S);
+                tma::mbar_wait(&bar[b], (it >> 1) & 1, kWaitPolls);
+                tma::mbar_wait(&bar[2], it & 1, kWaitPolls);
+                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, kWaitPolls);
+            }
+            break;
+        }
+        float2 v[C::E];
+        for_each_slot<C, false, true>([&](int e, int s, int pos) { v[e] = Pb[raw_row<C>(s, pos)]; });
+        __syncthreads();
+        transform<C, false>(v, Pb, tw);
+
+        ok = tma::mbar_wait(&bar[2], it & 1, kWaitPolls);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                raise_flag(S);
+                tma::mbar_wait(&bar[2], it & 1, kWaitPolls);
+                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, kWaitPolls);
+            }
+            break;
+        }
+        const float wid = S.w_id, wpf = S.w_pf, wps = S.w_ps, wpsf = S.w_psf;
+        const bool er = S.er;
+        for_each_slot<C, false, false>([&](int e, int s, int pos) {
+            const int a = raw_row<C>(s, pos);
+            const float f = support_factor(Sb[a]);
+            const float2 y = v[e];
+            float2 xn;
+            if (er) {
+                xn = cscale(y, f);
+            } else {
+                const float2 xk = Xb[a];
+                xn = make_float2(wid * xk.x + wpf * y.x + wps * (f * xk.x) + wpsf * (f * y.x),
+                                 wid * xk.y + wpf * y.y + wps * (f * xk.y) + wpsf * (f * y.y));
+            }
+            Xb[a] = xn;
+            v[e] = xn;
+        });
+        transform<C, true>(v, Pb, tw);
+        for_each_slot<C, true, false>([&](int e, int s, int pos) { Pb[raw_row<C>(s, pos)] = v[e]; });
+        tma::fence_async_shared();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int c = 0; c < npan; c += boxp) {
+                tma::tensor_store_3d(&S.tm[TM][0], 0, i0, c, Pb + (size_t)c * C::L * kPanel);
+                tma::tensor_store_3d(&S.tm[TM][1], 0, i0, c, Xb + (size_t)c * C::L * kPanel);
+            }
+            tma::bulk_commit();
+        }
+    }
+    if (threadIdx.x == 0) tma::bulk_wait_all();
+}
+
+} // namespace f32
+} // namespace nadia

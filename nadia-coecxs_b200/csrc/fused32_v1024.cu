@@ -1,0 +1,21 @@
+// fused32_v1024.cu -- the FP32 tile variants of transform length 1024.
+// Swizzles from swizzle_search.py (conflict-free exchanges).
+#include "fused32_kernels.cuh"
+
+namespace nadia {
+namespace f32 {
+
+void add_variants_1024(std::vector<TileVariant> &v)
+{
+    v.push_back(make_variant<1024, 256, 4, 2, Swizzle<4, 6, 3, 2>, 16, 16, 4>("16.16.4"));
+    v.push_back(make_variant<1024, 128, 4, 4, Swizzle<4, 6, 3, 2>, 16, 16, 4>("16.16.4"));
+    v.push_back(make_variant<1024, 512, 4, 2, Swizzle<4, 5, 3, 2>, 8, 8, 4, 4>("8.8.4.4"));
+    v.push_back(make_variant<1024, 512, 8, 1, Swizzle<4, 6, 3, 2>, 16, 16, 4>("16.16.4"));
+    v.push_back(make_persistent<1024, 256, 4, 2, Swizzle<4, 6, 3, 2>, 16, 16, 4>("16.16.4"));
+    v.push_back(make_persistent<1024, 128, 4, 4, Swizzle<4, 6, 3, 2>, 16, 16, 4>("16.16.4"));
+    v.push_back(make_persistent<1024, 512, 4, 2, Swizzle<4, 5, 3, 2>, 8, 8, 4, 4>("8.8.4.4"));
+    v.push_back(make_persistent<1024, 512, 8, 1, Swizzle<4, 6, 3, 2>, 16, 16, 4>("16.16.4"));
+}
+
+} // namespace f32
+} // namespace nadia

@@ -1,0 +1,22 @@
+// fused32_v2048.cu -- the FP32 tile variants of transform length 2048.
+// Swizzles from swizzle_search.py (conflict-free exchanges).
+#include "fused32_kernels.cuh"
+
+namespace nadia {
+namespace f32 {
+
+void add_variants_2048(std::vector<TileVariant> &v)
+{
+    v.push_back(make_variant<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
+    v.push_back(make_variant<2048, 256, 4, 2, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
+    v.push_back(make_variant<2048, 1024, 4, 1, Swizzle<4, 5, 3, 2>, 8, 8, 8, 4>("8.8.8.4"));
+    v.push_back(make_variant<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
+    v.push_back(make_variant<2048, 1024, 8, 1, Swizzle<4, 6, 3, 2>, 16, 16, 8>("16.16.8"));
+    v.push_back(make_persistent<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
+    v.push_back(make_persistent<2048, 256, 4, 2, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
+    v.push_back(make_persistent<2048, 1024, 4, 1, Swizzle<4, 5, 3, 2>, 8, 8, 8, 4>("8.8.8.4"));
+    v.push_back(make_persistent<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
+}
+
+} // namespace f32
+} // namespace nadia

@@ -1,0 +1,19 @@
+// fused32_v512.cu -- the FP32 tile variants of transform length 512.
+// Swizzles from swizzle_search.py (conflict-free exchanges).
+#include "fused32_kernels.cuh"
+
+namespace nadia {
+namespace f32 {
+
+void add_variants_512(std::vector<TileVariant> &v)
+{
+    v.push_back(make_variant<512, 256, 8, 2, Swizzle<4, 6, 3, 2>, 16, 8, 4>("16.8.4"));
+    v.push_back(make_variant<512, 128, 4, 4, Swizzle<4, 6, 3, 2>, 16, 8, 4>("16.8.4"));
+    v.push_back(make_variant<512, 256, 4, 3, Swizzle<4, 0, 7, 1>, 8, 8, 8>("8.8.8"));
+    v.push_back(make_persistent<512, 256, 8, 2, Swizzle<4, 6, 3, 2>, 16, 8, 4>("16.8.4"));
+    v.push_back(make_persistent<512, 128, 4, 4, Swizzle<4, 6, 3, 2>, 16, 8, 4>("16.8.4"));
+    v.push_back(make_persistent<512, 256, 4, 3, Swizzle<4, 0, 7, 1>, 8, 8, 8>("8.8.8"));
+}
+
+} // namespace f32
+} // namespace nadia

@@ -1,0 +1,19 @@
+// fused32_v768.cu -- the FP32 tile variants of transform length 768.
+// Swizzles from swizzle_search.py (conflict-free exchanges).
+#include "fused32_kernels.cuh"
+
+namespace nadia {
+namespace f32 {
+
+void add_variants_768(std::vector<TileVariant> &v)
+{
+    v.push_back(make_variant<768, 256, 8, 2, Swizzle<4, 6, 3, 2>, 8, 8, 4, 3>("8.8.4.3"));
+    v.push_back(make_variant<768, 128, 4, 4, Swizzle<4, 0, 7, 1>, 8, 8, 4, 3>("8.8.4.3"));
+    v.push_back(make_variant<768, 256, 4, 2, Swizzle<4, 6, 3, 2>, 4, 4, 4, 4, 3>("4.4.4.4.3"));
+    v.push_back(make_persistent<768, 256, 8, 2, Swizzle<4, 6, 3, 2>, 8, 8, 4, 3>("8.8.4.3"));
+    v.push_back(make_persistent<768, 128, 4, 4, Swizzle<4, 0, 7, 1>, 8, 8, 4, 3>("8.8.4.3"));
+    v.push_back(make_persistent<768, 256, 4, 2, Swizzle<4, 6, 3, 2>, 4, 4, 4, 4, 3>("4.4.4.4.3"));
+}
+
+} // namespace f32
+} // namespace nadia

@@ -93,7 +93,11 @@ Solver::~Solver()
     }
 }
 
-void Solver::sync() { NADIA_CUDA(cudaStreamSynchronize(st)); }
+void Solver::sync()
+{
+    NADIA_CUDA(cudaStreamSynchronize(st));
+    if (f32) f32->check_device_flag();
+}
 
 // ------------------------------------------------------------------ inputs
 
@@ -622,6 +626,7 @@ double Solver::get_error()
 {
     double e = 0;
     d2h(&e, d_err.p, sizeof(double), st);
+    if (f32) f32->check_device_flag();
     return e;
 }
 
