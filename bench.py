@@ -1,0 +1,413 @@
+#!/usr/bin/env python
+"""Benchmark: PlanarCDI HIO reconstructions per second at 2048^2.
+
+Workload (one "step"): a batch of B PlanarCDI reconstructions at 2048x2048,
+each 1000 HIO iterations (beta 0.9) with shrinkwrap every 50 (sigma 1.5,
+threshold 0.1), on the synthetic disk object (radius 320 px, phase smoothing
+sigma 4, 1e9 photons with Poisson noise, central 8x8 beam stop unmeasured),
+run in the fused FP32 form (complex FP32 transforms and projections, FP64
+error and support reductions) through nadia_iterate_many.  The batch's
+working set (~0.8 GB for B=8) is larger than the 126 MB L2, so no flush is
+needed between steps.
+
+  value  -- reconstructions/s with the inputs resident on the device, timed
+            with CUDA events on the library's launching stream, max over ranks
+  e2e    -- the same through the C ABI with host buffers: per step every
+            reconstruction uploads its intensity, support and beam stop,
+            initialises, runs and downloads its estimate and error metric
+  roofline -- the dominant fused pass (column or row) timed alone with events;
+            algorithmic bytes per pixel: column 20, row 36 (FP32 HIO)
+  cpu_baseline -- the reference's own C++ (float build, -O3 -ffast-math, FFTs
+            through the project's FFTW-API shim since FFTW is not installed)
+            on a bounded sample of the same workload on the host cores
+
+`--impl reference` times that reference CPU code alone (all host cores).
+Multi-GPU: independent replicas, one batch per rank (weak scaling).
+"""
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "nadia-coecxs_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+sys.path.insert(0, PKG)
+
+METRIC = "HIO recon/s and p50/p99 latency at 2048^2, FP32 batched vs FP64 plain, same error"
+N = 2048
+ITERS = 1000
+SW_EVERY = 50
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--batch", type=int, default=8)
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return p.parse_args()
+
+
+# --------------------------------------------------------------- CPU side
+
+def _cpu_worker(args):
+    """One reference-code reconstruction stream on one core: time `iters`
+    HIO iterations at 2048^2 (plus one shrinkwrap), return seconds/iteration
+    and seconds/shrinkwrap."""
+    libkind, iters = args
+    sys.path[:0] = [ORACLE, PKG]
+    import numpy as np
+    import pyoracle as po
+    from pynadia import synth
+    c = synth.planar_case("c3")
+    if libkind == "reference":
+        s = po.Reference("planar", N, N, variant="32_fast")
+    else:
+        s = po.Oracle("planar", N, N)
+    s.set_support(c.support)
+    s.set_intensity(c.intensity)
+    s.set_beam_stop(c.beam_stop)
+    s.initialise_estimate(0)
+    s.set_algorithm(3)
+    s.iterate(1)
+    t = time.perf_counter()
+    s.iterate(iters)
+    t_it = (time.perf_counter() - t) / iters
+    t = time.perf_counter()
+    s.apply_shrinkwrap(1.5, 0.1)
+    t_sw = time.perf_counter() - t
+    return t_it, t_sw
+
+
+def cpu_kind():
+    sys.path.insert(0, ORACLE)
+    import pyoracle as po
+    if po.reference_available("32_fast"):
+        return "reference"
+    return "port"
+
+
+def cpu_sample(procs, iters):
+    """Reconstructions/s of the reference CPU code on `procs` cores."""
+    kind = cpu_kind()
+    if kind == "port":
+        sys.path.insert(0, ORACLE)
+        import pyoracle as po
+        po.oracle_lib()  # builds oracle/liboracle.so if needed
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_cpu_worker, [(kind, iters)] * procs)
+    wall = time.perf_counter() - t0
+    per_recon = [t_it * ITERS + t_sw * (ITERS // SW_EVERY) for t_it, t_sw in res]
+    value = sum(1.0 / s for s in per_recon)
+    desc = ("%d independent %dx%d HIO streams, %d timed iterations + 1 shrinkwrap each, "
+            "extrapolated to %d iterations with shrinkwrap every %d; %s"
+            % (procs, N, N, iters, ITERS, SW_EVERY,
+               "reference C++ float build (-O3 -ffast-math) + project FFTW-API shim "
+               "(FFTW unavailable)" if kind == "reference" else "oracle restatement (FP64)"))
+    return {"value": value, "unit": "recon/s", "cores": procs, "kind": kind, "sample": desc,
+            "s_per_iteration": sum(r[0] for r in res) / len(res), "wall_s": wall}
+
+
+# --------------------------------------------------------------- GPU side
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def make_solvers(pynadia, case, batch, precision):
+    out = []
+    for _ in range(batch):
+        s = pynadia.Solver("planar", N, N, precision=precision)
+        s.set_support(case.support)
+        s.set_intensity(case.intensity)
+        s.set_beam_stop(case.beam_stop)
+        s.initialise_estimate(0)
+        s.set_algorithm("HIO")
+        out.append(s)
+    return out
+
+
+def run_program(pynadia, solvers):
+    """1000 HIO iterations with shrinkwrap every 50, all queued asynchronously."""
+    for _ in range(ITERS // SW_EVERY):
+        pynadia.iterate_many(solvers, SW_EVERY)
+        for s in solvers:
+            s.apply_shrinkwrap(1.5, 0.1)
+
+
+def phase_aligned_error(x, ref):
+    import numpy as np
+    inner = np.vdot(x, ref)
+    phi = np.angle(inner)
+    return float(np.linalg.norm(x * np.exp(1j * phi) - ref) / np.linalg.norm(ref))
+
+
+def ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import pynadia
+    from pynadia import synth
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    case = synth.planar_case("c3")
+    B = args.batch
+    solvers = make_solvers(pynadia, case, B, pynadia.FP32)
+    stream = torch.cuda.ExternalStream(solvers[0].stream())
+    member_streams = [torch.cuda.ExternalStream(s.stream()) for s in solvers[1:]]
+
+    def step():
+        run_program(pynadia, solvers)
+        for ms in member_streams:
+            stream.wait_stream(ms)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    for s in solvers:
+        s.synchronize()
+
+    # ---- timed: device-resident value
+    if dist:
+        dist.barrier()
+    l0 = pynadia.launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with Clocks(local_rank) as clk:
+        for a, b in ev:
+            a.record(stream)
+            step()
+            b.record(stream)
+        torch.cuda.synchronize()
+        for s in solvers:
+            s.synchronize()
+    launches = pynadia.launch_count() - l0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    tot_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([tot_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+        dist.barrier()
+    value = world * B * args.steps / (tot_ms / 1000.0)
+    clocks = clk.summary()
+
+    # ---- e2e through the C ABI with host buffers
+    e2e_times = []
+    esw = np.empty((N, N), np.complex128)
+    intensity, support, beam = case.intensity, case.support, case.beam_stop
+    h2d = B * N * N * (4 + 4 + 4 + 8)   # sqrt(I), beam mask folded, support, estimate (FP32)
+    d2h = B * (N * N * 8 + 8)            # estimate (FP32) + error metric
+    for k in range(args.steps):
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for s in solvers:
+            s.set_intensity(intensity)
+            s.set_beam_stop(beam)
+            s.set_support(support)
+            s.initialise_estimate(k)
+        run_program(pynadia, solvers)
+        errs = []
+        for s in solvers:
+            out = s.get_exit_surface_wave_f32()
+            errs.append(s.get_error())
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = sum(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * B * args.steps / e2e_s, "unit": "recon/s",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+
+    line = None
+    if rank == 0:
+        # ---- roofline of the dominant pass (timed alone with events)
+        col_us, row_us = pynadia.pass_times(solvers, reps=10)
+        px = B * N * N
+        passes = {"column": (col_us, 20 * px), "row": (row_us, 36 * px)}
+        dom = max(passes, key=lambda k: passes[k][0])
+        us, nbytes = passes[dom]
+        peak, peak_kind = measured_peak()
+        achieved = nbytes / (us * 1e-6) / 1e9
+        tr = traffic_per_launch()
+        traffic = None
+        if tr and dom in tr:
+            traffic = tr[dom]["bytes_per_pixel"] * px
+        roofline = {"bound": "hbm", "kernel": dom + " pass", "achieved": achieved,
+                    "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": traffic,
+                    "algorithmic_bytes_per_launch": nbytes,
+                    "pass_us": {"column": col_us, "row": row_us}}
+
+        # ---- FP64 plain form and "same error" check on one reconstruction:
+        # the same inputs, initial estimate and program in both forms
+        a = make_solvers(pynadia, case, 1, pynadia.FP64)[0]
+        b = make_solvers(pynadia, case, 1, pynadia.FP32)[0]
+        run_program(pynadia, [b])
+        b.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ITERS // SW_EVERY):
+            a.iterate(SW_EVERY)
+            a.apply_shrinkwrap(1.5, 0.1)
+        a.synchronize()
+        t64 = time.perf_counter() - t0
+        e64, e32 = a.get_error(), b.get_error()
+        x64, x32 = a.get_exit_surface_wave(), b.get_exit_surface_wave()
+        accuracy = {"fp64_final_error": e64, "fp32_final_error": e32,
+                    "final_error_rel_diff": abs(e32 - e64) / abs(e64),
+                    "phase_aligned_rel_error": phase_aligned_error(x32, x64)}
+        fp64 = {"recon_per_s": 1.0 / t64, "ms_per_iteration": 1000.0 * t64 / ITERS,
+                "ratio_fp32_batched_over_fp64": value / world / (1.0 / t64),
+                "note": "FP64 plain form, one reconstruction, same program, host wall clock"}
+
+        cpu = None
+        if not args.no_cpu:
+            procs = max(1, min(os.cpu_count() or 1, 8))
+            cpu = cpu_sample(procs, iters=2)
+        step_ms_sorted = sorted(step_ms)
+        line = {
+            "metric": METRIC, "value": value, "unit": "recon/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic: seeded disk object, 1e9 photons Poisson, 8x8 beam stop",
+            "config": {"workload": "PlanarCDI HIO 2048x2048, 1000 iterations, shrinkwrap every 50 "
+                                   "(sigma 1.5, t 0.1), batch of %d per GPU" % B,
+                       "batch_per_gpu": B, "grid": [N, N], "iterations": ITERS,
+                       "shrinkwrap_every": SW_EVERY, "precision_form": "FP32 fused",
+                       "l2": "working set %.2f GB > 126 MB L2, no flush" % (B * N * N * 24 / 1e9),
+                       "parallelism": "replicas x%d" % world},
+            "latency_ms": {"p50": step_ms_sorted[len(step_ms) // 2],
+                           "p99": step_ms_sorted[min(len(step_ms) - 1,
+                                                     int(math.ceil(0.99 * len(step_ms))) - 1)],
+                           "note": "per reconstruction in a batch = its batch's step time"},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": launches, "fp64_plain": fp64, "accuracy": accuracy,
+        }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def reference(args, rank, world):
+    if rank != 0:
+        return None
+    procs = max(1, os.cpu_count() or 1)
+    vals = []
+    info = None
+    for _ in range(args.warmup):
+        cpu_sample(procs, iters=1)
+    for _ in range(args.steps):
+        info = cpu_sample(procs, iters=1)
+        vals.append(info["value"])
+    value = sum(vals) / len(vals)
+    info["value"] = value
+    return {"metric": METRIC, "value": value, "unit": "recon/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * info["wall_s"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic: seeded disk object, 1e9 photons Poisson, 8x8 beam stop",
+            "config": {"workload": "PlanarCDI HIO 2048x2048, 1000 iterations, shrinkwrap every 50",
+                       "grid": [N, N], "iterations": ITERS, "shrinkwrap_every": SW_EVERY},
+            "impl": "reference", "cpu_baseline": info,
+            "e2e": {"value": value, "unit": "recon/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = reference(args, rank, world)
+    else:
+        line = ours(args, rank, world, local_rank)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

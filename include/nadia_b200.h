@@ -219,6 +219,23 @@ int nadia_synchronize(nadia_solver *s);
  * counterpart in the reference, which runs one reconstruction per process. */
 int nadia_iterate_many(nadia_solver *const *solvers, int count, int iterations);
 
+/* ---- diagnostics (no counterpart in the reference) ----------------------- */
+
+/* The CUDA stream (cudaStream_t) a handle's device work is queued on, so a
+ * caller can time it with events on that stream.  nadia_iterate_many queues
+ * on the stream of its first handle. */
+int nadia_get_stream(nadia_solver *s, void **stream);
+
+/* Mean device time in microseconds of one column pass and one row pass of
+ * the fused FP32 iteration for `count` handles of one size and geometry run
+ * as a batch (CUDA events around `reps` launches of each pass).  The passes
+ * run for real: each handle advances by 1 + reps iterations. */
+int nadia_pass_times(nadia_solver *const *solvers, int count, int reps, double out_us[2]);
+
+/* Kernels this library has launched in this process (graph replays count
+ * every kernel they contain). */
+long long nadia_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

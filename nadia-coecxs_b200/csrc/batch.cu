@@ -1,0 +1,251 @@
+// batch.cu -- several reconstructions stepped together (nadia_iterate_many).
+//
+// FP32 handles are grouped by grid size and geometry.  Each group runs one
+// launch per pass for all of its members (gridDim.y = members), the groups
+// run concurrently on forked streams, and a whole block of iterations is
+// captured once as a CUDA graph and replayed.  Handles the fused form cannot
+// batch (FP64, PolyCDI, n-best bookkeeping, algorithms with a PfPs term) are
+// stepped one by one on their own streams.
+#include <algorithm>
+#include <atomic>
+#include <list>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "batch.h"
+#include "fused32.h"
+#include "fused32_impl.h"
+#include "solver.h"
+
+namespace nadia {
+
+std::atomic<long long> g_launches{0};
+
+namespace {
+
+constexpr int kGraphIters = 16;
+constexpr size_t kMaxPlans = 8;
+
+struct Group {
+    int nx = 0, ny = 0;
+    bool fresnel = false;
+    const f32::Choice *choice = nullptr;
+    std::vector<Solver *> members;
+    DevBuf<f32::Slot *> ptrs;
+    const float2 *twx = nullptr, *twy = nullptr;
+    cudaStream_t st = nullptr; // side stream (null for the first group)
+};
+
+struct Plan {
+    std::vector<unsigned long long> key;
+    std::vector<Group> groups;
+    cudaStream_t st = nullptr;               // batch stream (first member's)
+    std::vector<cudaEvent_t> fork, join;     // per side stream
+    cudaGraphExec_t exec = nullptr;
+    ~Plan()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (auto &g : groups)
+            if (g.st) cudaStreamDestroy(g.st);
+        for (auto e : fork) cudaEventDestroy(e);
+        for (auto e : join) cudaEventDestroy(e);
+    }
+
+    void launch_block(int iters)
+    {
+        // fork side streams off the batch stream
+        for (size_t i = 1; i < groups.size(); ++i) {
+            NADIA_CUDA(cudaEventRecord(fork[i], st));
+            NADIA_CUDA(cudaStreamWaitEvent(groups[i].st, fork[i], 0));
+        }
+        for (auto &g : groups) {
+            cudaStream_t s = g.st ? g.st : st;
+            const int n = (int)g.members.size();
+            for (int it = 0; it < iters; ++it) {
+                g.choice->col->col(g.fresnel, g.ptrs.p, n, g.nx, g.ny, g.twx, s);
+                g.choice->row->row(f32::kRowFull, g.ptrs.p, n, g.nx, g.ny, g.twy, s);
+            }
+        }
+        for (size_t i = 1; i < groups.size(); ++i) {
+            NADIA_CUDA(cudaEventRecord(join[i], groups[i].st));
+            NADIA_CUDA(cudaStreamWaitEvent(st, join[i], 0));
+        }
+    }
+};
+
+std::mutex g_mu;
+std::list<std::unique_ptr<Plan>> g_plans; // most recently used first
+
+bool batchable(const Solver &s)
+{
+    return s.prec == NADIA_FP32 && s.kind != NADIA_POLY && s.n_best == 0 &&
+           (s.algorithm == NADIA_ER || s.w[PFS] == 0);
+}
+
+} // namespace
+
+void iterate_many(Solver *const *solvers, int count, int iterations)
+{
+    NADIA_REQUIRE(count >= 0 && iterations >= 0, NADIA_ERR_INVALID, "negative count");
+    std::vector<Solver *> fused, other;
+    for (int i = 0; i < count; ++i) {
+        NADIA_REQUIRE(solvers[i] != nullptr, NADIA_ERR_INVALID, "null handle in batch");
+        for (int j = 0; j < i; ++j)
+            NADIA_REQUIRE(solvers[j] != solvers[i], NADIA_ERR_INVALID, "handle listed twice");
+        (batchable(*solvers[i]) ? fused : other).push_back(solvers[i]);
+    }
+    for (Solver *s : other) s->iterate(iterations);
+    if (fused.empty() || iterations == 0) return;
+
+    std::lock_guard<std::mutex> lock(g_mu);
+    std::vector<unsigned long long> key;
+    for (Solver *s : fused) key.push_back(s->uid);
+    Plan *plan = nullptr;
+    for (auto it = g_plans.begin(); it != g_plans.end(); ++it)
+        if ((*it)->key == key) {
+            g_plans.splice(g_plans.begin(), g_plans, it);
+            plan = g_plans.front().get();
+            break;
+        }
+    if (!plan) {
+        std::unique_ptr<Plan> p(new Plan);
+        p->key = key;
+        p->st = fused[0]->st;
+        std::map<std::tuple<int, int, int>, size_t> index;
+        for (Solver *s : fused) {
+            auto k = std::make_tuple(s->nx, s->ny, s->kind == NADIA_FRESNEL ? 1 : 0);
+            auto f = index.find(k);
+            if (f == index.end()) {
+                index[k] = p->groups.size();
+                p->groups.emplace_back();
+                Group &g = p->groups.back();
+                g.nx = s->nx;
+                g.ny = s->ny;
+                g.fresnel = s->kind == NADIA_FRESNEL;
+                g.members.push_back(s);
+            } else {
+                p->groups[f->second].members.push_back(s);
+            }
+        }
+        p->fork.resize(p->groups.size(), nullptr);
+        p->join.resize(p->groups.size(), nullptr);
+        for (size_t i = 0; i < p->groups.size(); ++i) {
+            Group &g = p->groups[i];
+            g.choice = &f32::choose(g.nx, g.ny, g.fresnel, (int)g.members.size());
+            g.twx = f32::twiddle_table(g.nx);
+            g.twy = f32::twiddle_table(g.ny);
+            std::vector<f32::Slot *> hp;
+            for (Solver *s : g.members) hp.push_back(s->f32->impl->slot.p);
+            g.ptrs.alloc(hp.size());
+            NADIA_CUDA(cudaMemcpyAsync(g.ptrs.p, hp.data(), hp.size() * sizeof(f32::Slot *),
+                                       cudaMemcpyHostToDevice, p->st));
+            if (i > 0) {
+                NADIA_CUDA(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+                NADIA_CUDA(cudaEventCreateWithFlags(&p->fork[i], cudaEventDisableTiming));
+                NADIA_CUDA(cudaEventCreateWithFlags(&p->join[i], cudaEventDisableTiming));
+            }
+        }
+        NADIA_CUDA(cudaStreamSynchronize(p->st));
+        g_plans.emplace_front(std::move(p));
+        while (g_plans.size() > kMaxPlans) g_plans.pop_back();
+        plan = g_plans.front().get();
+    }
+
+    // order the batch after each member's queued work; set the members'
+    // descriptors for the variants this batch uses; prime stale work arrays
+    cudaEvent_t ev;
+    NADIA_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    for (Solver *s : fused) {
+        if (s->st == plan->st) continue;
+        NADIA_CUDA(cudaEventRecord(ev, s->st));
+        NADIA_CUDA(cudaStreamWaitEvent(plan->st, ev, 0));
+    }
+    for (auto &g : plan->groups)
+        for (Solver *s : g.members) {
+            Fused32::Impl &I = *s->f32->impl;
+            I.check_algorithm();
+            I.use_choice(g.choice);
+            I.push_slot_async(plan->st);
+            if (!I.p_valid) I.prime(plan->st);
+        }
+    int left = iterations;
+    if (left >= kGraphIters) {
+        if (!plan->exec) {
+            cudaGraph_t graph = nullptr;
+            NADIA_CUDA(cudaStreamBeginCapture(plan->st, cudaStreamCaptureModeThreadLocal));
+            plan->launch_block(kGraphIters);
+            NADIA_CUDA(cudaStreamEndCapture(plan->st, &graph));
+            NADIA_CUDA(cudaGraphInstantiate(&plan->exec, graph, 0));
+            cudaGraphDestroy(graph);
+        }
+        while (left >= kGraphIters) {
+            NADIA_CUDA(cudaGraphLaunch(plan->exec, plan->st));
+            g_launches += 2LL * kGraphIters * (long long)plan->groups.size();
+            left -= kGraphIters;
+        }
+    }
+    if (left > 0) {
+        plan->launch_block(left);
+        g_launches += 2LL * left * (long long)plan->groups.size();
+    }
+    NADIA_CUDA(cudaGetLastError());
+    NADIA_CUDA(cudaEventRecord(ev, plan->st));
+    for (Solver *s : fused) {
+        s->iters += iterations;
+        if (s->st != plan->st) NADIA_CUDA(cudaStreamWaitEvent(s->st, ev, 0));
+    }
+    NADIA_CUDA(cudaEventDestroy(ev));
+}
+
+// Device time of one column pass and one row pass (microseconds, mean of
+// `reps` launches with CUDA events on the launching stream) for the batch.
+void pass_times(Solver *const *solvers, int count, int reps, double out_us[2])
+{
+    NADIA_REQUIRE(count >= 1 && reps >= 1, NADIA_ERR_INVALID, "bad count");
+    for (int i = 0; i < count; ++i)
+        NADIA_REQUIRE(batchable(*solvers[i]) && solvers[i]->nx == solvers[0]->nx &&
+                          solvers[i]->ny == solvers[0]->ny && solvers[i]->kind == solvers[0]->kind,
+                      NADIA_ERR_INVALID, "pass timing needs FP32 handles of one size and kind");
+    // run one iteration through the batch path so the plan and graph exist
+    iterate_many(solvers, count, 1);
+    Plan *plan = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        plan = g_plans.front().get();
+    }
+    Group &g = plan->groups[0];
+    cudaStream_t st = plan->st;
+    const int n = (int)g.members.size();
+    cudaEvent_t e[3];
+    for (auto &x : e) NADIA_CUDA(cudaEventCreate(&x));
+    float col = 0, row = 0;
+    for (int r = 0; r < reps; ++r) {
+        NADIA_CUDA(cudaEventRecord(e[0], st));
+        g.choice->col->col(g.fresnel, g.ptrs.p, n, g.nx, g.ny, g.twx, st);
+        NADIA_CUDA(cudaEventRecord(e[1], st));
+        g.choice->row->row(f32::kRowFull, g.ptrs.p, n, g.nx, g.ny, g.twy, st);
+        NADIA_CUDA(cudaEventRecord(e[2], st));
+        NADIA_CUDA(cudaEventSynchronize(e[2]));
+        float a = 0, b = 0;
+        NADIA_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
+        NADIA_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
+        col += a;
+        row += b;
+    }
+    for (auto &x : e) cudaEventDestroy(x);
+    for (Solver *s : g.members) s->iters += reps;
+    out_us[0] = 1000.0 * col / reps;
+    out_us[1] = 1000.0 * row / reps;
+}
+
+void forget_batches_with(unsigned long long uid)
+{
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_plans.remove_if([&](const std::unique_ptr<Plan> &p) {
+        return std::find(p->key.begin(), p->key.end(), uid) != p->key.end();
+    });
+}
+
+} // namespace nadia

@@ -4,7 +4,9 @@
 #include <functional>
 #include <new>
 #include <string>
+#include <vector>
 
+#include "batch.h"
 #include "fused32.h"
 #include "solver.h"
 
@@ -332,6 +334,29 @@ extern "C" int nadia_iterate_many(nadia_solver *const *solvers, int count, int i
 {
     return guard([&] {
         need(solvers, "solvers");
-        for (int i = 0; i < count; ++i) S(solvers[i]).iterate(iterations);
+        std::vector<Solver *> v;
+        for (int i = 0; i < count; ++i) v.push_back(&S(solvers[i]));
+        nadia::iterate_many(v.data(), count, iterations);
     });
 }
+
+extern "C" int nadia_get_stream(nadia_solver *h, void **stream)
+{
+    return guard([&] {
+        need(stream, "stream");
+        *stream = (void *)S(h).st;
+    });
+}
+
+extern "C" int nadia_pass_times(nadia_solver *const *solvers, int count, int reps, double out_us[2])
+{
+    return guard([&] {
+        need(solvers, "solvers");
+        need(out_us, "out_us");
+        std::vector<Solver *> v;
+        for (int i = 0; i < count; ++i) v.push_back(&S(solvers[i]));
+        nadia::pass_times(v.data(), count, reps, out_us);
+    });
+}
+
+extern "C" long long nadia_launch_count(void) { return nadia::g_launches.load(); }

@@ -35,6 +35,7 @@
 #include <mutex>
 #include <vector>
 
+#include "batch.h"
 #include "fused32_kernels.cuh"
 #include "solver.h"
 
@@ -504,7 +505,7 @@ Fused32::Impl::Impl(Solver &s) : S(s)
     sup.alloc(n);
     mI.alloc(n);
     ncol = ny / choice->col->L;
-    partials.alloc(ncol);
+    partials.alloc(ny / kPanel);
     iter.alloc(1);
     flag.alloc(1);
     slot.alloc(1);
@@ -544,7 +545,18 @@ Fused32::Impl::~Impl()
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
 }
 
+void Fused32::Impl::use_choice(const f32::Choice *c)
+{
+    h_slot.ncol = ny / c->col->L;
+}
+
 void Fused32::Impl::push_slot()
+{
+    push_slot_async(S.st);
+    NADIA_CUDA(cudaStreamSynchronize(S.st));
+}
+
+void Fused32::Impl::push_slot_async(cudaStream_t st)
 {
     const double *w = S.w;
     h_slot.er = (S.algorithm == NADIA_ER);
@@ -553,8 +565,8 @@ void Fused32::Impl::push_slot()
     h_slot.w_ps = (float)w[PS];
     h_slot.w_psf = (float)w[PSF];
     h_slot.project = h_slot.er || w[PF] != 0 || w[PSF] != 0;
-    NADIA_CUDA(cudaMemcpyAsync(slot.p, &h_slot, sizeof(Slot), cudaMemcpyHostToDevice, S.st));
-    NADIA_CUDA(cudaStreamSynchronize(S.st));
+    // pageable source: the copy is staged before this returns
+    NADIA_CUDA(cudaMemcpyAsync(slot.p, &h_slot, sizeof(Slot), cudaMemcpyHostToDevice, st));
 }
 
 void Fused32::Impl::to_panel(const double *h, size_t stride, std::vector<float> &out) const
@@ -815,6 +827,7 @@ void Fused32::Impl::prime(cudaStream_t st)
 {
     const Slot *const *sl = slot_ptr.p;
     choice->row->row(kRowPrime, sl, 1, nx, ny, twy, st);
+    g_launches += 1;
     p_valid = true;
 }
 
@@ -829,6 +842,7 @@ void Fused32::iterate(int count)
 {
     Impl &I = *impl;
     I.check_algorithm();
+    I.use_choice(I.choice);
     I.push_slot();
     cudaStream_t st = I.S.st;
     if (!I.p_valid) I.prime(st);
@@ -846,10 +860,14 @@ void Fused32::iterate(int count)
         }
         while (left >= G) {
             NADIA_CUDA(cudaGraphLaunch(I.graph_exec, st));
+            g_launches += 2 * G;
             left -= G;
         }
     }
-    for (; left > 0; --left) I.launch_iteration(st);
+    for (; left > 0; --left) {
+        I.launch_iteration(st);
+        g_launches += 2;
+    }
     NADIA_CUDA(cudaGetLastError());
     I.S.iters += count;
 }
@@ -881,6 +899,7 @@ void Fused32::shrinkwrap(double gauss_width, double threshold)
     k_max<<<gb, 256, 0, I.S.st>>>(I.tmp2.p, I.n, I.maxpart.p);
     k_max_final<<<1, 256, 0, I.S.st>>>(I.maxpart.p, gb);
     k_divide<<<gb, 256, 0, I.S.st>>>(I.tmp2.p, I.sup.p, I.n, I.maxpart.p + gb);
+    g_launches += 7;
     NADIA_CUDA(cudaGetLastError());
 }
 

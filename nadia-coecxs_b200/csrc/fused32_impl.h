@@ -121,6 +121,10 @@ struct Fused32::Impl {
     explicit Impl(Solver &s);
     ~Impl();
     void push_slot();
+    void push_slot_async(cudaStream_t st);
+    // the variants the next launches use (the handle's own, or a batch's);
+    // sets the column-block count the row pass sums over
+    void use_choice(const f32::Choice *c);
     void to_panel(const double *h, size_t stride, std::vector<float> &out) const;
     void from_panel(const std::vector<float> &in, size_t stride, double *h) const;
     void upload(void *dst, const std::vector<float> &v);

@@ -3,12 +3,18 @@
 #include "solver.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 
+#include "batch.h"
 #include "fused32.h"
 
 namespace nadia {
+
+namespace {
+std::atomic<unsigned long long> g_uid{1};
+}
 
 namespace {
 void h2d(void *d, const void *h, size_t bytes, cudaStream_t s)
@@ -45,6 +51,7 @@ Solver::Solver(int kind_, int nx_, int ny_, int prec_, int n_best_)
     FftPlan tmpx = make_plan(nx), tmpy = make_plan(ny);
     (void)tmpx; (void)tmpy;
     n = (size_t)nx * ny;
+    uid = g_uid++;
     NADIA_CUDA(cudaGetDevice(&device));
     NADIA_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     h_isqrt.assign(n, 0.0);
@@ -86,6 +93,7 @@ Solver::Solver(int kind_, int nx_, int ny_, int prec_, int n_best_)
 
 Solver::~Solver()
 {
+    forget_batches_with(uid);
     if (st) {
         cudaStreamSynchronize(st);
         f32.reset();

@@ -21,6 +21,7 @@ struct Solver {
     int kind = NADIA_PLANAR, nx = 0, ny = 0, prec = NADIA_FP64, n_best = 0;
     size_t n = 0;
     int device = 0;
+    unsigned long long uid = 0; // unique per handle (batch plans key on it)
     cudaStream_t st = nullptr;
 
     // algorithm state (BaseCDI.h:87-150)

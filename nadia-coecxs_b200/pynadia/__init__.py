@@ -87,6 +87,9 @@ _PROTOS = {
     "nadia_get_intensity_autocorrelation": (_I, [_H, _D]),
     "nadia_synchronize": (_I, [_H]),
     "nadia_iterate_many": (_I, [ctypes.POINTER(_H), _I, _I]),
+    "nadia_get_stream": (_I, [_H, ctypes.POINTER(ctypes.c_void_p)]),
+    "nadia_pass_times": (_I, [ctypes.POINTER(_H), _I, _I, _D]),
+    "nadia_launch_count": (ctypes.c_longlong, []),
 }
 
 _LIB = None
@@ -315,9 +318,28 @@ class Solver:
     def synchronize(self):
         _check(self.lib.nadia_synchronize(self.h))
 
+    def stream(self):
+        """The cudaStream_t (as an int) this handle's work is queued on."""
+        p = ctypes.c_void_p()
+        _check(self.lib.nadia_get_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
 
 def iterate_many(solvers, iterations):
     """Step several reconstructions together (nadia_iterate_many)."""
     lib = load()
     arr = (_H * len(solvers))(*[s.h for s in solvers])
     _check(lib.nadia_iterate_many(arr, len(solvers), int(iterations)))
+
+
+def pass_times(solvers, reps=5):
+    """Device microseconds of one column pass and one row pass for a batch."""
+    lib = load()
+    arr = (_H * len(solvers))(*[s.h for s in solvers])
+    out = np.zeros(2)
+    _check(lib.nadia_pass_times(arr, len(solvers), int(reps), _ptr(out)))
+    return float(out[0]), float(out[1])
+
+
+def launch_count():
+    return int(load().nadia_launch_count())

@@ -180,3 +180,55 @@ def test_fp32_unsupported_paths_report_status():
     with pytest.raises(pynadia.NadiaError) as e:
         pynadia.Solver("planar", 320, 320, precision=pynadia.FP32)
     assert e.value.code == 3
+
+
+def test_iterate_many_matches_individual_runs():
+    """Reconstructions stepped together (mixed sizes and geometries, one
+    batched launch per pass and size group, graph replay) give the result
+    each gives alone; the batch may use another tuned tile variant, so the
+    comparison allows FP32 rounding."""
+    def make():
+        out = []
+        for n, seed in ((256, 1), (256, 2), (512, 3)):
+            c = synth.PlanarCase(n, n * 0.16, 2, 1e8, seed=seed, support_side=int(n * 0.42))
+            s = pynadia.Solver("planar", n, n, precision=pynadia.FP32)
+            s.set_support(c.support)
+            s.set_intensity(c.intensity)
+            s.initialise_estimate(seed)
+            s.set_algorithm("ER")
+            out.append(s)
+        f = synth.FresnelCase(256, seed=5)
+        s = pynadia.Solver("fresnel", 256, 256, precision=pynadia.FP32, white_field=f.white_field,
+                           wavelength=f.wavelength, focal_detector_length=f.zfd,
+                           focal_sample_length=f.zfs, pixel_size=f.pixel)
+        s.set_support(f.support)
+        s.set_intensity(f.intensity)
+        s.initialise_estimate(1)
+        out.append(s)
+        return out
+
+    alone, mixed = make(), make()
+    for s in alone:
+        s.iterate(20)
+    pynadia.iterate_many(mixed, 20)
+    for a, b in zip(alone, mixed):
+        ha, hb = a.get_error_history(20), b.get_error_history(20)
+        assert np.max(np.abs(ha - hb) / ha) <= RUN_TOL
+        assert l2rel(b.get_exit_surface_wave(), a.get_exit_surface_wave()) <= 1e-4
+    # and again, now replaying the captured graph, after a shrinkwrap on each
+    for s in alone + mixed:
+        s.apply_shrinkwrap(1.5, 0.1)
+    for s in alone:
+        s.iterate(33)
+    pynadia.iterate_many(mixed, 33)
+    for a, b in zip(alone, mixed):
+        assert abs(a.get_error() - b.get_error()) <= RUN_TOL * a.get_error()
+
+
+def test_pass_times_and_launch_count():
+    _, b = planar_pair(512)
+    b.set_algorithm("HIO")
+    l0 = pynadia.launch_count()
+    col, row = pynadia.pass_times([b], reps=3)
+    assert col > 0 and row > 0
+    assert pynadia.launch_count() > l0
