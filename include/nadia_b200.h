@@ -236,6 +236,27 @@ int nadia_pass_times(nadia_solver *const *solvers, int count, int reps, double o
  * every kernel they contain). */
 long long nadia_launch_count(void);
 
+/* ---- shrinkwrap without device allocation (no counterpart in the reference)
+ *
+ * For callers that cannot allocate device memory when they need a support
+ * update: a server stepping many reconstructions on concurrent streams,
+ * where cudaMalloc/cudaFree would synchronise the device and stall the other
+ * streams, or a process whose device memory is already committed to an
+ * admission budget or another allocator.  Same computation as
+ * BaseCDI::apply_shrinkwrap (BaseCDI.c++:416-429) in single precision, on
+ * caller-owned device buffers: esw_dev holds nx*ny interleaved complex
+ * floats, support_dev receives nx*ny floats (element (x,y) at x*ny+y).  Work
+ * is queued on `stream` (a cudaStream_t; NULL = the default stream) and the
+ * call returns without waiting.  It allocates nothing: its working memory is
+ * a 128 KB array built into the library that every GPU using this entry point
+ * keeps until the process exits, which limits the grid to 4096 x 4096
+ * (larger grids return NADIA_ERR_INVALID).  All calls on a device share that
+ * array, so calls whose work overlaps on the GPU race: serialise them.  The
+ * first call on a device looks the array up; make it before capturing a
+ * stream on that device. */
+int nadia_shrinkwrap_noalloc_f32(const float *esw_dev, float *support_dev, int nx, int ny,
+                                 double gauss_width, double threshold, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

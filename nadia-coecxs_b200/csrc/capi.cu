@@ -360,3 +360,21 @@ extern "C" int nadia_pass_times(nadia_solver *const *solvers, int count, int rep
 }
 
 extern "C" long long nadia_launch_count(void) { return nadia::g_launches.load(); }
+
+namespace nadia {
+namespace noalloc {
+void shrinkwrap(const float *esw, float *support, int nx, int ny, double gauss_width,
+                double threshold, cudaStream_t st);
+}
+} // namespace nadia
+
+extern "C" int nadia_shrinkwrap_noalloc_f32(const float *esw_dev, float *support_dev, int nx,
+                                            int ny, double gauss_width, double threshold,
+                                            void *stream)
+{
+    return guard([&] {
+        nadia::noalloc::shrinkwrap(esw_dev, support_dev, nx, ny, gauss_width, threshold,
+                                   static_cast<cudaStream_t>(stream));
+        nadia::g_launches += 5;
+    });
+}

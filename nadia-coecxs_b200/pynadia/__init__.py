@@ -90,6 +90,8 @@ _PROTOS = {
     "nadia_get_stream": (_I, [_H, ctypes.POINTER(ctypes.c_void_p)]),
     "nadia_pass_times": (_I, [ctypes.POINTER(_H), _I, _I, _D]),
     "nadia_launch_count": (ctypes.c_longlong, []),
+    "nadia_shrinkwrap_noalloc_f32": (_I, [ctypes.c_void_p, ctypes.c_void_p, _I, _I,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
 }
 
 _LIB = None
@@ -343,3 +345,10 @@ def pass_times(solvers, reps=5):
 
 def launch_count():
     return int(load().nadia_launch_count())
+
+
+def shrinkwrap_noalloc_f32(esw_ptr, support_ptr, nx, ny, gauss_width=1.5, threshold=0.1,
+                           stream=0):
+    """nadia_shrinkwrap_noalloc_f32 on device pointers (ints); queued on `stream`."""
+    _check(load().nadia_shrinkwrap_noalloc_f32(esw_ptr, support_ptr, int(nx), int(ny),
+                                               float(gauss_width), float(threshold), stream))
