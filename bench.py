@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=8)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--quick", action="store_true",
+                   help="device-resident steps only (for profiling): no e2e, FP64, CPU legs")
     return p.parse_args()
 
 
@@ -263,6 +265,14 @@ def ours(args, rank, world, local_rank):
             s.synchronize()
     launches = pynadia.launch_count() - l0
     step_ms = [a.elapsed_time(b) for a, b in ev]
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "batch": B, "ms_per_step": step_ms,
+                              "launches": launches}), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return None
     tot_ms = sum(step_ms)
     if dist:
         t = torch.tensor([tot_ms], device="cuda")

@@ -264,11 +264,24 @@ struct Swizzle {
         const int t = (a >> S1_) ^ (S2_ ? (a >> S2_) : 0);
         return a ^ ((t & M_) << SH_);
     }
+    // Adding a multiple of 2^B, B above every bit the swizzle reads
+    // (S1..S1+2, S2..S2+2) and writes (SH..SH+2), commutes with it:
+    // apply(a + r*c) = apply(a) + r*c.
+    static constexpr bool stride_commutes(int c)
+    {
+        const int hi = (S1_ > S2_ ? S1_ : S2_) + 3;
+        return c > 0 && c % (1 << hi) == 0 && SH_ + 3 <= hi;
+    }
 };
 
-template <int N_, int NT_, int L_, int MAP_, class RL, class SW, int MINB_ = 1>
+// PING: exchanges alternate between two shared buffers, which saves the
+// barrier between reading one pass's inputs and writing the next pass's
+// outputs (a thread only overwrites a buffer after a barrier that every
+// thread reaches once it has finished reading that buffer).
+template <int N_, int NT_, int L_, int MAP_, class RL, class SW, int MINB_ = 1, bool PING_ = false>
 struct TileCfg {
     static constexpr int N = N_, NT = NT_, L = L_, MAP = MAP_, MINB = MINB_;
+    static constexpr bool PING = PING_;
     static constexpr int E = N * L / NT;
     static constexpr int P = RL::P;
     using Rad = RL;
@@ -292,8 +305,9 @@ struct TileCfg {
         return s;
     }
     // shared-memory words (float2)
-    static constexpr int smem_words() { return N * L; }
+    static constexpr int smem_words() { return N * L * (PING ? 2 : 1); }
     static __device__ __forceinline__ int sidx(int s, int pos) { return SW::apply(pos * L + s); }
+    using Swz = SW;
     // butterfly beta of a pass whose signals hold NR = N/R butterflies
     static __device__ __forceinline__ void map(int beta, int NR, int &s, int &j)
     {
@@ -367,32 +381,47 @@ __device__ __forceinline__ void pass_compute(float2 (&v)[C::E], const float2 *__
 
 // After pass p: write outputs to shared memory, then load the inputs of pass p+1.
 template <class C, bool FWD, int p>
-__device__ __forceinline__ void pass_exchange(float2 (&v)[C::E], float2 *sm)
+__device__ __forceinline__ void pass_exchange(float2 (&v)[C::E], float2 *sm0)
 {
+    float2 *sm = (C::PING && (p & 1)) ? sm0 + C::N * C::L : sm0;
     constexpr int R = C::radix(p, FWD);
     constexpr int Ns = C::span(p, FWD);
     constexpr int NR = C::N / R;
     constexpr int B = C::E / R;
+    constexpr int WSTRIDE = Ns * C::L;
 #pragma unroll
     for (int q = 0; q < B; ++q) {
         int s, j;
         C::map(threadIdx.x + q * C::NT, NR, s, j);
         const int base = (j / Ns) * Ns * R + (j % Ns);
+        if constexpr (C::Swz::stride_commutes(WSTRIDE)) {
+            const int a0 = C::sidx(s, base);
 #pragma unroll
-        for (int r = 0; r < R; ++r) sm[C::sidx(s, base + r * Ns)] = v[q * R + r];
+            for (int r = 0; r < R; ++r) sm[a0 + r * WSTRIDE] = v[q * R + r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) sm[C::sidx(s, base + r * Ns)] = v[q * R + r];
+        }
     }
     __syncthreads();
     constexpr int R2 = C::radix(p + 1, FWD);
     constexpr int NR2 = C::N / R2;
     constexpr int B2 = C::E / R2;
+    constexpr int RSTRIDE = NR2 * C::L;
 #pragma unroll
     for (int q = 0; q < B2; ++q) {
         int s, j;
         C::map(threadIdx.x + q * C::NT, NR2, s, j);
+        if constexpr (C::Swz::stride_commutes(RSTRIDE)) {
+            const int a0 = C::sidx(s, j);
 #pragma unroll
-        for (int r = 0; r < R2; ++r) v[q * R2 + r] = sm[C::sidx(s, j + r * NR2)];
+            for (int r = 0; r < R2; ++r) v[q * R2 + r] = sm[a0 + r * RSTRIDE];
+        } else {
+#pragma unroll
+            for (int r = 0; r < R2; ++r) v[q * R2 + r] = sm[C::sidx(s, j + r * NR2)];
+        }
     }
-    __syncthreads();
+    if (!C::PING) __syncthreads();
 }
 
 template <class C, bool FWD, int p = 0>

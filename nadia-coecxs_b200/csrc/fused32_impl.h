@@ -72,6 +72,7 @@ using RowLaunch = void (*)(int mode, const Slot *const *slots, int nslots, int n
 struct TileVariant {
     int n = 0, nt = 0, L = 0, minb = 0;
     bool persistent = false;
+    bool ping = false;
     const char *radices = "";
     void (*prepare)() = nullptr;
     ColLaunch col = nullptr;
@@ -131,6 +132,7 @@ struct Fused32::Impl {
     void download(std::vector<float> &v, const void *src, size_t count);
     void upload_intensity();
     void blur(bool cplx, const void *in, double gauss_width, int cut);
+    int blur_blocks() const;
     void check_algorithm() const;
     void prime(cudaStream_t st);
     void launch_iteration(cudaStream_t st);

@@ -19,6 +19,26 @@ __device__ __forceinline__ float support_factor(float s)
     return s == 0.f ? 0.f : (s < 1.f ? s : 1.f);
 }
 
+// Modulus projection of one transform value (BaseCDI::scale_intensity,
+// BaseCDI.c++:163-189, with Complex_2D::set_mag, Complex_2D.h:205-215):
+// u is the detector-plane value, m its sqrt(I) (-1 = unmeasured).  Returns
+// the projected value and adds (|u| - m)^2 to diff for measured pixels.
+// Written with selects rather than branches.
+__device__ __forceinline__ float2 modulus(float2 u, float m, double &diff)
+{
+    const float a2 = u.x * u.x + u.y * u.y;
+    const bool measured = !(m < 0.f);
+    const bool zero = !(a2 > 0.f);
+    const float inv = rsqrtf(zero ? 1.f : a2);
+    const float mag = zero ? 0.f : a2 * inv;
+    const float sc = measured ? m * inv : 1.f;
+    float2 r = make_float2(u.x * sc, u.y * sc);
+    if (measured && zero) r = make_float2(m, 0.f);
+    const double d = (double)mag - (double)m;
+    diff += measured ? d * d : 0.0;
+    return r;
+}
+
 // FP64 block sum; result valid in thread 0
 template <int NT>
 __device__ __forceinline__ double block_sum(double v)
@@ -63,36 +83,12 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_col(const Slot *const *slots
         const float m = __ldg(&mI[a]);
         float2 X = v[e];
         if (!FRESNEL) {
-            if (!(m < 0.f)) {
-                const float a2 = X.x * X.x + X.y * X.y;
-                if (a2 > 0.f) {
-                    const float inv = rsqrtf(a2);
-                    const double d = (double)(a2 * inv * s0) - (double)m;
-                    diff += d * d;
-                    X = cscale(X, m * s0 * inv);
-                } else {
-                    diff += (double)m * (double)m;
-                    X = make_float2(m * s0, 0.f);
-                }
-            } else {
-                X = cscale(X, s0 * s0);
-            }
+            // Planar: Psi = X s0; back-propagated value = projected Psi * s0
+            X = cscale(modulus(cscale(X, s0), m, diff), s0);
         } else {
             const float2 cf = cmul(__ldg(&S.tx[kx]), __ldg(&S.ty[ky]));
             const float2 w = S.W[a];
-            float2 u = cadd(cscale(cmul(cf, X), s0), w);
-            if (!(m < 0.f)) {
-                const float a2 = u.x * u.x + u.y * u.y;
-                if (a2 > 0.f) {
-                    const float inv = rsqrtf(a2);
-                    const double d = (double)(a2 * inv) - (double)m;
-                    diff += d * d;
-                    u = cscale(u, m * inv);
-                } else {
-                    diff += (double)m * (double)m;
-                    u = make_float2(m, 0.f);
-                }
-            }
+            const float2 u = modulus(cadd(cscale(cmul(cf, X), s0), w), m, diff);
             X = cscale(cmulc(csub(u, w), cf), s0);
         }
         v[e] = X;
@@ -282,6 +278,25 @@ TileVariant make_variant(const char *radices)
     t.nt = NT;
     t.L = L;
     t.minb = MINB;
+    t.radices = radices;
+    t.prepare = &prepare_variant<CC, CR>;
+    t.col = &launch_col<CC>;
+    t.row = &launch_row<CR>;
+    return t;
+}
+
+// The same tile shape with ping-pong exchange buffers (twice the shared memory).
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_ping(const char *radices)
+{
+    using CC = TileCfg<N, NT, L, kColMap, Radices<Rs...>, SW, MINB, true>;
+    using CR = TileCfg<N, NT, L, kRowMap, Radices<Rs...>, SW, MINB, true>;
+    TileVariant t;
+    t.n = N;
+    t.nt = NT;
+    t.L = L;
+    t.minb = MINB;
+    t.ping = true;
     t.radices = radices;
     t.prepare = &prepare_variant<CC, CR>;
     t.col = &launch_col<CC>;

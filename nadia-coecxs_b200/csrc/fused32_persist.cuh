@@ -104,37 +104,12 @@ __global__ void __launch_bounds__(C::NT, 1)
             const float m = Mb[raw_col<C>(s, kx)];
             float2 X = v[e];
             if (!FRESNEL) {
-                if (!(m < 0.f)) {
-                    const float a2 = X.x * X.x + X.y * X.y;
-                    if (a2 > 0.f) {
-                        const float inv = rsqrtf(a2);
-                        const double d = (double)(a2 * inv * s0) - (double)m;
-                        diff += d * d;
-                        X = cscale(X, m * s0 * inv);
-                    } else {
-                        diff += (double)m * (double)m;
-                        X = make_float2(m * s0, 0.f);
-                    }
-                } else {
-                    X = cscale(X, s0 * s0);
-                }
+                X = cscale(modulus(cscale(X, s0), m, diff), s0);
             } else {
                 const int ky = c0 * kPanel + s;
                 const float2 cf = cmul(__ldg(&S.tx[kx]), __ldg(&S.ty[ky]));
                 const float2 w = __ldg(&S.W[paddr(kx, ky, nx)]);
-                float2 u = cadd(cscale(cmul(cf, X), s0), w);
-                if (!(m < 0.f)) {
-                    const float a2 = u.x * u.x + u.y * u.y;
-                    if (a2 > 0.f) {
-                        const float inv = rsqrtf(a2);
-                        const double d = (double)(a2 * inv) - (double)m;
-                        diff += d * d;
-                        u = cscale(u, m * inv);
-                    } else {
-                        diff += (double)m * (double)m;
-                        u = make_float2(m, 0.f);
-                    }
-                }
+                const float2 u = modulus(cadd(cscale(cmul(cf, X), s0), w), m, diff);
                 X = cscale(cmulc(csub(u, w), cf), s0);
             }
             v[e] = X;

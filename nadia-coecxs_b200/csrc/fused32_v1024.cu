@@ -15,6 +15,8 @@ void add_variants_1024(std::vector<TileVariant> &v)
     v.push_back(make_persistent<1024, 128, 4, 4, Swizzle<4, 6, 3, 2>, 16, 16, 4>("16.16.4"));
     v.push_back(make_persistent<1024, 512, 4, 2, Swizzle<4, 5, 3, 2>, 8, 8, 4, 4>("8.8.4.4"));
     v.push_back(make_persistent<1024, 512, 8, 1, Swizzle<4, 6, 3, 2>, 16, 16, 4>("16.16.4"));
+    v.push_back(make_ping<1024, 256, 4, 2, Swizzle<4, 6, 3, 2>, 16, 16, 4>("16.16.4"));
+    v.push_back(make_ping<1024, 512, 4, 2, Swizzle<4, 5, 3, 2>, 8, 8, 4, 4>("8.8.4.4"));
 }
 
 } // namespace f32

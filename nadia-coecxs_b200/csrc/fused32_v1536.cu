@@ -11,6 +11,7 @@ void add_variants_1536(std::vector<TileVariant> &v)
     v.push_back(make_variant<1536, 512, 4, 1, Swizzle<4, 5, 3, 2>, 4, 4, 4, 4, 2, 3>("4.4.4.4.2.3"));
     v.push_back(make_persistent<1536, 256, 4, 2, Swizzle<4, 5, 7, 1>, 8, 8, 8, 3>("8.8.8.3"));
     v.push_back(make_persistent<1536, 512, 4, 1, Swizzle<4, 5, 3, 2>, 4, 4, 4, 4, 2, 3>("4.4.4.4.2.3"));
+    v.push_back(make_ping<1536, 256, 4, 2, Swizzle<4, 5, 7, 1>, 8, 8, 8, 3>("8.8.8.3"));
 }
 
 } // namespace f32

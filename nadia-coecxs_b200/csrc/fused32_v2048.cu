@@ -16,6 +16,9 @@ void add_variants_2048(std::vector<TileVariant> &v)
     v.push_back(make_persistent<2048, 256, 4, 2, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
     v.push_back(make_persistent<2048, 1024, 4, 1, Swizzle<4, 5, 3, 2>, 8, 8, 8, 4>("8.8.8.4"));
     v.push_back(make_persistent<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
+    v.push_back(make_ping<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
+    v.push_back(make_ping<2048, 1024, 4, 1, Swizzle<4, 5, 3, 2>, 8, 8, 8, 4>("8.8.8.4"));
+    v.push_back(make_ping<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
 }
 
 } // namespace f32

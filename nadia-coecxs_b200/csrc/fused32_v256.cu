@@ -13,6 +13,7 @@ void add_variants_256(std::vector<TileVariant> &v)
     v.push_back(make_persistent<256, 256, 16, 2, Swizzle<4, 8, 3, 2>, 16, 16>("16.16"));
     v.push_back(make_persistent<256, 128, 8, 4, Swizzle<4, 7, 3, 2>, 16, 16>("16.16"));
     v.push_back(make_persistent<256, 256, 8, 3, Swizzle<4, 6, 3, 2>, 8, 8, 4>("8.8.4"));
+    v.push_back(make_ping<256, 256, 16, 2, Swizzle<4, 8, 3, 2>, 16, 16>("16.16"));
 }
 
 } // namespace f32

@@ -13,6 +13,7 @@ void add_variants_512(std::vector<TileVariant> &v)
     v.push_back(make_persistent<512, 256, 8, 2, Swizzle<4, 6, 3, 2>, 16, 8, 4>("16.8.4"));
     v.push_back(make_persistent<512, 128, 4, 4, Swizzle<4, 6, 3, 2>, 16, 8, 4>("16.8.4"));
     v.push_back(make_persistent<512, 256, 4, 3, Swizzle<4, 0, 7, 1>, 8, 8, 8>("8.8.8"));
+    v.push_back(make_ping<512, 256, 8, 2, Swizzle<4, 6, 3, 2>, 16, 8, 4>("16.8.4"));
 }
 
 } // namespace f32
