@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=8)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--serve-requests", type=int, default=48,
+                   help="requests in the saturated serving run (0 = skip serving)")
+    p.add_argument("--serve-only", action="store_true", help="print the serving report only")
     p.add_argument("--quick", action="store_true",
                    help="device-resident steps only (for profiling): no e2e, FP64, CPU legs")
     return p.parse_args()
@@ -212,6 +215,106 @@ def run_program(pynadia, solvers):
             s.apply_shrinkwrap(1.5, 0.1)
 
 
+# --------------------------------------------------------------- serving
+
+SERVE_ITERS = 500
+
+
+class ServeInputs:
+    """Patterns for the serving stream: PlanarCDI at 1024^2 (radius 160,
+    sigma 2, 1e8 photons) and 2048^2 (radius 320, sigma 4, 1e9 photons, 8x8
+    beam stop) and PolyCDI at 1024^2 with a 10-line Gaussian spectrum of 5%
+    FWHM (padding 28: padded grid 1080^2), `per_kind` seeded patterns each;
+    every request also gets its own initialise_estimate seed."""
+
+    def __init__(self, synth, per_kind=2):
+        self.planar1024 = [synth.PlanarCase(1024, 160, 2, 1e8, seed=100 + i, support_side=400)
+                           for i in range(per_kind)]
+        self.planar2048 = [synth.PlanarCase(2048, 320, 4, 1e9, seed=200 + i, support_side=800,
+                                            beam_stop=8) for i in range(per_kind)]
+        self.poly1024 = [synth.PolyCase(1024, seed=300 + i, padding=28) for i in range(per_kind)]
+
+
+def serve(pynadia, inputs, rate, n_req, seed, planar_precision, poly_precision,
+          budget=80 * 10**9, max_active=16, chunk=25):
+    """Poisson arrivals at `rate`/s (seeded exponential gaps): 35% PlanarCDI
+    1024^2, 35% PlanarCDI 2048^2, 30% PolyCDI 1024^2, each 500 HIO iterations
+    (beta 0.9) with shrinkwrap every 50.  Latency = arrival (scheduled time)
+    to result on the host."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, n_req)
+    kinds = rng.choice(3, size=n_req, p=[0.35, 0.35, 0.30])
+    srv = pynadia.Server(budget, max_active=max_active, chunk=chunk)
+    ids, lag, sizes = [], [], []
+    t_start = time.perf_counter()
+    t_sched = t_start
+    for i in range(n_req):
+        t_sched += gaps[i]
+        while True:
+            d = t_sched - time.perf_counter()
+            if d <= 0:
+                break
+            time.sleep(min(d, 0.002))
+        k = int(kinds[i])
+        common = dict(algorithm="HIO", beta=0.9, iterations=SERVE_ITERS, shrinkwrap_every=50,
+                      shrinkwrap_sigma=1.5, shrinkwrap_threshold=0.1, seed=i)
+        lag.append(time.perf_counter() - t_sched)
+        if k == 2:
+            c = inputs.poly1024[i % len(inputs.poly1024)]
+            ids.append(srv.submit("poly", c.intensity, c.support, precision=poly_precision,
+                                  spectrum=c.spectrum, **common))
+        else:
+            c = (inputs.planar1024 if k == 0 else inputs.planar2048)[i % 2]
+            ids.append(srv.submit("planar", c.intensity, c.support, precision=planar_precision,
+                                  beam_stop=c.beam_stop, **common))
+        sizes.append(k)
+    lat, queue_wait, errs = [], [], []
+    for rid, lg in zip(ids, lag):
+        srv.wait(rid, -1)
+        _, _, err, t = srv.result(rid)
+        lat.append(lg + t[2])
+        queue_wait.append(t[0])
+        errs.append(err)
+    wall = time.perf_counter() - t_start
+    st = srv.stats()
+    srv.close()
+    lat_sorted = sorted(lat)
+
+    def pct(a, q):
+        a = sorted(a)
+        return 1000.0 * a[min(len(a) - 1, int(math.ceil(q * len(a))) - 1)]
+
+    return {"offered_rate_per_s": rate, "requests": n_req,
+            "mix": {"planar1024": int((kinds == 0).sum()), "planar2048": int((kinds == 1).sum()),
+                    "poly1024": int((kinds == 2).sum())},
+            "recon_per_s": n_req / wall, "wall_s": wall,
+            "latency_ms": {"p50": pct(lat_sorted, 0.5), "p99": pct(lat_sorted, 0.99),
+                           "max": 1000.0 * lat_sorted[-1]},
+            "queue_wait_ms": {"p50": pct(queue_wait, 0.5), "p99": pct(queue_wait, 0.99)},
+            "peak_charged_gb": st["peak_bytes"] / 1e9, "steps": st["steps"],
+            "failed": st["failed"], "precision": {"planar": "FP32" if planar_precision else "FP64",
+                                                   "poly": "FP32" if poly_precision else "FP64"}}
+
+
+def serving_report(pynadia, synth, n_req=48, n_req_fp64=12):
+    """Config 5 on one GPU: the offered 200/s stream (saturated), a stream at
+    about 80% of the rate it sustained, and the same stream served in the
+    FP64 plain form."""
+    inputs = ServeInputs(synth)
+    FP32, FP64 = pynadia.FP32, pynadia.FP64
+    # untimed warm-up: tune the tile variants of both sizes, build plans
+    serve(pynadia, inputs, 200.0, 6, 7, FP32, FP64)
+    sat = serve(pynadia, inputs, 200.0, n_req, 1, FP32, FP64)
+    rate = max(1.0, 0.8 * sat["recon_per_s"])
+    sus = serve(pynadia, inputs, rate, max(12, n_req // 2), 2, FP32, FP64)
+    fp64 = serve(pynadia, inputs, 200.0, n_req_fp64, 1, FP64, FP64)
+    return {"saturated": sat, "sustainable": sus, "fp64_plain": fp64,
+            "note": "PolyCDI requests run in the FP64 form in every run (the FP32 form covers "
+                    "PlanarCDI and FresnelCDI); admission by an 80 GB budget, at most 16 "
+                    "active, steps of up to 25 iterations"}
+
+
 def phase_aligned_error(x, ref):
     import numpy as np
     inner = np.vdot(x, ref)
@@ -226,6 +329,8 @@ def ours(args, rank, world, local_rank):
     from pynadia import synth
 
     torch.cuda.set_device(local_rank)
+    if args.serve_only:
+        return {"serving": serving_report(pynadia, synth, n_req=args.serve_requests)}
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -352,6 +457,10 @@ def ours(args, rank, world, local_rank):
                 "ratio_fp32_batched_over_fp64": value / world / (1.0 / t64),
                 "note": "FP64 plain form, one reconstruction, same program, host wall clock"}
 
+        serving = None
+        if args.serve_requests > 0:
+            serving = serving_report(pynadia, synth, n_req=args.serve_requests)
+
         cpu = None
         if not args.no_cpu:
             procs = max(1, min(os.cpu_count() or 1, 8))
@@ -374,6 +483,7 @@ def ours(args, rank, world, local_rank):
                            "note": "per reconstruction in a batch = its batch's step time"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": launches, "fp64_plain": fp64, "accuracy": accuracy,
+            "serving": serving,
         }
     if dist:
         dist.barrier()

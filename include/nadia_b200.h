@@ -138,8 +138,10 @@ void nadia_custom_weights(const double m[10], double w[5]);
 /* ---- estimate ----------------------------------------------------------- */
 
 /* initialise_estimate(seed): PlanarCDI.c++:39-62, FresnelCDI.c++:152-201,
- * PolyCDI.c++:102-126.  Uses the C library's srand/rand on the host, as the
- * reference does, then uploads the estimate. */
+ * PolyCDI.c++:102-126.  Draws the C library's srand(seed)/rand() sequence on
+ * the host, as the reference does, from a private generator state (the
+ * process's own rand() state is left alone, so handles can initialise from
+ * several threads), then uploads the estimate. */
 int nadia_initialise_estimate(nadia_solver *s, int seed);
 
 /* BaseCDI::set_exit_surface_wave / get_exit_surface_wave -- NADIA/include/BaseCDI.h:285-291. */
@@ -194,6 +196,14 @@ int nadia_fresnel_auto_set_norm(nadia_solver *s);
 int nadia_fresnel_set_norm(nadia_solver *s, double normalisation);
 int nadia_fresnel_get_illumination_at_sample(nadia_solver *s, double *illumination);
 
+/* FresnelCDI::set_experimental_parameters (FresnelCDI.c++:57-95) and
+ * FresnelCDI::set_normalisation (FresnelCDI.h:187-189: records the
+ * normalisation without rescaling, so the next set_norm scales relative to it). */
+int nadia_fresnel_set_experimental_parameters(nadia_solver *s, double beam_wavelength,
+                                              double focal_detector_length,
+                                              double focal_sample_length, double pixel_size);
+int nadia_fresnel_set_normalisation(nadia_solver *s, double normalisation);
+
 /* The single operators, as the IDL binding exposes them
  * (IDL_interface.c:947-985): each transforms the complex array in place
  * on an nx*ny grid (PLANAR and FRESNEL). */
@@ -205,6 +215,11 @@ int nadia_project_intensity(nadia_solver *s, double *field);
 
 /* PlanarCDI::get_intensity_autocorrelation -- PlanarCDI.c++:13-36. */
 int nadia_get_intensity_autocorrelation(nadia_solver *s, double *autoc);
+
+/* Complex_2D::perform_forward_fft / perform_backward_fft (Complex_2D.c++:487-503)
+ * on a host array: in-place unnormalised 2-D DFT (forward = sign -1), FP64,
+ * computed on the current device with the canonical transform schedule. */
+int nadia_fft2d(double *field, int nx, int ny, int forward);
 
 /* Waits for the handle's queued device work. */
 int nadia_synchronize(nadia_solver *s);
@@ -218,6 +233,81 @@ int nadia_synchronize(nadia_solver *s);
  * that `iterations` calls of nadia_iterate would have left it in.  No
  * counterpart in the reference, which runs one reconstruction per process. */
 int nadia_iterate_many(nadia_solver *const *solvers, int count, int iterations);
+
+/* ---- serving (no counterpart in the reference) ----------------------------
+ *
+ * A request loop on the current GPU: diffraction patterns are submitted at
+ * any time from any thread, admitted in arrival order while at most
+ * `max_active` reconstructions are on the device and the admission charge of
+ * the active ones (nadia_estimate_device_bytes) stays within `budget_bytes`,
+ * and all active reconstructions step together (as nadia_iterate_many) in
+ * steps of up to `chunk` iterations, shortened so that no request passes its
+ * next shrinkwrap or its last iteration.  Each request's estimate, support
+ * and intensity stay on the device until it finishes; its result then waits
+ * on the host until nadia_server_result collects it.  A request's result is
+ * the same whether it ran alone or among others.  A request runs the calls
+ * of a reference driver loop (CDI_reconstruction.c:377-439):
+ *   create -> [FRESNEL: auto_set_norm if asked] -> set_support ->
+ *   set_intensity -> [set_beam_stop] -> [POLY: set_spectrum] ->
+ *   initialise_estimate(seed) -> set_relaxation_parameter(beta) ->
+ *   set_algorithm(algorithm) -> iterations x (iterate, and apply_shrinkwrap
+ *   after every `shrinkwrap_every`-th iteration). */
+typedef struct nadia_server nadia_server;
+
+typedef struct nadia_request {
+    int kind;                    /* NADIA_PLANAR, NADIA_FRESNEL or NADIA_POLY */
+    int nx, ny;
+    int precision;               /* NADIA_FP32 or NADIA_FP64 */
+    const double *intensity;     /* nx*ny, copied at submit */
+    const double *support;       /* nx*ny, copied at submit */
+    const double *beam_stop;     /* nx*ny or NULL */
+    const double *spectrum;      /* POLY: nlambda rows of (wavelength, weight) */
+    int nlambda;
+    const double *white_field;   /* FRESNEL: nx*ny interleaved complex */
+    double wavelength, focal_detector_length, focal_sample_length, pixel_size;
+    double normalisation;        /* FRESNEL */
+    int fresnel_auto_norm;       /* FRESNEL: call auto_set_norm before initialising */
+    int algorithm;               /* NADIA_ER, NADIA_HIO, NADIA_RAAR, ... */
+    double beta;                 /* relaxation parameter */
+    int iterations;
+    int shrinkwrap_every;        /* 0 = no shrinkwrap */
+    double shrinkwrap_sigma, shrinkwrap_threshold;
+    int seed;                    /* initialise_estimate(seed) */
+} nadia_request;
+
+int nadia_server_create(unsigned long long budget_bytes, int max_active, int chunk,
+                        nadia_server **out);
+
+/* Copies the request's arrays and queues it; *id identifies it.  Returns
+ * NADIA_ERR_NOMEM if its admission charge exceeds the whole budget. */
+int nadia_server_submit(nadia_server *srv, const nadia_request *req, long long *id);
+
+/* Waits up to timeout_s seconds (negative = no limit) for a request to
+ * finish; *done = 1 when it has finished or failed. */
+int nadia_server_wait(nadia_server *srv, long long id, double timeout_s, int *done);
+
+/* Collects a finished request and forgets it: esw (2*nx*ny doubles),
+ * support (nx*ny) and the final error metric, each optional (NULL), and
+ * times[3] = {queued, on the device, arrival to result} in seconds.
+ * Returns the request's own status if it failed. */
+int nadia_server_result(nadia_server *srv, long long id, double *esw, double *support,
+                        double *final_error, double times[3]);
+
+/* out[8] = {queued, active, completed, failed, bytes charged now, peak bytes
+ * charged, steps run, requests admitted}. */
+int nadia_server_stats(nadia_server *srv, long long out[8]);
+
+/* Stops the loop (queued and unfinished requests fail) and frees the server. */
+int nadia_server_destroy(nadia_server *srv);
+
+/* The admission charge: device bytes one reconstruction holds once all its
+ * buffers exist.  poly_pad_x/poly_pad_y: PolyCDI's padding (else 0). */
+int nadia_estimate_device_bytes(int kind, int nx, int ny, int precision, int n_best,
+                                int poly_pad_x, int poly_pad_y, int nlambda,
+                                unsigned long long *bytes);
+
+/* Bytes of device memory the library's reconstructions hold now. */
+long long nadia_device_bytes(void);
 
 /* ---- diagnostics (no counterpart in the reference) ----------------------- */
 

@@ -26,6 +26,7 @@ std::atomic<long long> g_launches{0};
 namespace {
 
 constexpr int kGraphIters = 16;
+constexpr int kBatchClass = 4; // tuner class of batched groups (fused32.cu: choose)
 constexpr size_t kMaxPlans = 8;
 
 struct Group {
@@ -49,8 +50,12 @@ struct Plan {
         if (exec) cudaGraphExecDestroy(exec);
         for (auto &g : groups)
             if (g.st) cudaStreamDestroy(g.st);
-        for (auto e : fork) cudaEventDestroy(e);
-        for (auto e : join) cudaEventDestroy(e);
+        // group 0 runs on the batch stream and has no events of its own;
+        // destroying a null event would leave an error for the next check
+        for (auto e : fork)
+            if (e) cudaEventDestroy(e);
+        for (auto e : join)
+            if (e) cudaEventDestroy(e);
     }
 
     void launch_block(int iters)
@@ -133,7 +138,9 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
         p->join.resize(p->groups.size(), nullptr);
         for (size_t i = 0; i < p->groups.size(); ++i) {
             Group &g = p->groups[i];
-            g.choice = &f32::choose(g.nx, g.ny, g.fresnel, (int)g.members.size());
+            // the batched tuning class for every group, whatever its size, so a
+            // handle's arithmetic does not depend on the other handles of the call
+            g.choice = &f32::choose(g.nx, g.ny, g.fresnel, kBatchClass);
             g.twx = f32::twiddle_table(g.nx);
             g.twy = f32::twiddle_table(g.ny);
             std::vector<f32::Slot *> hp;

@@ -8,6 +8,7 @@
 
 #include "batch.h"
 #include "fused32.h"
+#include "server.h"
 #include "solver.h"
 
 using nadia::Error;
@@ -293,6 +294,25 @@ int nadia_fresnel_get_illumination_at_sample(nadia_solver *h, double *a)
     return guard([&] { need(a, "illumination"); S(h).get_illumination_at_sample(a); });
 }
 
+int nadia_fresnel_set_experimental_parameters(nadia_solver *h, double wl, double zfd, double zfs,
+                                              double pixel)
+{
+    return guard([&] {
+        Solver &s = S(h);
+        NADIA_REQUIRE(s.kind == NADIA_FRESNEL, NADIA_ERR_INVALID, "needs a FresnelCDI handle");
+        s.fresnel_set_experimental_parameters(wl, zfd, zfs, pixel);
+    });
+}
+
+int nadia_fresnel_set_normalisation(nadia_solver *h, double nn)
+{
+    return guard([&] {
+        Solver &s = S(h);
+        NADIA_REQUIRE(s.kind == NADIA_FRESNEL, NADIA_ERR_INVALID, "needs a FresnelCDI handle");
+        s.norm = nn;
+    });
+}
+
 int nadia_propagate_to_detector(nadia_solver *h, double *a)
 {
     return guard([&] { need(a, "field"); S(h).single_op(0, a); });
@@ -321,6 +341,29 @@ int nadia_project_intensity(nadia_solver *h, double *a)
 int nadia_get_intensity_autocorrelation(nadia_solver *h, double *a)
 {
     return guard([&] { need(a, "autoc"); S(h).autocorrelation(a); });
+}
+
+int nadia_fft2d(double *a, int nx, int ny, int forward)
+{
+    return guard([&] {
+        need(a, "field");
+        NADIA_REQUIRE(nx >= 1 && ny >= 1, NADIA_ERR_INVALID, "grid sizes must be positive");
+        cudaStream_t st;
+        NADIA_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        try {
+            nadia::plain::Fft2d fft;
+            fft.init(nx, ny);
+            nadia::DevBuf<double2> d((size_t)nx * ny);
+            NADIA_CUDA(cudaMemcpyAsync(d.p, a, d.bytes(), cudaMemcpyHostToDevice, st));
+            fft.exec(d.p, forward != 0, st);
+            NADIA_CUDA(cudaMemcpyAsync(a, d.p, d.bytes(), cudaMemcpyDeviceToHost, st));
+            NADIA_CUDA(cudaStreamSynchronize(st));
+        } catch (...) {
+            cudaStreamDestroy(st);
+            throw;
+        }
+        cudaStreamDestroy(st);
+    });
 }
 
 int nadia_synchronize(nadia_solver *h)
@@ -378,3 +421,84 @@ extern "C" int nadia_shrinkwrap_noalloc_f32(const float *esw_dev, float *support
         nadia::g_launches += 5;
     });
 }
+
+// ---- serving (server.h) -----------------------------------------------------
+
+struct nadia_server {
+    nadia::Server *srv;
+};
+
+namespace {
+nadia::Server &SV(nadia_server *h)
+{
+    if (!h || !h->srv) throw Error(NADIA_ERR_INVALID, "null server");
+    return *h->srv;
+}
+} // namespace
+
+extern "C" int nadia_server_create(unsigned long long budget_bytes, int max_active, int chunk,
+                                   nadia_server **out)
+{
+    return guard([&] {
+        need(out, "out");
+        *out = nullptr;
+        std::unique_ptr<nadia::Server> s(new nadia::Server((size_t)budget_bytes, max_active, chunk));
+        *out = new nadia_server{s.release()};
+    });
+}
+
+extern "C" int nadia_server_submit(nadia_server *h, const nadia_request *req, long long *id)
+{
+    return guard([&] {
+        need(req, "request");
+        need(id, "id");
+        *id = SV(h).submit(*req);
+    });
+}
+
+extern "C" int nadia_server_wait(nadia_server *h, long long id, double timeout_s, int *done)
+{
+    return guard([&] {
+        need(done, "done");
+        *done = SV(h).wait(id, timeout_s) ? 1 : 0;
+    });
+}
+
+extern "C" int nadia_server_result(nadia_server *h, long long id, double *esw, double *support,
+                                   double *final_error, double times[3])
+{
+    return guard([&] { SV(h).result(id, esw, support, final_error, times); });
+}
+
+extern "C" int nadia_server_stats(nadia_server *h, long long out[8])
+{
+    return guard([&] {
+        need(out, "out");
+        SV(h).stats(out);
+    });
+}
+
+extern "C" int nadia_server_destroy(nadia_server *h)
+{
+    return guard([&] {
+        if (!h) return;
+        delete h->srv;
+        delete h;
+    });
+}
+
+extern "C" int nadia_estimate_device_bytes(int kind, int nx, int ny, int precision, int n_best,
+                                           int poly_pad_x, int poly_pad_y, int nlambda,
+                                           unsigned long long *bytes)
+{
+    return guard([&] {
+        need(bytes, "bytes");
+        NADIA_REQUIRE(nx > 0 && ny > 0 && n_best >= 0 && poly_pad_x >= 0 && poly_pad_y >= 0 &&
+                          nlambda >= 0,
+                      NADIA_ERR_INVALID, "negative size");
+        *bytes = nadia::footprint_bytes(kind, nx, ny, precision, n_best, nx + 2 * poly_pad_x,
+                                        ny + 2 * poly_pad_y, nlambda);
+    });
+}
+
+extern "C" long long nadia_device_bytes(void) { return nadia::g_device_bytes.load(); }

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -35,6 +36,9 @@ struct Error : std::runtime_error {
         if (!(cond)) throw ::nadia::Error((code), (msg));                                 \
     } while (0)
 
+// Bytes currently held by DevBuf allocations of this process (all devices).
+inline std::atomic<long long> g_device_bytes{0};
+
 // Owning device allocation.
 template <class T>
 struct DevBuf {
@@ -56,10 +60,12 @@ struct DevBuf {
         release();
         if (count) NADIA_CUDA(cudaMalloc((void **)&p, count * sizeof(T)));
         n = count;
+        g_device_bytes += (long long)(n * sizeof(T));
     }
     void release()
     {
         if (p) cudaFree(p);
+        g_device_bytes -= (long long)(n * sizeof(T));
         p = nullptr;
         n = 0;
     }

@@ -588,10 +588,13 @@ void Fft2d::init(int nx_, int ny_)
     col_smem = 2 * (size_t)cols_per_block * nx * sizeof(double2);
     NADIA_REQUIRE(row_smem <= 227 * 1024 && col_smem <= 227 * 1024, NADIA_ERR_INVALID,
                   "grid too large for the FP64 transform");
+    // the attribute belongs to the kernel, not to this plan: every plan sets
+    // the same (largest) limit, so a smaller plan made later cannot lower it
+    // below what an earlier, larger plan launches with
     NADIA_CUDA(cudaFuncSetAttribute(k_fft_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)std::max<size_t>(row_smem, 48 * 1024)));
+                                    227 * 1024));
     NADIA_CUDA(cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)std::max<size_t>(col_smem, 48 * 1024)));
+                                    227 * 1024));
 }
 
 void Fft2d::exec(double2 *a, bool forward, cudaStream_t s) const

@@ -27,6 +27,30 @@ void d2h(void *h, const void *d, size_t bytes, cudaStream_t s)
     NADIA_CUDA(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, s));
     NADIA_CUDA(cudaStreamSynchronize(s));
 }
+// The C library's srand(seed)/rand() sequence (the reference seeds and draws
+// with them in initialise_estimate) from a private generator state: glibc's
+// rand() is random() on a 128-byte TYPE_3 state, which initstate_r/random_r
+// reproduce exactly, so reconstructions can initialise concurrently.
+class GlibcRand {
+public:
+    explicit GlibcRand(int seed)
+    {
+        std::memset(&rd_, 0, sizeof rd_);
+        std::memset(state_, 0, sizeof state_);
+        initstate_r((unsigned)seed, state_, sizeof state_, &rd_);
+    }
+    int operator()()
+    {
+        int32_t r = 0;
+        random_r(&rd_, &r);
+        return r;
+    }
+
+private:
+    random_data rd_;
+    char state_[128];
+};
+
 // Real_2D::get_max, Double_2D.h:252-265
 double host_max(const double *a, size_t n)
 {
@@ -123,9 +147,15 @@ std::vector<double> Solver::gauss_table(double gauss_width, int cut) const
 
 void Solver::plain_convolve(double *arr, double gauss_width, int cut)
 {
-    std::vector<double> g = gauss_table(gauss_width, cut);
-    gauss.alloc(g.size());
-    h2d(gauss.p, g.data(), g.size() * sizeof(double), st);
+    // the table stays on the device while the width and cut-off repeat, so
+    // a periodic shrinkwrap neither allocates nor waits for the stream
+    if (!(gauss && gauss_width == gauss_width_ && cut == gauss_cut_)) {
+        std::vector<double> g = gauss_table(gauss_width, cut);
+        gauss.alloc(g.size());
+        h2d(gauss.p, g.data(), g.size() * sizeof(double), st);
+        gauss_width_ = gauss_width;
+        gauss_cut_ = cut;
+    }
     plain::convolve(arr, tmp.p, nx, ny, gauss.p, cut, st);
     NADIA_CUDA(cudaMemcpyAsync(arr, tmp.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
 }
@@ -347,10 +377,10 @@ void Solver::set_relaxation_parameter(double b)
 void Solver::initialise_estimate(int seed)
 {
     std::vector<double> h(2 * n, 0.0);
-    srand(seed);
+    GlibcRand rnd(seed);
     if (kind == NADIA_FRESNEL) {
         for (size_t k = 0; k < n; ++k) {
-            double real = 1 - 0.2 * rand() / ((double)RAND_MAX);
+            double real = 1 - 0.2 * rnd() / ((double)RAND_MAX);
             h[2 * k] = real;
             h[2 * k + 1] = 0;
         }
@@ -375,9 +405,9 @@ void Solver::initialise_estimate(int seed)
             h[2 * k + 1] = 0;
         } else {
             // `max_value*rand()` is an int product that wraps modulo 2^32
-            int p1 = (int)((unsigned)max_value * (unsigned)rand());
+            int p1 = (int)((unsigned)max_value * (unsigned)rnd());
             double r = h_support[k] * (p1 / (double)RAND_MAX);
-            int p2 = (int)((unsigned)max_value * (unsigned)rand());
+            int p2 = (int)((unsigned)max_value * (unsigned)rnd());
             double im = h_support[k] * (p2 / (double)RAND_MAX);
             h[2 * k] = r;
             h[2 * k + 1] = im;

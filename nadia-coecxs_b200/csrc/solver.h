@@ -53,6 +53,8 @@ struct Solver {
     DevBuf<double> support, isqrt, beam_stop;
     plain::Fft2d fft;
     DevBuf<double> recon, tmp, gauss, dmax;
+    double gauss_width_ = -1; // the blur table now in `gauss`
+    int gauss_cut_ = -1;
 
     // FresnelCDI
     std::vector<double> h_illum; // detector white field x norm (interleaved)

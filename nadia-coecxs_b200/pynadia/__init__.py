@@ -41,6 +41,24 @@ _F = ctypes.POINTER(ctypes.c_float)
 _H = ctypes.c_void_p
 _I = ctypes.c_int
 
+class _Request(ctypes.Structure):
+    """struct nadia_request (include/nadia_b200.h)."""
+    _fields_ = [("kind", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                ("precision", ctypes.c_int),
+                ("intensity", _D), ("support", _D), ("beam_stop", _D),
+                ("spectrum", _D), ("nlambda", ctypes.c_int),
+                ("white_field", _D),
+                ("wavelength", ctypes.c_double), ("focal_detector_length", ctypes.c_double),
+                ("focal_sample_length", ctypes.c_double), ("pixel_size", ctypes.c_double),
+                ("normalisation", ctypes.c_double), ("fresnel_auto_norm", ctypes.c_int),
+                ("algorithm", ctypes.c_int), ("beta", ctypes.c_double),
+                ("iterations", ctypes.c_int), ("shrinkwrap_every", ctypes.c_int),
+                ("shrinkwrap_sigma", ctypes.c_double), ("shrinkwrap_threshold", ctypes.c_double),
+                ("seed", ctypes.c_int)]
+
+
+_LL = ctypes.c_longlong
+
 _PROTOS = {
     "nadia_last_error": (ctypes.c_char_p, []),
     "nadia_version": (ctypes.c_char_p, []),
@@ -79,6 +97,9 @@ _PROTOS = {
     "nadia_fresnel_auto_set_norm": (_I, [_H]),
     "nadia_fresnel_set_norm": (_I, [_H, ctypes.c_double]),
     "nadia_fresnel_get_illumination_at_sample": (_I, [_H, _D]),
+    "nadia_fresnel_set_experimental_parameters": (_I, [_H, ctypes.c_double, ctypes.c_double,
+                                                      ctypes.c_double, ctypes.c_double]),
+    "nadia_fresnel_set_normalisation": (_I, [_H, ctypes.c_double]),
     "nadia_propagate_to_detector": (_I, [_H, _D]),
     "nadia_propagate_from_detector": (_I, [_H, _D]),
     "nadia_scale_intensity": (_I, [_H, _D]),
@@ -86,12 +107,22 @@ _PROTOS = {
     "nadia_project_intensity": (_I, [_H, _D]),
     "nadia_get_intensity_autocorrelation": (_I, [_H, _D]),
     "nadia_synchronize": (_I, [_H]),
+    "nadia_fft2d": (_I, [_D, _I, _I, _I]),
     "nadia_iterate_many": (_I, [ctypes.POINTER(_H), _I, _I]),
     "nadia_get_stream": (_I, [_H, ctypes.POINTER(ctypes.c_void_p)]),
     "nadia_pass_times": (_I, [ctypes.POINTER(_H), _I, _I, _D]),
     "nadia_launch_count": (ctypes.c_longlong, []),
     "nadia_shrinkwrap_noalloc_f32": (_I, [ctypes.c_void_p, ctypes.c_void_p, _I, _I,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
+    "nadia_server_create": (_I, [ctypes.c_ulonglong, _I, _I, ctypes.POINTER(_H)]),
+    "nadia_server_submit": (_I, [_H, ctypes.POINTER(_Request), ctypes.POINTER(_LL)]),
+    "nadia_server_wait": (_I, [_H, _LL, ctypes.c_double, ctypes.POINTER(_I)]),
+    "nadia_server_result": (_I, [_H, _LL, _D, _D, _D, _D]),
+    "nadia_server_stats": (_I, [_H, ctypes.POINTER(_LL)]),
+    "nadia_server_destroy": (_I, [_H]),
+    "nadia_estimate_device_bytes": (_I, [_I, _I, _I, _I, _I, _I, _I, _I,
+                                         ctypes.POINTER(ctypes.c_ulonglong)]),
+    "nadia_device_bytes": (_LL, []),
 }
 
 _LIB = None
@@ -352,3 +383,104 @@ def shrinkwrap_noalloc_f32(esw_ptr, support_ptr, nx, ny, gauss_width=1.5, thresh
     """nadia_shrinkwrap_noalloc_f32 on device pointers (ints); queued on `stream`."""
     _check(load().nadia_shrinkwrap_noalloc_f32(esw_ptr, support_ptr, int(nx), int(ny),
                                                float(gauss_width), float(threshold), stream))
+
+
+def estimate_device_bytes(kind, nx, ny, precision=FP32, n_best=0, poly_padding=(0, 0),
+                          nlambda=0):
+    """Admission charge of one reconstruction (nadia_estimate_device_bytes)."""
+    out = ctypes.c_ulonglong()
+    k = KINDS[kind] if isinstance(kind, str) else kind
+    _check(load().nadia_estimate_device_bytes(k, nx, ny, precision, n_best, poly_padding[0],
+                                              poly_padding[1], nlambda, ctypes.byref(out)))
+    return int(out.value)
+
+
+def device_bytes():
+    """Device bytes the library's reconstructions hold now."""
+    return int(load().nadia_device_bytes())
+
+
+class Server:
+    """The request loop of nadia_server_* : submit patterns at any time,
+    collect each reconstruction when it is done."""
+
+    STATS = ("queued", "active", "completed", "failed", "bytes", "peak_bytes", "steps",
+             "admitted")
+
+    def __init__(self, budget_bytes, max_active=64, chunk=25):
+        self.lib = load()
+        self.h = _H()
+        _check(self.lib.nadia_server_create(int(budget_bytes), int(max_active), int(chunk),
+                                            ctypes.byref(self.h)))
+        self.sizes = {}
+
+    def close(self):
+        if self.h:
+            self.lib.nadia_server_destroy(self.h)
+            self.h = _H()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, kind, intensity, support, precision=FP32, beam_stop=None, spectrum=None,
+               white_field=None, wavelength=0.0, focal_detector_length=0.0,
+               focal_sample_length=0.0, pixel_size=0.0, normalisation=1.0,
+               auto_norm=False, algorithm="HIO", beta=0.9, iterations=500,
+               shrinkwrap_every=0, shrinkwrap_sigma=1.5, shrinkwrap_threshold=0.1, seed=0):
+        k = KINDS[kind] if isinstance(kind, str) else kind
+        intensity = np.ascontiguousarray(intensity, dtype=np.float64)
+        nx, ny = intensity.shape
+        support = np.ascontiguousarray(support, dtype=np.float64)
+        assert support.shape == (nx, ny)
+        keep = [intensity, support]
+        r = _Request()
+        r.kind, r.nx, r.ny, r.precision = k, nx, ny, precision
+        r.intensity, r.support = _ptr(intensity), _ptr(support)
+        if beam_stop is not None:
+            b = np.ascontiguousarray(beam_stop, dtype=np.float64)
+            keep.append(b)
+            r.beam_stop = _ptr(b)
+        if spectrum is not None:
+            sp = np.ascontiguousarray(spectrum, dtype=np.float64)
+            keep.append(sp)
+            r.spectrum, r.nlambda = _ptr(sp), sp.shape[0]
+        if white_field is not None:
+            w = np.ascontiguousarray(white_field, dtype=np.complex128)
+            keep.append(w)
+            r.white_field = w.ctypes.data_as(_D)
+        r.wavelength, r.focal_detector_length = wavelength, focal_detector_length
+        r.focal_sample_length, r.pixel_size = focal_sample_length, pixel_size
+        r.normalisation, r.fresnel_auto_norm = normalisation, int(bool(auto_norm))
+        r.algorithm = ALGORITHMS[algorithm] if isinstance(algorithm, str) else algorithm
+        r.beta, r.iterations, r.shrinkwrap_every = beta, iterations, shrinkwrap_every
+        r.shrinkwrap_sigma, r.shrinkwrap_threshold, r.seed = (shrinkwrap_sigma,
+                                                              shrinkwrap_threshold, seed)
+        rid = _LL()
+        _check(self.lib.nadia_server_submit(self.h, ctypes.byref(r), ctypes.byref(rid)))
+        self.sizes[rid.value] = (nx, ny)
+        return rid.value
+
+    def wait(self, rid, timeout=-1.0):
+        done = _I()
+        _check(self.lib.nadia_server_wait(self.h, rid, float(timeout), ctypes.byref(done)))
+        return bool(done.value)
+
+    def result(self, rid):
+        """(esw, support, final_error, times) of a finished request; times =
+        (queued, on the device, arrival to result) in seconds."""
+        nx, ny = self.sizes.pop(rid)
+        esw = np.empty((nx, ny), dtype=np.complex128)
+        sup = np.empty((nx, ny))
+        err = np.zeros(1)
+        t = np.zeros(3)
+        _check(self.lib.nadia_server_result(self.h, rid, esw.ctypes.data_as(_D), _ptr(sup),
+                                            _ptr(err), _ptr(t)))
+        return esw, sup, float(err[0]), tuple(t)
+
+    def stats(self):
+        out = (_LL * 8)()
+        _check(self.lib.nadia_server_stats(self.h, out))
+        return dict(zip(self.STATS, list(out)))

@@ -194,3 +194,29 @@ def test_spectrum_file_matches_reference_semantics(tmp_path):
     q = po.ctypes.c_int(), po.ctypes.c_int()
     po.oracle_lib().lib.orc_padding(o.h, po.ctypes.byref(q[0]), po.ctypes.byref(q[1]))
     assert (px, py) == (q[0].value, q[1].value) and px > 0
+
+
+def test_handles_of_different_sizes_coexist():
+    """A smaller FP64 handle made after a larger one leaves the larger one's
+    transforms working (the kernels' shared-memory limit is shared by all
+    handles)."""
+    big = sc.planar_inputs(256)
+    a = gpu("planar", 256, 256)
+    a.set_support(big.support)
+    a.set_intensity(big.intensity)
+    a.initialise_estimate(1)
+    b = gpu("planar", 64, 64)
+    small = sc.planar_inputs(64)
+    b.set_support(small.support)
+    b.set_intensity(small.intensity)
+    b.initialise_estimate(1)
+    a.set_algorithm(sc.HIO)
+    a.iterate(2)
+    b.iterate(2)
+    o = orc("planar", 256, 256)
+    o.set_support(big.support)
+    o.set_intensity(big.intensity)
+    o.initialise_estimate(1)
+    o.set_algorithm(sc.HIO)
+    o.iterate(2)
+    assert np.array_equal(a.get_exit_surface_wave(), o.get_exit_surface_wave())
