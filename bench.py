@@ -55,6 +55,10 @@ def parse():
     p.add_argument("--serve-requests", type=int, default=48,
                    help="requests in the saturated serving run (0 = skip serving)")
     p.add_argument("--serve-only", action="store_true", help="print the serving report only")
+    p.add_argument("--fresnel-batch", type=int, default=64,
+                   help="items in the FresnelCDI uneven-size batch report (0 = skip)")
+    p.add_argument("--fresnel-only", action="store_true",
+                   help="print the FresnelCDI batch report only")
     p.add_argument("--quick", action="store_true",
                    help="device-resident steps only (for profiling): no e2e, FP64, CPU legs")
     return p.parse_args()
@@ -315,6 +319,63 @@ def serving_report(pynadia, synth, n_req=48, n_req_fp64=12):
                     "active, steps of up to 25 iterations"}
 
 
+# ------------------------------------------------ FresnelCDI batch of uneven sizes
+
+FRESNEL_SIZES = (512, 768, 1024, 1536, 2048)
+
+
+def fresnel_batch_report(pynadia, synth, n_items=64, iters=300):
+    """64 FresnelCDI reconstructions in one nadia_iterate_many call, grids
+    drawn uniformly from {512,768,1024,1536,2048}^2 (seeded), 8 keV, sample
+    1 mm from focus, detector 1 m, 13.5 um pixels, disk objects of radius 30%
+    of the grid; one synthetic pattern per size, every item its own
+    initialise_estimate seed; 300 HIO iterations each, timed with CUDA events
+    on the batch stream."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(4)
+    sizes = [int(x) for x in rng.choice(FRESNEL_SIZES, n_items)]
+    cases = {n: synth.FresnelCase(n, seed=400 + n) for n in sorted(set(sizes))}
+    solvers = []
+    for i, n in enumerate(sizes):
+        f = cases[n]
+        s = pynadia.Solver("fresnel", n, n, precision=pynadia.FP32, white_field=f.white_field,
+                           wavelength=f.wavelength, focal_detector_length=f.zfd,
+                           focal_sample_length=f.zfs, pixel_size=f.pixel)
+        s.set_support(f.support)
+        s.set_intensity(f.intensity)
+        s.auto_set_norm()
+        s.initialise_estimate(i)
+        s.set_algorithm("HIO")
+        solvers.append(s)
+    pynadia.iterate_many(solvers, 16)       # tuning, plan, graph capture
+    for s in solvers:
+        s.synchronize()
+    st = torch.cuda.ExternalStream(solvers[0].stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    pynadia.iterate_many(solvers, iters)
+    b.record(st)
+    b.synchronize()
+    for s in solvers:
+        s.synchronize()
+    sec = a.elapsed_time(b) / 1000.0
+    px = sum(n * n for n in sizes)
+    bytes_per_iter = px * (28 + 36)          # FP32 Fresnel HIO: column 28, row 36 B/px
+    peak, peak_kind = measured_peak()
+    out = {"items": n_items, "iterations": iters,
+           "sizes": {str(n): sizes.count(n) for n in sorted(set(sizes))},
+           "total_mpx": px / 1e6, "seconds": sec, "recon_per_s": n_items / sec,
+           "hbm_gbs_algorithmic": bytes_per_iter * iters / sec / 1e9,
+           "roofline_frac": bytes_per_iter * iters / sec / 1e9 / peak,
+           "tiles": {str(n): pynadia.tuned_tiles(n, n, fresnel=True, batched=True)
+                     for n in sorted(set(sizes))},
+           "state_gb": pynadia.device_bytes() / 1e9}
+    for s in solvers:
+        s.close()
+    return out
+
+
 def phase_aligned_error(x, ref):
     import numpy as np
     inner = np.vdot(x, ref)
@@ -326,11 +387,13 @@ def ours(args, rank, world, local_rank):
     import numpy as np
     import torch
     import pynadia
-    from pynadia import synth
+    from pynadia import replicas, synth
 
     torch.cuda.set_device(local_rank)
     if args.serve_only:
         return {"serving": serving_report(pynadia, synth, n_req=args.serve_requests)}
+    if args.fresnel_only:
+        return {"fresnel_batch": fresnel_batch_report(pynadia, synth, n_items=args.fresnel_batch)}
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -378,13 +441,9 @@ def ours(args, rank, world, local_rank):
             dist.barrier()
             dist.destroy_process_group()
         return None
-    tot_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([tot_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
-        dist.barrier()
-    value = world * B * args.steps / (tot_ms / 1000.0)
+    # replicas: every rank ran its own batch; the job's time is the slowest rank's
+    tot_ms = replicas.max_over_ranks(sum(step_ms), device="cuda")
+    value = replicas.job_rate(B * args.steps, tot_ms / 1000.0, device="cuda")
     clocks = clk.summary()
 
     # ---- e2e through the C ABI with host buffers
@@ -408,12 +467,8 @@ def ours(args, rank, world, local_rank):
             out = s.get_exit_surface_wave_f32()
             errs.append(s.get_error())
         e2e_times.append(time.perf_counter() - t0)
-    e2e_s = sum(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": world * B * args.steps / e2e_s, "unit": "recon/s",
+    e2e_rate = replicas.job_rate(B * args.steps, sum(e2e_times), device="cuda")
+    e2e = {"value": e2e_rate, "unit": "recon/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
     line = None
@@ -457,6 +512,10 @@ def ours(args, rank, world, local_rank):
                 "ratio_fp32_batched_over_fp64": value / world / (1.0 / t64),
                 "note": "FP64 plain form, one reconstruction, same program, host wall clock"}
 
+        fresnel_batch = None
+        if args.fresnel_batch > 0:
+            fresnel_batch = fresnel_batch_report(pynadia, synth, n_items=args.fresnel_batch)
+
         serving = None
         if args.serve_requests > 0:
             serving = serving_report(pynadia, synth, n_req=args.serve_requests)
@@ -483,7 +542,7 @@ def ours(args, rank, world, local_rank):
                            "note": "per reconstruction in a batch = its batch's step time"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": launches, "fp64_plain": fp64, "accuracy": accuracy,
-            "serving": serving,
+            "serving": serving, "fresnel_batch": fresnel_batch,
         }
     if dist:
         dist.barrier()

@@ -326,6 +326,13 @@ int nadia_pass_times(nadia_solver *const *solvers, int count, int reps, double o
  * every kernel they contain). */
 long long nadia_launch_count(void);
 
+/* The tile variants the autotuner picked for FP32 grids of nx x ny (tuning
+ * them now, on the current GPU, if this process has not yet): one line
+ * naming the column- and row-pass variants and their timed microseconds
+ * (0 when the choice came from NADIA_TUNE=0 or a tune file).  batched != 0:
+ * the choice nadia_iterate_many uses. */
+int nadia_tuned_tiles(int nx, int ny, int fresnel, int batched, char *buf, int len);
+
 /* ---- shrinkwrap without device allocation (no counterpart in the reference)
  *
  * For callers that cannot allocate device memory when they need a support

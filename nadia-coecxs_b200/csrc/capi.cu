@@ -8,6 +8,7 @@
 
 #include "batch.h"
 #include "fused32.h"
+#include "fused32_impl.h"
 #include "server.h"
 #include "solver.h"
 
@@ -502,3 +503,22 @@ extern "C" int nadia_estimate_device_bytes(int kind, int nx, int ny, int precisi
 }
 
 extern "C" long long nadia_device_bytes(void) { return nadia::g_device_bytes.load(); }
+
+extern "C" int nadia_tuned_tiles(int nx, int ny, int fresnel, int batched, char *buf, int len)
+{
+    return guard([&] {
+        need(buf, "buf");
+        NADIA_REQUIRE(len > 0, NADIA_ERR_INVALID, "empty buffer");
+        const nadia::f32::Choice &c = nadia::f32::choose(nx, ny, fresnel != 0, batched ? 4 : 1);
+        auto desc = [](const nadia::f32::TileVariant *v) {
+            char t[160];
+            snprintf(t, sizeof t, "n=%d threads=%d signals/tile=%d radices=%s%s", v->n, v->nt,
+                     v->L, v->radices, v->persistent ? " persistent-TMA" : (v->ping ? " ping" : ""));
+            return std::string(t);
+        };
+        char t[512];
+        snprintf(t, sizeof t, "column pass: %s (%.1f us); row pass: %s (%.1f us)",
+                 desc(c.col).c_str(), c.col_us, desc(c.row).c_str(), c.row_us);
+        snprintf(buf, (size_t)len, "%s", t);
+    });
+}

@@ -123,6 +123,7 @@ _PROTOS = {
     "nadia_estimate_device_bytes": (_I, [_I, _I, _I, _I, _I, _I, _I, _I,
                                          ctypes.POINTER(ctypes.c_ulonglong)]),
     "nadia_device_bytes": (_LL, []),
+    "nadia_tuned_tiles": (_I, [_I, _I, _I, _I, ctypes.c_char_p, _I]),
 }
 
 _LIB = None
@@ -484,3 +485,11 @@ class Server:
         out = (_LL * 8)()
         _check(self.lib.nadia_server_stats(self.h, out))
         return dict(zip(self.STATS, list(out)))
+
+
+def tuned_tiles(nx, ny, fresnel=False, batched=True):
+    """The autotuner's column- and row-pass variants for an FP32 grid."""
+    buf = ctypes.create_string_buffer(512)
+    _check(load().nadia_tuned_tiles(int(nx), int(ny), int(bool(fresnel)), int(bool(batched)),
+                                    buf, 512))
+    return buf.value.decode()
