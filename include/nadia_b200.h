@@ -293,9 +293,11 @@ int nadia_server_wait(nadia_server *srv, long long id, double timeout_s, int *do
 int nadia_server_result(nadia_server *srv, long long id, double *esw, double *support,
                         double *final_error, double times[3]);
 
-/* out[8] = {queued, active, completed, failed, bytes charged now, peak bytes
- * charged, steps run, requests admitted}. */
-int nadia_server_stats(nadia_server *srv, long long out[8]);
+/* out[12] = {queued, active, completed, failed, bytes charged now, peak bytes
+ * charged, steps run, requests admitted, then host microseconds spent by the
+ * stepping thread stepping and waiting for work, and by the worker threads
+ * preparing requests and reading them back}. */
+int nadia_server_stats(nadia_server *srv, long long out[12]);
 
 /* Stops the loop (queued and unfinished requests fail) and frees the server. */
 int nadia_server_destroy(nadia_server *srv);

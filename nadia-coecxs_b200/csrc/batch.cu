@@ -118,6 +118,9 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
         std::unique_ptr<Plan> p(new Plan);
         p->key = key;
         p->st = fused[0]->st;
+        // the plan's buffers are ordered on its stream (a member's, which
+        // outlives the plan: plans go before their members' streams do)
+        AllocScope scope(p->st);
         std::map<std::tuple<int, int, int>, size_t> index;
         for (Solver *s : fused) {
             auto k = std::make_tuple(s->nx, s->ny, s->kind == NADIA_FRESNEL ? 1 : 0);
@@ -154,7 +157,6 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
                 NADIA_CUDA(cudaEventCreateWithFlags(&p->join[i], cudaEventDisableTiming));
             }
         }
-        NADIA_CUDA(cudaStreamSynchronize(p->st));
         g_plans.emplace_front(std::move(p));
         while (g_plans.size() > kMaxPlans) g_plans.pop_back();
         plan = g_plans.front().get();

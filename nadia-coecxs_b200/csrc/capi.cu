@@ -26,8 +26,13 @@ thread_local std::string g_last_error;
 template <class F>
 int guard(F &&f)
 {
+    // allocations outside a handle's call are ordered on the thread's own stream
+    struct Reset {
+        ~Reset() { nadia::t_alloc_stream = cudaStreamPerThread; }
+    } reset;
     try {
         g_last_error.clear();
+        nadia::t_alloc_stream = cudaStreamPerThread;
         f();
         return NADIA_OK;
     } catch (const Error &e) {
@@ -46,6 +51,7 @@ Solver &S(nadia_solver *h)
 {
     if (!h || !h->s) throw Error(NADIA_ERR_INVALID, "null handle");
     NADIA_CUDA(cudaSetDevice(h->s->device));
+    nadia::t_alloc_stream = h->s->st; // buffers made during the call follow its stream
     return *h->s;
 }
 
@@ -471,7 +477,7 @@ extern "C" int nadia_server_result(nadia_server *h, long long id, double *esw, d
     return guard([&] { SV(h).result(id, esw, support, final_error, times); });
 }
 
-extern "C" int nadia_server_stats(nadia_server *h, long long out[8])
+extern "C" int nadia_server_stats(nadia_server *h, long long out[12])
 {
     return guard([&] {
         need(out, "out");

@@ -39,38 +39,83 @@ struct Error : std::runtime_error {
 // Bytes currently held by DevBuf allocations of this process (all devices).
 inline std::atomic<long long> g_device_bytes{0};
 
+// Device allocations come from the device's stream-ordered memory pool.  An
+// allocation is ordered on the stream that is current for allocations on the
+// calling thread (AllocScope; otherwise the thread's per-thread stream), and
+// its release is a free ordered on that same stream: a reconstruction's
+// buffers are freed behind the last work queued on its own stream, with no
+// device-wide synchronisation (cudaFree waits for the whole device, which
+// would stall every other reconstruction sharing the GPU).  A buffer is
+// usable on any stream once alloc returns.  Rule for temporaries allocated
+// outside a scope: release them only after the work that uses them is done.
+inline thread_local cudaStream_t t_alloc_stream = cudaStreamPerThread;
+
+struct AllocScope {
+    cudaStream_t saved;
+    explicit AllocScope(cudaStream_t s) : saved(t_alloc_stream) { t_alloc_stream = s; }
+    ~AllocScope() { t_alloc_stream = saved; }
+    AllocScope(const AllocScope &) = delete;
+    AllocScope &operator=(const AllocScope &) = delete;
+};
+
+// keep freed pool memory for reuse instead of returning it to the driver
+void retain_pool_memory();
+
 // Owning device allocation.
 template <class T>
 struct DevBuf {
     T *p = nullptr;
     size_t n = 0;
+    cudaStream_t st = nullptr; // the stream its allocation and release are ordered on
     DevBuf() = default;
     explicit DevBuf(size_t count) { alloc(count); }
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
-    DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n), st(o.st) { o.p = nullptr; o.n = 0; }
     DevBuf &operator=(DevBuf &&o) noexcept
     {
-        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        if (this != &o) {
+            release();
+            p = o.p; n = o.n; st = o.st;
+            o.p = nullptr; o.n = 0;
+        }
         return *this;
     }
     ~DevBuf() { release(); }
     void alloc(size_t count)
     {
         release();
-        if (count) NADIA_CUDA(cudaMalloc((void **)&p, count * sizeof(T)));
+        if (count) {
+            retain_pool_memory();
+            st = t_alloc_stream;
+            NADIA_CUDA(cudaMallocAsync((void **)&p, count * sizeof(T), st));
+            NADIA_CUDA(cudaStreamSynchronize(st));
+        }
         n = count;
         g_device_bytes += (long long)(n * sizeof(T));
     }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, st);
         g_device_bytes -= (long long)(n * sizeof(T));
         p = nullptr;
         n = 0;
     }
     size_t bytes() const { return n * sizeof(T); }
     explicit operator bool() const { return p != nullptr; }
+};
+
+// A stream owned by an object whose buffers are ordered on it: declared
+// before those buffers, so it outlives their releases.
+struct OwnedStream {
+    cudaStream_t s = nullptr;
+    OwnedStream() = default;
+    OwnedStream(const OwnedStream &) = delete;
+    OwnedStream &operator=(const OwnedStream &) = delete;
+    ~OwnedStream()
+    {
+        if (s) cudaStreamDestroy(s);
+    }
 };
 
 // Host-to-device copy that has landed when it returns.  A plain cudaMemcpy

@@ -177,16 +177,20 @@ struct Dft<5, FWD> {
 };
 
 // Good-Thomas prime-factor DFT for R = A*B with gcd(A,B) = 1 (no twiddles):
-// input n = (B n1 + A n2) mod R, output k with k = k1 (mod A), k = k2 (mod B).
-constexpr int crt_index(int k1, int k2, int A, int B)
+// input n = (B n1 + A n2) mod R, output k with k = k1 (mod A), k = k2 (mod B),
+// that is k = (k1 e1 + k2 e2) mod R with e1 = 1 (mod A), 0 (mod B) and
+// e2 = 0 (mod A), 1 (mod B).  The indices are plain arithmetic on unrolled
+// loop counters, so every access of v resolves to a register.
+constexpr int crt_unit(int A, int B) // the multiple of B that is 1 modulo A
 {
-    int k = 0;
-    while (!(k % A == k1 && k % B == k2)) ++k;
-    return k;
+    int e = B;
+    while (e % A != 1) e += B;
+    return e;
 }
 
 template <int A, int B, bool FWD>
 struct Pfa {
+    static constexpr int E1 = crt_unit(A, B), E2 = crt_unit(B, A);
     static __device__ __forceinline__ void run(float2 *v)
     {
         constexpr int R = A * B;
@@ -207,7 +211,7 @@ struct Pfa {
             for (int n2 = 0; n2 < B; ++n2) u[n2] = t[n2][k1];
             Dft<B, FWD>::run(u);
 #pragma unroll
-            for (int k2 = 0; k2 < B; ++k2) v[crt_index(k1, k2, A, B)] = u[k2];
+            for (int k2 = 0; k2 < B; ++k2) v[(k1 * E1 + k2 * E2) % R] = u[k2];
         }
     }
 };

@@ -589,13 +589,6 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots)
 
 using namespace f32;
 
-namespace {
-inline size_t panel_index(int x, int y, int nx)
-{
-    return ((size_t)(y / kPanel) * nx + x) * kPanel + (y % kPanel);
-}
-} // namespace
-
 Fused32::Fused32(Solver &s) : impl(new Impl(s)) {}
 Fused32::~Fused32() { delete impl; }
 
@@ -604,17 +597,22 @@ Fused32::Impl::Impl(Solver &s) : S(s)
     nx = s.nx;
     ny = s.ny;
     n = s.n;
-    NADIA_REQUIRE(supported(nx) && supported(ny), NADIA_ERR_UNSUPPORTED,
-                  "the FP32 form supports grid sizes 256, 512, 768, 1024, 1536, 2048 and 4096 "
-                  "per axis; use NADIA_FP64 for other sizes");
-    NADIA_REQUIRE(s.kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
-                  "PolyCDI runs in the FP64 form");
-    choice = &choose(nx, ny, s.kind == NADIA_FRESNEL, 1);
+    const bool poly = s.kind == NADIA_POLY;
+    if (poly) {
+        // the transforms run on the padded grid, sized by set_spectrum
+        NADIA_REQUIRE(nx % 8 == 0 && ny % 4 == 0, NADIA_ERR_UNSUPPORTED,
+                      "the FP32 PolyCDI form needs nx a multiple of 8 and ny of 4");
+    } else {
+        NADIA_REQUIRE(supported(nx) && supported(ny), NADIA_ERR_UNSUPPORTED,
+                      "the FP32 form supports grid sizes 256, 512, 768, 1024, 1536, 2048 and "
+                      "4096 per axis; use NADIA_FP64 for other sizes");
+        choice = &choose(nx, ny, s.kind == NADIA_FRESNEL, 1);
+    }
     P.alloc(n);
     x.alloc(n);
     sup.alloc(n);
     mI.alloc(n);
-    ncol = ny / choice->col->L;
+    ncol = poly ? 0 : ny / choice->col->L;
     partials.alloc(ny / kPanel);
     iter.alloc(1);
     flag.alloc(1);
@@ -628,8 +626,10 @@ Fused32::Impl::Impl(Solver &s) : S(s)
     NADIA_CUDA(cudaMemsetAsync(partials.p, 0, partials.bytes(), st));
     NADIA_CUDA(cudaMemsetAsync(iter.p, 0, iter.bytes(), st));
     NADIA_CUDA(cudaMemsetAsync(flag.p, 0, flag.bytes(), st));
-    twx = twiddle_table(nx);
-    twy = twiddle_table(ny);
+    if (!poly) {
+        twx = twiddle_table(nx);
+        twy = twiddle_table(ny);
+    }
     h_slot = Slot{};
     h_slot.P = P.p;
     h_slot.x = x.p;
@@ -644,7 +644,7 @@ Fused32::Impl::Impl(Solver &s) : S(s)
     h_slot.s0 = (float)(1.0 / sqrt((double)nx * (double)ny));
     h_slot.inv_norm2 = 0.0;
     h_slot.flag = flag.p;
-    encode_tensor_maps(h_slot, nx, ny);
+    if (!poly) encode_tensor_maps(h_slot, nx, ny);
     Slot *sp = slot.p;
     NADIA_CUDA(cudaMemcpyAsync(slot_ptr.p, &sp, sizeof(Slot *), cudaMemcpyHostToDevice, st));
     push_slot();
@@ -679,37 +679,91 @@ void Fused32::Impl::push_slot_async(cudaStream_t st)
     NADIA_CUDA(cudaMemcpyAsync(slot.p, &h_slot, sizeof(Slot), cudaMemcpyHostToDevice, st));
 }
 
-void Fused32::Impl::to_panel(const double *h, size_t stride, std::vector<float> &out) const
+// Host arrays are in the reference's order (element (x, y) at x*ny + y); the
+// device arrays in the panel layout.  The conversion runs on the GPU through
+// a staging buffer, so the host only converts doubles to floats in order.
+namespace {
+template <int ST>
+__global__ void k_natural_to_panel(const float *__restrict__ src, float *__restrict__ dst, int nx,
+                                   int ny, int fold)
 {
-    out.resize(n * stride);
-    for (int xx = 0; xx < nx; ++xx)
-        for (int yy = 0; yy < ny; ++yy) {
-            size_t a = panel_index(xx, yy, nx), b = (size_t)xx * ny + yy;
-            for (size_t c = 0; c < stride; ++c) out[a * stride + c] = (float)h[b * stride + c];
+    const size_t n = (size_t)nx * ny;
+    for (size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x; a < n;
+         a += (size_t)gridDim.x * blockDim.x) {
+        const size_t t = a / kPanel;
+        const int kx = (int)(t % nx), ky = (int)(t / nx) * kPanel + (int)(a % kPanel);
+        int dx = kx, dy = ky;
+        if (fold) {
+            dx = kx + nx / 2;
+            dx = dx >= nx ? dx - nx : dx;
+            dy = ky + ny / 2;
+            dy = dy >= ny ? dy - ny : dy;
         }
+        const size_t d = (size_t)dx * ny + dy;
+#pragma unroll
+        for (int c = 0; c < ST; ++c) dst[a * ST + c] = src[d * ST + c];
+    }
 }
 
-void Fused32::Impl::from_panel(const std::vector<float> &in, size_t stride, double *h) const
+template <int ST>
+__global__ void k_panel_to_natural(const float *__restrict__ src, float *__restrict__ dst, int nx,
+                                   int ny)
 {
-    for (int xx = 0; xx < nx; ++xx)
-        for (int yy = 0; yy < ny; ++yy) {
-            size_t a = panel_index(xx, yy, nx), b = (size_t)xx * ny + yy;
-            for (size_t c = 0; c < stride; ++c) h[b * stride + c] = in[a * stride + c];
-        }
+    const size_t n = (size_t)nx * ny;
+    for (size_t d = blockIdx.x * (size_t)blockDim.x + threadIdx.x; d < n;
+         d += (size_t)gridDim.x * blockDim.x) {
+        const int xx = (int)(d / ny), yy = (int)(d % ny);
+        const size_t a = panel_index_dev(xx, yy, nx);
+#pragma unroll
+        for (int c = 0; c < ST; ++c) dst[d * ST + c] = src[a * ST + c];
+    }
+}
+} // namespace
+
+void Fused32::Impl::ensure_stage()
+{
+    if (!stage) stage.alloc(n);
 }
 
-void Fused32::Impl::upload(void *dst, const std::vector<float> &v)
+void Fused32::Impl::put_panel_f(const float *h, int stride, void *dst, bool fold)
 {
-    NADIA_CUDA(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice,
+    ensure_stage();
+    NADIA_CUDA(cudaMemcpyAsync(stage.p, h, n * stride * sizeof(float), cudaMemcpyHostToDevice,
                                S.st));
+    const float *src = reinterpret_cast<const float *>(stage.p);
+    if (stride == 1)
+        k_natural_to_panel<1><<<grid1(n), 256, 0, S.st>>>(src, (float *)dst, nx, ny, fold);
+    else
+        k_natural_to_panel<2><<<grid1(n), 256, 0, S.st>>>(src, (float *)dst, nx, ny, fold);
+    g_launches += 1;
     NADIA_CUDA(cudaStreamSynchronize(S.st));
 }
 
-void Fused32::Impl::download(std::vector<float> &v, const void *src, size_t count)
+void Fused32::Impl::put_panel(const double *h, int stride, void *dst, bool fold)
 {
-    v.resize(count);
-    NADIA_CUDA(cudaMemcpyAsync(v.data(), src, count * sizeof(float), cudaMemcpyDeviceToHost, S.st));
+    std::vector<float> f(n * stride);
+    for (size_t k = 0; k < f.size(); ++k) f[k] = (float)h[k];
+    put_panel_f(f.data(), stride, dst, fold);
+}
+
+void Fused32::Impl::get_panel_f(const void *src, int stride, float *h)
+{
+    ensure_stage();
+    float *d = reinterpret_cast<float *>(stage.p);
+    if (stride == 1)
+        k_panel_to_natural<1><<<grid1(n), 256, 0, S.st>>>((const float *)src, d, nx, ny);
+    else
+        k_panel_to_natural<2><<<grid1(n), 256, 0, S.st>>>((const float *)src, d, nx, ny);
+    g_launches += 1;
+    NADIA_CUDA(cudaMemcpyAsync(h, d, n * stride * sizeof(float), cudaMemcpyDeviceToHost, S.st));
     NADIA_CUDA(cudaStreamSynchronize(S.st));
+}
+
+void Fused32::Impl::get_panel(const void *src, int stride, double *h)
+{
+    std::vector<float> f(n * stride);
+    get_panel_f(src, stride, f.data());
+    for (size_t k = 0; k < f.size(); ++k) h[k] = f[k];
 }
 
 // sqrt(I) in transform order with the unmeasured pixels marked -1; the
@@ -718,17 +772,16 @@ void Fused32::Impl::upload_intensity()
 {
     std::vector<float> m(n);
     double norm2 = 0;
-    const bool planar = S.kind == NADIA_PLANAR;
-    for (int kx = 0; kx < nx; ++kx)
-        for (int ky = 0; ky < ny; ++ky) {
-            int dx = planar ? (kx + nx / 2) % nx : kx, dy = planar ? (ky + ny / 2) % ny : ky;
-            size_t d = (size_t)dx * ny + dy;
-            bool measured = !S.has_beam_stop || h_bs[d] > 0;
-            float v = (float)S.h_isqrt[d];
-            if (measured) norm2 += (double)v * (double)v;
-            m[panel_index(kx, ky, nx)] = measured ? v : -1.f;
-        }
-    upload(mI.p, m);
+    for (size_t d = 0; d < n; ++d) {
+        const bool measured = !S.has_beam_stop || h_bs[d] > 0;
+        const float v = (float)S.h_isqrt[d];
+        if (measured) norm2 += (double)v * (double)v;
+        m[d] = measured ? v : -1.f;
+    }
+    // PlanarCDI's detector is centred (Complex_2D::invert): fold it into
+    // transform order; Fresnel folds the swap into its phase factors, and
+    // PolyCDI gathers in centred coordinates
+    put_panel_f(m.data(), 1, mI.p, S.kind == NADIA_PLANAR);
     h_slot.inv_norm2 = 1.0 / norm2;
     push_slot();
 }
@@ -741,12 +794,7 @@ void Fused32::upload_beam_stop(const double *mask)
     impl->upload_intensity();
 }
 
-void Fused32::upload_support(const double *h)
-{
-    std::vector<float> f;
-    impl->to_panel(h, 1, f);
-    impl->upload(impl->sup.p, f);
-}
+void Fused32::upload_support(const double *h) { impl->put_panel(h, 1, impl->sup.p, false); }
 
 void Fused32::soften_support()
 {
@@ -757,16 +805,13 @@ void Fused32::soften_support()
     impl->S.sync();
 }
 
-void Fused32::set_spectrum() { throw Error(NADIA_ERR_UNSUPPORTED, "PolyCDI runs in the FP64 form"); }
 
 void Fused32::upload_illumination()
 {
     Impl &I = *impl;
     I.W.alloc(I.n);
     I.ill.alloc(I.n);
-    std::vector<float> f;
-    I.to_panel(I.S.h_illum.data(), 2, f);
-    I.upload(I.W.p, f);
+    I.put_panel(I.S.h_illum.data(), 2, I.W.p, false);
     I.h_slot.W = I.W.p;
     I.push_slot();
 }
@@ -817,9 +862,7 @@ void Fused32::set_fresnel_geometry(double factor)
     std::vector<double> h(2 * I.n);
     NADIA_CUDA(cudaMemcpyAsync(h.data(), c.p, c.bytes(), cudaMemcpyDeviceToHost, S.st));
     NADIA_CUDA(cudaStreamSynchronize(S.st));
-    std::vector<float> f;
-    I.to_panel(h.data(), 2, f);
-    I.upload(I.ill.p, f);
+    I.put_panel(h.data(), 2, I.ill.p, false);
 }
 
 void Fused32::scale_illumination(double f)
@@ -841,73 +884,38 @@ void Fused32::fresnel_initialise(const double *t)
 void Fused32::fresnel_set_transmission(const double *t)
 {
     Impl &I = *impl;
-    std::vector<float> f;
-    I.to_panel(t, 2, f);
-    DevBuf<float2> d(I.n);
-    I.upload(d.p, f);
-    k_fresnel_set_t<<<grid1(I.n), 256, 0, I.S.st>>>(d.p, I.ill.p, I.x.p, I.nx, I.ny);
-    I.S.sync();
+    // the work array holds T for the moment; the next iteration rebuilds it
     I.p_valid = false;
+    I.put_panel(t, 2, I.P.p, false);
+    k_fresnel_set_t<<<grid1(I.n), 256, 0, I.S.st>>>(I.P.p, I.ill.p, I.x.p, I.nx, I.ny);
+    I.S.sync();
 }
 
 void Fused32::fresnel_get_transmission(double *t)
 {
     Impl &I = *impl;
-    DevBuf<float2> d(I.n);
-    k_fresnel_get_t<<<grid1(I.n), 256, 0, I.S.st>>>(I.x.p, I.ill.p, d.p, I.n);
-    std::vector<float> f;
-    I.download(f, d.p, 2 * I.n);
-    I.from_panel(f, 2, t);
+    I.p_valid = false; // T is formed in the work array
+    k_fresnel_get_t<<<grid1(I.n), 256, 0, I.S.st>>>(I.x.p, I.ill.p, I.P.p, I.n);
+    I.get_panel(I.P.p, 2, t);
 }
 
-void Fused32::get_illumination_at_sample(double *h)
-{
-    std::vector<float> f;
-    impl->download(f, impl->ill.p, 2 * impl->n);
-    impl->from_panel(f, 2, h);
-}
+void Fused32::get_illumination_at_sample(double *h) { impl->get_panel(impl->ill.p, 2, h); }
 
 void Fused32::set_x(const double *h)
 {
-    std::vector<float> f;
-    impl->to_panel(h, 2, f);
-    impl->upload(impl->x.p, f);
+    impl->put_panel(h, 2, impl->x.p, false);
     impl->p_valid = false;
 }
 
-void Fused32::get_x(double *h)
-{
-    std::vector<float> f;
-    impl->download(f, impl->x.p, 2 * impl->n);
-    impl->from_panel(f, 2, h);
-}
+void Fused32::get_x(double *h) { impl->get_panel(impl->x.p, 2, h); }
 
 void Fused32::set_x_f32(const float *h)
 {
-    Impl &I = *impl;
-    std::vector<float> f(2 * I.n);
-    for (int xx = 0; xx < I.nx; ++xx)
-        for (int yy = 0; yy < I.ny; ++yy) {
-            size_t a = panel_index(xx, yy, I.nx), b = (size_t)xx * I.ny + yy;
-            f[2 * a] = h[2 * b];
-            f[2 * a + 1] = h[2 * b + 1];
-        }
-    I.upload(I.x.p, f);
-    I.p_valid = false;
+    impl->put_panel_f(h, 2, impl->x.p, false);
+    impl->p_valid = false;
 }
 
-void Fused32::get_x_f32(float *h)
-{
-    Impl &I = *impl;
-    std::vector<float> f;
-    I.download(f, I.x.p, 2 * I.n);
-    for (int xx = 0; xx < I.nx; ++xx)
-        for (int yy = 0; yy < I.ny; ++yy) {
-            size_t a = panel_index(xx, yy, I.nx), b = (size_t)xx * I.ny + yy;
-            h[2 * b] = f[2 * a];
-            h[2 * b + 1] = f[2 * a + 1];
-        }
-}
+void Fused32::get_x_f32(float *h) { impl->get_panel_f(impl->x.p, 2, h); }
 
 // n-best copies are kept in the natural layout so get_best_result can
 // download them directly
@@ -951,6 +959,10 @@ void Fused32::Impl::launch_iteration(cudaStream_t st)
 void Fused32::iterate(int count)
 {
     Impl &I = *impl;
+    if (I.S.kind == NADIA_POLY) {
+        iterate_poly(count);
+        return;
+    }
     I.check_algorithm();
     I.use_choice(I.choice);
     I.push_slot();
@@ -1058,12 +1070,7 @@ void Fused32::check_device_flag()
     }
 }
 
-void Fused32::get_support(double *h)
-{
-    std::vector<float> f;
-    impl->download(f, impl->sup.p, impl->n);
-    impl->from_panel(f, 1, h);
-}
+void Fused32::get_support(double *h) { impl->get_panel(impl->sup.p, 1, h); }
 
 void Fused32::single_op(int, double *)
 {

@@ -30,6 +30,7 @@ public:
     void get_x_f32(float *h);
     void copy_x_to(float2 *dst);
     void iterate(int count);
+    void iterate_poly(int count);
     void shrinkwrap(double gauss_width, double threshold);
     void get_support(double *h);
     void single_op(int op, double *field);

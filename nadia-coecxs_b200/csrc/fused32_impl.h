@@ -39,6 +39,15 @@ struct alignas(64) Slot {
     float s0;               // 1/sqrt(nx*ny)
     double inv_norm2;       // 1 / sum of sqrt(I)^2 over measured pixels
     int *flag;              // raised when a device-side wait gives up
+    // PolyCDI: P is the padded mx x my grid (the estimate sits at rows
+    // px..px+nx-1, columns py..py+ny-1); q holds |Psi|^2 of the padded
+    // detector field in centred coordinates (panel layout over mx rows);
+    // gx/gy[l][i] are the rows/columns sampled for wavelength l at unpadded
+    // row/column i (-1: outside the grid); wl[l] the normalised weights
+    float *q;
+    const int *gx, *gy;
+    const float *wl;
+    int nl, px, py, mx, my;
 };
 
 struct Gauss {
@@ -79,6 +88,23 @@ struct TileVariant {
     RowLaunch row = nullptr;
 };
 
+// PolyCDI passes of one tile shape: forward column transform of the padded
+// grid (writes Psi and |Psi|^2), modulus against the wavelength-expanded
+// intensity plus inverse column transform, and the row pass over the
+// estimate's rows of the padded grid.
+using PolyLaunch = void (*)(const Slot *const *slots, int nslots, int tiles, cudaStream_t st,
+                            const float2 *tw);
+using PolyRowLaunch = void (*)(int mode, const Slot *const *slots, int nslots, int tiles,
+                               cudaStream_t st, const float2 *tw);
+struct PolyVariant {
+    int n = 0, nt = 0, L = 0;
+    const char *radices = "";
+    void (*prepare)() = nullptr;
+    PolyLaunch col_fwd = nullptr, col_inv = nullptr;
+    PolyRowLaunch row = nullptr;
+};
+const std::vector<PolyVariant> &poly_variants(int n);
+
 // the variants of a transform length (empty when the length has none)
 const std::vector<TileVariant> &variants(int n);
 bool supported(int n);
@@ -105,7 +131,7 @@ struct Fused32::Impl {
     Solver &S;
     int nx = 0, ny = 0, ncol = 0;
     size_t n = 0;
-    DevBuf<float2> P, x, W, ill, tx, ty;
+    DevBuf<float2> P, x, W, ill, tx, ty, stage;
     DevBuf<float> sup, mI, tmp1, tmp2, maxpart;
     DevBuf<double> partials;
     DevBuf<long long> iter;
@@ -117,6 +143,11 @@ struct Fused32::Impl {
     const f32::Choice *choice = nullptr;
     std::vector<double> h_bs;
     bool p_valid = false;
+    // PolyCDI
+    int mx = 0, my = 0, pcols = 0;
+    DevBuf<float> q, wl;
+    DevBuf<int> gx, gy;
+    const f32::PolyVariant *pcol = nullptr, *prow = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
 
     explicit Impl(Solver &s);
@@ -126,10 +157,14 @@ struct Fused32::Impl {
     // the variants the next launches use (the handle's own, or a batch's);
     // sets the column-block count the row pass sums over
     void use_choice(const f32::Choice *c);
-    void to_panel(const double *h, size_t stride, std::vector<float> &out) const;
-    void from_panel(const std::vector<float> &in, size_t stride, double *h) const;
-    void upload(void *dst, const std::vector<float> &v);
-    void download(std::vector<float> &v, const void *src, size_t count);
+    // host arrays in the reference's order <-> device arrays in the panel
+    // layout (stride 1: real, 2: complex; fold: PlanarCDI's centred detector
+    // to transform order), converted on the device through `stage`
+    void ensure_stage();
+    void put_panel(const double *h, int stride, void *dst, bool fold);
+    void put_panel_f(const float *h, int stride, void *dst, bool fold);
+    void get_panel(const void *src, int stride, double *h);
+    void get_panel_f(const void *src, int stride, float *h);
     void upload_intensity();
     void blur(bool cplx, const void *in, double gauss_width, int cut);
     int blur_blocks() const;

@@ -3,13 +3,14 @@
 //
 // Admission is in arrival order: a request waits while the slot limit or
 // the HBM budget would be exceeded, and later ones wait behind it.  Admitted
-// requests are prepared by a few preparing threads (device buffers, inputs,
+// requests are prepared by host worker threads (device buffers, inputs,
 // initial estimate, each on the reconstruction's own stream) and handed to
 // the stepping thread, which steps every active reconstruction together with
 // iterate_many for the same number of iterations: the chunk size, shortened
 // so that no request passes its next shrinkwrap or its last iteration.
-// Finished requests are copied out and their device memory released, which
-// frees their slot and budget for the next admission; arrivals therefore
+// Finished requests go back to the worker threads, which copy them out and
+// release their device memory, freeing their slot and budget for the next
+// admission; arrivals therefore
 // overlap with the work of the requests already on the GPU.
 //
 // Every request is stepped only through iterate_many, whose tile choice does
@@ -44,20 +45,26 @@ size_t footprint_bytes(int kind, int nx, int ny, int prec, int n_best, int pad_n
             b += 16 * (size_t)nlambda + 16 * (size_t)pad_nx * pad_ny + 8 * n +
                  16 * (size_t)(pad_nx + pad_ny);
     } else {
-        b += n * (8 + 8 + 4 + 4);                     // P, x, support, sqrt(I)
+        b += n * (8 + 8 + 4 + 4 + 8);                 // P, x, support, sqrt(I), staging
         b += 8 * (size_t)(ny / 4) + 8 + 4 + 2 * 8;    // partials, counter, flag, slot pointer
         b += sizeof(f32::Slot);
         const size_t tiles = ((size_t)(nx + 31) / 32) * ((ny + 31) / 32);
         b += 2 * 4 * n + 4 * (std::max<size_t>(tiles, 592) + 2); // shrinkwrap scratch
         b += (size_t)n_best * 8 * n;
         if (kind == NADIA_FRESNEL) b += 8 * n + 8 * n + 8 * (size_t)(nx + ny);
+        if (kind == NADIA_POLY) {
+            const size_t m = (size_t)pad_nx * pad_ny;
+            b += 8 * m + 4 * m;                                  // padded work array, |Psi|^2
+            b += 4 * (size_t)nlambda * (nx + ny + 1);            // gather tables, weights
+            b += 8 * (size_t)(pad_ny / 8 + 1);                   // column-tile partials
+        }
     }
     return b;
 }
 
 namespace {
 
-constexpr int kPreparers = 4; // threads preparing admitted requests
+constexpr int kPreparers = 8; // host worker threads (prepare and read back requests)
 
 // PolyCDI's padding from its spectrum (PolyCDI.c++:66-89)
 void poly_padding(const double *sp, int nl, int nx, int ny, int *px, int *py)
@@ -105,12 +112,14 @@ Server::~Server()
     for (auto &t : preparers_)
         if (t.joinable()) t.join();
     if (worker_.joinable()) worker_.join();
-    // what never reached the stepping thread
+    // what never reached the stepping thread or its readback
     std::vector<Record *> left;
     {
         std::lock_guard<std::mutex> lk(mu_);
         left.assign(ready_.begin(), ready_.end());
+        left.insert(left.end(), done_.begin(), done_.end());
         ready_.clear();
+        done_.clear();
     }
     for (Record *r : left) fail(*r, NADIA_ERR_STATE, "the server stopped");
 }
@@ -201,9 +210,13 @@ void Server::result(long long id, double *esw, double *support, double *final_er
     if (final_error) *final_error = r->final_error;
 }
 
-void Server::stats(long long out[8])
+void Server::stats(long long out[12])
 {
     std::lock_guard<std::mutex> lk(mu_);
+    out[8] = us_step_;
+    out[9] = us_idle_;
+    out[10] = us_prepare_;
+    out[11] = us_readback_;
     out[0] = (long long)queue_.size();
     out[1] = slots_;
     out[2] = completed_;
@@ -228,6 +241,7 @@ void Server::start(Record &r)
     const nadia_request &q = r.req;
     r.solver.reset(new Solver(q.kind, q.nx, q.ny, q.precision, 0));
     Solver &s = *r.solver;
+    AllocScope scope(s.st);
     if (q.kind == NADIA_FRESNEL)
         s.fresnel_init(r.white_field.data(), q.wavelength, q.focal_detector_length,
                        q.focal_sample_length, q.pixel_size, q.normalisation);
@@ -250,6 +264,7 @@ void Server::start(Record &r)
 void Server::finish(Record &r)
 {
     Solver &s = *r.solver;
+    AllocScope scope(s.st);
     r.final_error = s.get_error();
     r.esw.resize(2 * s.n);
     s.get_esw(r.esw.data());
@@ -293,16 +308,44 @@ bool Server::can_admit() const
            bytes_in_use_ + queue_.front()->bytes <= budget_;
 }
 
-// preparing thread: admit the next request that fits, build it, hand it over
+// worker thread: read back a finished request, or admit the next request
+// that fits, build it and hand it to the stepping thread
 void Server::prepare_loop()
 {
     cudaSetDevice(device_);
     for (;;) {
         Record *r = nullptr;
+        bool readback = false;
         {
             std::unique_lock<std::mutex> lk(mu_);
-            cv_admit_.wait(lk, [&] { return stop_ || can_admit(); });
+            cv_admit_.wait(lk, [&] { return stop_ || !done_.empty() || can_admit(); });
             if (stop_) return;
+            if (!done_.empty()) { // finishing first: it frees a slot and budget
+                r = done_.front();
+                done_.pop_front();
+                readback = true;
+            }
+        }
+        if (readback) {
+            const double t0 = now();
+            try {
+                finish(*r);
+            } catch (const Error &e) {
+                fail(*r, e.code, e.what());
+            } catch (const std::exception &e) {
+                fail(*r, NADIA_ERR_CUDA, e.what());
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                us_readback_ += (long long)(1e6 * (now() - t0));
+            }
+            cv_done_.notify_all();
+            continue;
+        }
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            if (stop_) return;
+            if (!can_admit()) continue;
             r = queue_.front();
             queue_.pop_front();
             bytes_in_use_ += r->bytes;
@@ -312,7 +355,8 @@ void Server::prepare_loop()
             r->t_admit = now();
             ++admitted_;
         }
-        cv_admit_.notify_all(); // another preparer may admit the next one
+        cv_admit_.notify_all(); // another worker may admit the next one
+        const double t0 = now();
         try {
             start(*r);
         } catch (const Error &e) {
@@ -324,6 +368,7 @@ void Server::prepare_loop()
         }
         {
             std::lock_guard<std::mutex> lk(mu_);
+            us_prepare_ += (long long)(1e6 * (now() - t0));
             ready_.push_back(r);
         }
         cv_ready_.notify_all();
@@ -337,7 +382,9 @@ void Server::run()
     for (;;) {
         {
             std::unique_lock<std::mutex> lk(mu_);
+            const double t0 = now();
             if (active_.empty()) cv_ready_.wait(lk, [&] { return stop_ || !ready_.empty(); });
+            us_idle_ += (long long)(1e6 * (now() - t0));
             if (stop_) break;
             active_.insert(active_.end(), ready_.begin(), ready_.end());
             ready_.clear();
@@ -351,24 +398,27 @@ void Server::run()
             handles.push_back(r->solver.get());
         }
         std::vector<Record *> keep;
+        const double t0 = now();
         try {
             if (c > 0) iterate_many(handles.data(), (int)handles.size(), c);
-            {
-                std::lock_guard<std::mutex> lk(mu_);
-                ++steps_;
-            }
             for (Record *r : active_) {
                 r->done_iters += c;
                 const int k = r->req.shrinkwrap_every;
                 if (k > 0 && r->done_iters % k == 0 && c > 0)
                     r->solver->apply_shrinkwrap(r->req.shrinkwrap_sigma, r->req.shrinkwrap_threshold);
             }
-            for (Record *r : active_) {
-                if (r->done_iters >= r->req.iterations)
-                    finish(*r);
-                else
-                    keep.push_back(r);
+            // finished requests go to the worker threads for their readback
+            // (which waits for their streams) while this thread steps the rest
+            std::vector<Record *> finished;
+            for (Record *r : active_)
+                (r->done_iters >= r->req.iterations ? finished : keep).push_back(r);
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                ++steps_;
+                us_step_ += (long long)(1e6 * (now() - t0));
+                done_.insert(done_.end(), finished.begin(), finished.end());
             }
+            if (!finished.empty()) cv_admit_.notify_all();
         } catch (const Error &e) {
             // a failure inside a shared step fails every request in it
             for (Record *r : active_)

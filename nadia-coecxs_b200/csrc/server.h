@@ -2,9 +2,10 @@
 // diffraction patterns arrive at any time, are admitted while an HBM budget
 // and a slot limit allow, keep their estimate, support and intensity resident
 // on the device, and step together (iterate_many) until each has run its
-// iterations; results wait on the host until collected.  A few preparing
+// iterations; results wait on the host until collected.  A few host worker
 // threads build admitted reconstructions (device buffers, inputs, initial
-// estimate) while one stepping thread keeps the GPU busy with the others.
+// estimate) and read finished ones back, while one stepping thread keeps the
+// GPU busy with the others.
 #pragma once
 
 #include <chrono>
@@ -38,7 +39,7 @@ public:
     // own error if it failed
     void result(long long id, double *esw, double *support, double *final_error,
                 double times[3]);
-    void stats(long long out[8]);
+    void stats(long long out[12]);
 
 private:
     enum State { QUEUED, ACTIVE, DONE, FAILED };
@@ -75,11 +76,15 @@ private:
     std::condition_variable cv_admit_, cv_ready_, cv_done_;
     std::deque<Record *> queue_;                           // submitted, not admitted
     std::vector<Record *> ready_;                          // admitted and prepared
+    std::deque<Record *> done_;    // iterations queued, waiting for their readback
     std::map<long long, std::unique_ptr<Record>> records_;
     std::vector<Record *> active_; // stepped; touched by the stepping thread only
     int slots_ = 0;                // admitted and not yet finished
     size_t bytes_in_use_ = 0, peak_bytes_ = 0;
     long long next_id_ = 1, completed_ = 0, failed_ = 0, steps_ = 0, admitted_ = 0;
+    // host microseconds: stepping thread stepping / waiting for work; worker
+    // threads preparing / reading back
+    long long us_step_ = 0, us_idle_ = 0, us_prepare_ = 0, us_readback_ = 0;
     bool stop_ = false;
     std::thread worker_;
     std::vector<std::thread> preparers_;

@@ -6,6 +6,7 @@
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "batch.h"
 #include "fused32.h"
@@ -14,6 +15,22 @@ namespace nadia {
 
 namespace {
 std::atomic<unsigned long long> g_uid{1};
+std::mutex g_pool_mu;
+bool g_pool_set[64] = {};
+} // namespace
+
+void retain_pool_memory()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (g_pool_set[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = ~(uint64_t)0;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    g_pool_set[dev] = true;
 }
 
 namespace {
@@ -78,6 +95,8 @@ Solver::Solver(int kind_, int nx_, int ny_, int prec_, int n_best_)
     uid = g_uid++;
     NADIA_CUDA(cudaGetDevice(&device));
     NADIA_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    own_st.s = st;
+    AllocScope scope(st); // this reconstruction's buffers are ordered on its stream
     h_isqrt.assign(n, 0.0);
     h_support.assign(n, 0.0);
     d_err.alloc(1);
@@ -121,12 +140,14 @@ Solver::~Solver()
     if (st) {
         cudaStreamSynchronize(st);
         f32.reset();
-        cudaStreamDestroy(st);
     }
+    // the buffers are released behind the stream's work as the members go;
+    // own_st, declared before them, destroys the stream last
 }
 
 void Solver::sync()
 {
+    AllocScope scope(st);
     NADIA_CUDA(cudaStreamSynchronize(st));
     if (f32) f32->check_device_flag();
 }
@@ -147,6 +168,7 @@ std::vector<double> Solver::gauss_table(double gauss_width, int cut) const
 
 void Solver::plain_convolve(double *arr, double gauss_width, int cut)
 {
+    AllocScope scope(st);
     // the table stays on the device while the width and cut-off repeat, so
     // a periodic shrinkwrap neither allocates nor waits for the stream
     if (!(gauss && gauss_width == gauss_width_ && cut == gauss_cut_)) {
@@ -162,6 +184,7 @@ void Solver::plain_convolve(double *arr, double gauss_width, int cut)
 
 void Solver::upload_support()
 {
+    AllocScope scope(st);
     if (prec == NADIA_FP64)
         h2d(support.p, h_support.data(), n * sizeof(double), st);
     else
@@ -171,6 +194,7 @@ void Solver::upload_support()
 // BaseCDI::set_support, BaseCDI.c++:95-108
 void Solver::set_support(const double *obj, bool soften)
 {
+    AllocScope scope(st);
     double max = host_max(obj, n);
     for (size_t k = 0; k < n; ++k) h_support[k] = obj[k] / max;
     h_support_valid = true;
@@ -188,6 +212,7 @@ void Solver::set_support(const double *obj, bool soften)
 // BaseCDI::set_intensity, BaseCDI.c++:118-124
 void Solver::set_intensity(const double *I)
 {
+    AllocScope scope(st);
     for (size_t k = 0; k < n; ++k) h_isqrt[k] = sqrt(I[k]);
     if (prec == NADIA_FP64)
         h2d(isqrt.p, h_isqrt.data(), n * sizeof(double), st);
@@ -198,6 +223,7 @@ void Solver::set_intensity(const double *I)
 // BaseCDI::set_beam_stop, BaseCDI.c++:112-116
 void Solver::set_beam_stop(const double *mask)
 {
+    AllocScope scope(st);
     has_beam_stop = true;
     if (prec == NADIA_FP64) {
         if (!beam_stop) beam_stop.alloc(n);
@@ -210,8 +236,10 @@ void Solver::set_beam_stop(const double *mask)
 // PolyCDI::set_spectrum(Double_2D), PolyCDI.c++:66-89
 void Solver::set_spectrum(const double *wl_weight, int nl)
 {
+    AllocScope scope(st);
     NADIA_REQUIRE(kind == NADIA_POLY, NADIA_ERR_INVALID, "set_spectrum needs a PolyCDI handle");
     NADIA_REQUIRE(nl >= 1, NADIA_ERR_INVALID, "empty spectrum");
+    NADIA_CUDA(cudaStreamSynchronize(st)); // buffers of an earlier spectrum may be replaced
     std::vector<double> sp(wl_weight, wl_weight + 2 * (size_t)nl);
     double maxweight = 0, totweight = 0, lc = 0;
     for (int i = 0; i < nl; i++) {
@@ -257,6 +285,7 @@ void Solver::require_poly_ready() const
 void Solver::fresnel_init(const double *wf, double wl, double zfd_, double zfs_, double pixel_,
                           double norm_)
 {
+    AllocScope scope(st);
     norm = norm_;
     h_illum.assign(2 * n, 0.0);
     for (size_t k = 0; k < 2 * n; ++k) h_illum[k] = wf[k] * norm;
@@ -275,6 +304,7 @@ void Solver::fresnel_init(const double *wf, double wl, double zfd_, double zfs_,
 void Solver::fresnel_set_experimental_parameters(double wl, double zfd_, double zfs_,
                                                  double pixel_)
 {
+    AllocScope scope(st);
     wavelength = wl;
     pixel = pixel_;
     zfd = zfd_;
@@ -303,6 +333,7 @@ void Solver::fresnel_set_experimental_parameters(double wl, double zfd_, double 
 // FresnelCDI::set_norm, FresnelCDI.c++:139-148
 void Solver::fresnel_set_norm(double nn)
 {
+    AllocScope scope(st);
     NADIA_REQUIRE(kind == NADIA_FRESNEL, NADIA_ERR_INVALID, "set_norm needs a FresnelCDI handle");
     double old = norm;
     norm = nn;
@@ -319,6 +350,7 @@ void Solver::fresnel_set_norm(double nn)
 // FresnelCDI::auto_set_norm, FresnelCDI.c++:129-137
 void Solver::fresnel_auto_set_norm()
 {
+    AllocScope scope(st);
     NADIA_REQUIRE(kind == NADIA_FRESNEL, NADIA_ERR_INVALID,
                   "auto_set_norm needs a FresnelCDI handle");
     double wf_norm = 0, int_norm = 0;
@@ -333,6 +365,7 @@ void Solver::fresnel_auto_set_norm()
 // BaseCDI::set_algorithm, BaseCDI.c++:192-237
 void Solver::set_algorithm(int alg)
 {
+    AllocScope scope(st);
     if (algorithm == alg) return;
     double b = beta;
     double m[10] = {0};
@@ -356,6 +389,7 @@ void Solver::set_algorithm(int alg)
 // BaseCDI::set_custom_algorithm, BaseCDI.c++:240-255
 void Solver::set_custom(const double m[10])
 {
+    AllocScope scope(st);
     w[PSF] = m[0] + m[1] + m[2] + m[3];
     w[PFS] = -m[0] + m[4] + m[5] + m[6];
     w[PS] = -m[2] - m[5] - m[7] + m[9];
@@ -367,6 +401,7 @@ void Solver::set_custom(const double m[10])
 // BaseCDI::set_relaxation_parameter, BaseCDI.h:264-267
 void Solver::set_relaxation_parameter(double b)
 {
+    AllocScope scope(st);
     beta = b;
     set_algorithm(algorithm);
 }
@@ -376,6 +411,7 @@ void Solver::set_relaxation_parameter(double b)
 // PlanarCDI.c++:39-62 / PolyCDI.c++:102-126 / FresnelCDI.c++:152-201
 void Solver::initialise_estimate(int seed)
 {
+    AllocScope scope(st);
     std::vector<double> h(2 * n, 0.0);
     GlibcRand rnd(seed);
     if (kind == NADIA_FRESNEL) {
@@ -418,6 +454,7 @@ void Solver::initialise_estimate(int seed)
 
 void Solver::set_esw(const double *h)
 {
+    AllocScope scope(st);
     if (prec == NADIA_FP64)
         h2d(x.p, h, n * sizeof(double2), st);
     else
@@ -426,6 +463,7 @@ void Solver::set_esw(const double *h)
 
 void Solver::get_esw(double *h)
 {
+    AllocScope scope(st);
     if (prec == NADIA_FP64)
         d2h(h, x.p, n * sizeof(double2), st);
     else
@@ -434,6 +472,7 @@ void Solver::get_esw(double *h)
 
 void Solver::set_esw_f32(const float *h)
 {
+    AllocScope scope(st);
     if (prec == NADIA_FP32) {
         f32->set_x_f32(h);
         return;
@@ -445,6 +484,7 @@ void Solver::set_esw_f32(const float *h)
 
 void Solver::get_esw_f32(float *h)
 {
+    AllocScope scope(st);
     if (prec == NADIA_FP32) {
         f32->get_x_f32(h);
         return;
@@ -456,6 +496,7 @@ void Solver::get_esw_f32(float *h)
 
 void Solver::set_transmission(const double *h)
 {
+    AllocScope scope(st);
     if (kind != NADIA_FRESNEL) {
         set_esw(h);
         return;
@@ -472,6 +513,7 @@ void Solver::set_transmission(const double *h)
 
 void Solver::get_transmission(double *h)
 {
+    AllocScope scope(st);
     if (kind != NADIA_FRESNEL) {
         get_esw(h);
         return;
@@ -487,6 +529,7 @@ void Solver::get_transmission(double *h)
 
 void Solver::get_illumination_at_sample(double *h)
 {
+    AllocScope scope(st);
     NADIA_REQUIRE(kind == NADIA_FRESNEL, NADIA_ERR_INVALID, "needs a FresnelCDI handle");
     if (prec == NADIA_FP64)
         d2h(h, illum_sample.p, n * sizeof(double2), st);
@@ -498,6 +541,7 @@ void Solver::get_illumination_at_sample(double *h)
 
 void Solver::plain_propagate_to(double2 *c, bool pg)
 {
+    AllocScope scope(st);
     if (kind == NADIA_FRESNEL) {
         // FresnelCDI::propagate_to_detector, FresnelCDI.c++:245-250
         plain::invert(c, nx, ny, true, st);
@@ -516,6 +560,7 @@ void Solver::plain_propagate_to(double2 *c, bool pg)
 
 void Solver::plain_propagate_from(double2 *c, bool pg)
 {
+    AllocScope scope(st);
     if (kind == NADIA_FRESNEL) {
         // FresnelCDI::propagate_from_detector, FresnelCDI.c++:238-243
         plain::multiply_factors(c, coef.p, nx, ny, +1, st);
@@ -533,6 +578,7 @@ void Solver::plain_propagate_from(double2 *c, bool pg)
 
 void Solver::plain_scale(double2 *c)
 {
+    AllocScope scope(st);
     if (kind == NADIA_FRESNEL) {
         // FresnelCDI::scale_intensity, FresnelCDI.c++:217-236
         plain::add_scaled(c, illum.p, 1.0, n, st);
@@ -551,6 +597,7 @@ void Solver::plain_scale(double2 *c)
 // projection in get_padded / get_unpadded (PolyCDI.c++:143-152, 175-181)
 void Solver::plain_project(double2 *c)
 {
+    AllocScope scope(st);
     if (kind == NADIA_POLY) {
         plain::pad(c, nx, ny, padded.p, px, py, st);
         plain_propagate_to(padded.p, true);
@@ -567,6 +614,7 @@ void Solver::plain_project(double2 *c)
 // reallocate_temp_complex_memory, BaseCDI.c++:257-275
 void Solver::ensure_temps()
 {
+    AllocScope scope(st);
     if (w[PFS] != 0 && !tPFS) tPFS.alloc(n);
     if (w[PF] != 0 && !tPF) tPF.alloc(n);
     if (w[PS] != 0 && !tPS) tPS.alloc(n);
@@ -576,6 +624,7 @@ void Solver::ensure_temps()
 // BaseCDI::iterate, BaseCDI.c++:297-387; PolyCDI::iterate, PolyCDI.c++:130-250
 void Solver::plain_iterate_once()
 {
+    AllocScope scope(st);
     const size_t nb = n * sizeof(double2);
     if (algorithm == NADIA_ER) {
         plain_project(x.p);
@@ -620,6 +669,7 @@ void Solver::record_error()
 // BaseCDI::update_n_best, BaseCDI.c++:390-413
 void Solver::update_n_best()
 {
+    AllocScope scope(st);
     if (n_best <= 0) return;
     double cur = get_error();
     int place = 0;
@@ -643,6 +693,7 @@ void Solver::update_n_best()
 
 void Solver::iterate(int count)
 {
+    AllocScope scope(st);
     NADIA_REQUIRE(count >= 0, NADIA_ERR_INVALID, "negative iteration count");
     require_poly_ready();
     if (prec == NADIA_FP32 && n_best == 0) {
@@ -662,6 +713,7 @@ void Solver::iterate(int count)
 
 double Solver::get_error()
 {
+    AllocScope scope(st);
     double e = 0;
     d2h(&e, d_err.p, sizeof(double), st);
     if (f32) f32->check_device_flag();
@@ -670,6 +722,7 @@ double Solver::get_error()
 
 void Solver::get_error_history(double *out, int count)
 {
+    AllocScope scope(st);
     NADIA_REQUIRE(count >= 0 && count <= kRing && count <= iters, NADIA_ERR_RANGE,
                   "fewer iterations recorded than requested");
     std::vector<double> ring(kRing);
@@ -680,6 +733,7 @@ void Solver::get_error_history(double *out, int count)
 // BaseCDI::apply_shrinkwrap, BaseCDI.c++:416-429
 void Solver::apply_shrinkwrap(double gauss_width, double thresh)
 {
+    AllocScope scope(st);
     if (prec == NADIA_FP32) {
         f32->shrinkwrap(gauss_width, thresh);
         h_support_valid = false;
@@ -697,6 +751,7 @@ void Solver::apply_shrinkwrap(double gauss_width, double thresh)
 
 void Solver::get_support(double *h)
 {
+    AllocScope scope(st);
     if (h_support_valid) {
         if (h != h_support.data()) std::memcpy(h, h_support.data(), n * sizeof(double));
         return;
@@ -712,6 +767,7 @@ void Solver::get_support(double *h)
 // BaseCDI::get_best_result, BaseCDI.c++:82-91
 void Solver::get_best(int index, double *err, double *h)
 {
+    AllocScope scope(st);
     NADIA_REQUIRE(index >= 0 && index < n_best, NADIA_ERR_RANGE,
                   "index out of bounds in get_best_result");
     *err = best_err[index];
@@ -727,12 +783,14 @@ void Solver::get_best(int index, double *err, double *h)
 
 void Solver::reset_best()
 {
+    AllocScope scope(st);
     for (int i = 0; i < n_best; ++i) best_err[i] = 1;
 }
 
 // single operators on a caller's field (IDL_interface.c:947-985)
 void Solver::single_op(int op, double *field)
 {
+    AllocScope scope(st);
     NADIA_REQUIRE(kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
                   "single operators act on the unpadded grid (PLANAR, FRESNEL)");
     if (prec == NADIA_FP32) {
@@ -755,6 +813,7 @@ void Solver::single_op(int op, double *field)
 // PlanarCDI::get_intensity_autocorrelation, PlanarCDI.c++:13-36
 void Solver::autocorrelation(double *out)
 {
+    AllocScope scope(st);
     NADIA_REQUIRE(kind == NADIA_PLANAR, NADIA_ERR_INVALID, "needs a PlanarCDI handle");
     if (prec == NADIA_FP32) {
         f32->autocorrelation(out);

@@ -22,6 +22,7 @@ struct Solver {
     size_t n = 0;
     int device = 0;
     unsigned long long uid = 0; // unique per handle (batch plans key on it)
+    OwnedStream own_st;         // outlives every buffer below
     cudaStream_t st = nullptr;
 
     // algorithm state (BaseCDI.h:87-150)

@@ -406,7 +406,7 @@ class Server:
     collect each reconstruction when it is done."""
 
     STATS = ("queued", "active", "completed", "failed", "bytes", "peak_bytes", "steps",
-             "admitted")
+             "admitted", "us_step", "us_idle", "us_prepare", "us_readback")
 
     def __init__(self, budget_bytes, max_active=64, chunk=25):
         self.lib = load()
@@ -482,7 +482,7 @@ class Server:
         return esw, sup, float(err[0]), tuple(t)
 
     def stats(self):
-        out = (_LL * 8)()
+        out = (_LL * 12)()
         _check(self.lib.nadia_server_stats(self.h, out))
         return dict(zip(self.STATS, list(out)))
 

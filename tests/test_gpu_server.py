@@ -52,7 +52,8 @@ def run_alone(request):
                                          ("planar", pynadia.FP32, 512),
                                          ("fresnel", pynadia.FP64, 128),
                                          ("fresnel", pynadia.FP32, 256),
-                                         ("poly", pynadia.FP64, 96)])
+                                         ("poly", pynadia.FP64, 96),
+                                         ("poly", pynadia.FP32, 240)])
 def test_admission_charge_covers_device_bytes(kind, prec, n):
     before = pynadia.device_bytes()
     kw = {}
@@ -62,7 +63,7 @@ def test_admission_charge_covers_device_bytes(kind, prec, n):
                   focal_detector_length=f.zfd, focal_sample_length=f.zfs, pixel_size=f.pixel)
         inten, sup = f.intensity, f.support
     elif kind == "poly":
-        p = synth.PolyCase(n, seed=3, padding=4, photons=1e7)
+        p = synth.PolyCase(n, seed=3, padding=8 if prec == pynadia.FP32 else 4, photons=1e7)
         inten, sup = p.intensity, p.support
     else:
         c = planar(n, 3)
