@@ -485,7 +485,7 @@ def ours(args, rank, world, local_rank):
     line = None
     if rank == 0:
         # ---- roofline of the dominant pass (timed alone with events)
-        col_us, row_us = pynadia.pass_times(solvers, reps=10)
+        col_us, _, row_us = pynadia.pass_times(solvers, reps=10)
         px = B * N * N
         passes = {"column": (col_us, 20 * px), "row": (row_us, 36 * px)}
         dom = max(passes, key=lambda k: passes[k][0])

@@ -318,11 +318,13 @@ long long nadia_device_bytes(void);
  * on the stream of its first handle. */
 int nadia_get_stream(nadia_solver *s, void **stream);
 
-/* Mean device time in microseconds of one column pass and one row pass of
- * the fused FP32 iteration for `count` handles of one size and geometry run
- * as a batch (CUDA events around `reps` launches of each pass).  The passes
- * run for real: each handle advances by 1 + reps iterations. */
-int nadia_pass_times(nadia_solver *const *solvers, int count, int reps, double out_us[2]);
+/* Mean device time in microseconds of each pass of the fused FP32 iteration
+ * for `count` handles of one size and geometry run as a batch (CUDA events
+ * around `reps` launches of each pass): out_us = {column pass, second column
+ * pass (PolyCDI's modulus and inverse column transform; 0 otherwise), row
+ * pass}.  The passes run for real: each handle advances by 1 + reps
+ * iterations. */
+int nadia_pass_times(nadia_solver *const *solvers, int count, int reps, double out_us[3]);
 
 /* Kernels this library has launched in this process (graph replays count
  * every kernel they contain). */

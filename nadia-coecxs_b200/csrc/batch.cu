@@ -33,6 +33,10 @@ struct Group {
     int nx = 0, ny = 0;
     bool fresnel = false;
     const f32::Choice *choice = nullptr;
+    // PolyCDI groups (same grid and padding): the padded-grid passes
+    const f32::PolyVariant *pcol = nullptr, *prow = nullptr;
+    int pcols = 0, rtiles = 0;
+    int launches_per_iter() const { return pcol ? 3 : 2; }
     std::vector<Solver *> members;
     DevBuf<f32::Slot *> ptrs;
     const float2 *twx = nullptr, *twy = nullptr;
@@ -69,14 +73,27 @@ struct Plan {
             cudaStream_t s = g.st ? g.st : st;
             const int n = (int)g.members.size();
             for (int it = 0; it < iters; ++it) {
-                g.choice->col->col(g.fresnel, g.ptrs.p, n, g.nx, g.ny, g.twx, s);
-                g.choice->row->row(f32::kRowFull, g.ptrs.p, n, g.nx, g.ny, g.twy, s);
+                if (g.pcol) {
+                    g.pcol->col_fwd(g.ptrs.p, n, g.pcols, s, g.twx);
+                    g.pcol->col_inv(g.ptrs.p, n, g.pcols, s, g.twx);
+                    g.prow->row(f32::kRowFull, g.ptrs.p, n, g.rtiles, s, g.twy);
+                } else {
+                    g.choice->col->col(g.fresnel, g.ptrs.p, n, g.nx, g.ny, g.twx, s);
+                    g.choice->row->row(f32::kRowFull, g.ptrs.p, n, g.nx, g.ny, g.twy, s);
+                }
             }
         }
         for (size_t i = 1; i < groups.size(); ++i) {
             NADIA_CUDA(cudaEventRecord(join[i], groups[i].st));
             NADIA_CUDA(cudaStreamWaitEvent(st, join[i], 0));
         }
+    }
+
+    long long launches_per_iter() const
+    {
+        long long l = 0;
+        for (const auto &g : groups) l += g.launches_per_iter();
+        return l;
     }
 };
 
@@ -85,7 +102,8 @@ std::list<std::unique_ptr<Plan>> g_plans; // most recently used first
 
 bool batchable(const Solver &s)
 {
-    return s.prec == NADIA_FP32 && s.kind != NADIA_POLY && s.n_best == 0 &&
+    return s.prec == NADIA_FP32 && s.n_best == 0 &&
+           (s.kind != NADIA_POLY || s.f32->impl->pcol != nullptr) &&
            (s.algorithm == NADIA_ER || s.w[PFS] == 0);
 }
 
@@ -121,9 +139,11 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
         // the plan's buffers are ordered on its stream (a member's, which
         // outlives the plan: plans go before their members' streams do)
         AllocScope scope(p->st);
-        std::map<std::tuple<int, int, int>, size_t> index;
+        std::map<std::tuple<int, int, int, int, int>, size_t> index;
         for (Solver *s : fused) {
-            auto k = std::make_tuple(s->nx, s->ny, s->kind == NADIA_FRESNEL ? 1 : 0);
+            // PolyCDI members of a group share the padding too
+            auto k = std::make_tuple(s->nx, s->ny, s->kind, s->kind == NADIA_POLY ? s->px : 0,
+                                     s->kind == NADIA_POLY ? s->py : 0);
             auto f = index.find(k);
             if (f == index.end()) {
                 index[k] = p->groups.size();
@@ -141,11 +161,22 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
         p->join.resize(p->groups.size(), nullptr);
         for (size_t i = 0; i < p->groups.size(); ++i) {
             Group &g = p->groups[i];
-            // the batched tuning class for every group, whatever its size, so a
-            // handle's arithmetic does not depend on the other handles of the call
-            g.choice = &f32::choose(g.nx, g.ny, g.fresnel, kBatchClass);
-            g.twx = f32::twiddle_table(g.nx);
-            g.twy = f32::twiddle_table(g.ny);
+            if (g.members[0]->kind == NADIA_POLY) {
+                // the padded-grid variants the members picked (the same for all)
+                const Fused32::Impl &I0 = *g.members[0]->f32->impl;
+                g.pcol = I0.pcol;
+                g.prow = I0.prow;
+                g.pcols = I0.pcols;
+                g.rtiles = I0.nx / I0.prow->L;
+                g.twx = I0.twx;
+                g.twy = I0.twy;
+            } else {
+                // the batched tuning class for every group, whatever its size, so a
+                // handle's arithmetic does not depend on the other handles of the call
+                g.choice = &f32::choose(g.nx, g.ny, g.fresnel, kBatchClass);
+                g.twx = f32::twiddle_table(g.nx);
+                g.twy = f32::twiddle_table(g.ny);
+            }
             std::vector<f32::Slot *> hp;
             for (Solver *s : g.members) hp.push_back(s->f32->impl->slot.p);
             g.ptrs.alloc(hp.size());
@@ -175,7 +206,7 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
         for (Solver *s : g.members) {
             Fused32::Impl &I = *s->f32->impl;
             I.check_algorithm();
-            I.use_choice(g.choice);
+            if (g.choice) I.use_choice(g.choice);
             I.push_slot_async(plan->st);
             if (!I.p_valid) I.prime(plan->st);
         }
@@ -191,13 +222,13 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
         }
         while (left >= kGraphIters) {
             NADIA_CUDA(cudaGraphLaunch(plan->exec, plan->st));
-            g_launches += 2LL * kGraphIters * (long long)plan->groups.size();
+            g_launches += kGraphIters * plan->launches_per_iter();
             left -= kGraphIters;
         }
     }
     if (left > 0) {
         plan->launch_block(left);
-        g_launches += 2LL * left * (long long)plan->groups.size();
+        g_launches += left * plan->launches_per_iter();
     }
     NADIA_CUDA(cudaGetLastError());
     NADIA_CUDA(cudaEventRecord(ev, plan->st));
@@ -210,12 +241,13 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
 
 // Device time of one column pass and one row pass (microseconds, mean of
 // `reps` launches with CUDA events on the launching stream) for the batch.
-void pass_times(Solver *const *solvers, int count, int reps, double out_us[2])
+void pass_times(Solver *const *solvers, int count, int reps, double out_us[3])
 {
     NADIA_REQUIRE(count >= 1 && reps >= 1, NADIA_ERR_INVALID, "bad count");
     for (int i = 0; i < count; ++i)
         NADIA_REQUIRE(batchable(*solvers[i]) && solvers[i]->nx == solvers[0]->nx &&
-                          solvers[i]->ny == solvers[0]->ny && solvers[i]->kind == solvers[0]->kind,
+                          solvers[i]->ny == solvers[0]->ny && solvers[i]->kind == solvers[0]->kind &&
+                          solvers[i]->px == solvers[0]->px && solvers[i]->py == solvers[0]->py,
                       NADIA_ERR_INVALID, "pass timing needs FP32 handles of one size and kind");
     // run one iteration through the batch path so the plan and graph exist
     iterate_many(solvers, count, 1);
@@ -227,26 +259,36 @@ void pass_times(Solver *const *solvers, int count, int reps, double out_us[2])
     Group &g = plan->groups[0];
     cudaStream_t st = plan->st;
     const int n = (int)g.members.size();
-    cudaEvent_t e[3];
+    cudaEvent_t e[4];
     for (auto &x : e) NADIA_CUDA(cudaEventCreate(&x));
-    float col = 0, row = 0;
+    float t[3] = {0, 0, 0};
     for (int r = 0; r < reps; ++r) {
         NADIA_CUDA(cudaEventRecord(e[0], st));
-        g.choice->col->col(g.fresnel, g.ptrs.p, n, g.nx, g.ny, g.twx, st);
-        NADIA_CUDA(cudaEventRecord(e[1], st));
-        g.choice->row->row(f32::kRowFull, g.ptrs.p, n, g.nx, g.ny, g.twy, st);
-        NADIA_CUDA(cudaEventRecord(e[2], st));
-        NADIA_CUDA(cudaEventSynchronize(e[2]));
-        float a = 0, b = 0;
-        NADIA_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
-        NADIA_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
-        col += a;
-        row += b;
+        if (g.pcol) {
+            g.pcol->col_fwd(g.ptrs.p, n, g.pcols, st, g.twx);
+            NADIA_CUDA(cudaEventRecord(e[1], st));
+            g.pcol->col_inv(g.ptrs.p, n, g.pcols, st, g.twx);
+            NADIA_CUDA(cudaEventRecord(e[2], st));
+            g.prow->row(f32::kRowFull, g.ptrs.p, n, g.rtiles, st, g.twy);
+        } else {
+            g.choice->col->col(g.fresnel, g.ptrs.p, n, g.nx, g.ny, g.twx, st);
+            NADIA_CUDA(cudaEventRecord(e[1], st));
+            NADIA_CUDA(cudaEventRecord(e[2], st));
+            g.choice->row->row(f32::kRowFull, g.ptrs.p, n, g.nx, g.ny, g.twy, st);
+        }
+        NADIA_CUDA(cudaEventRecord(e[3], st));
+        NADIA_CUDA(cudaEventSynchronize(e[3]));
+        for (int k = 0; k < 3; ++k) {
+            float ms = 0;
+            NADIA_CUDA(cudaEventElapsedTime(&ms, e[k], e[k + 1]));
+            t[k] += ms;
+        }
     }
+    g_launches += (long long)reps * g.launches_per_iter();
     for (auto &x : e) cudaEventDestroy(x);
+    if (!g.pcol) t[1] = 0; // no second column pass
+    for (int k = 0; k < 3; ++k) out_us[k] = 1000.0 * t[k] / reps;
     for (Solver *s : g.members) s->iters += reps;
-    out_us[0] = 1000.0 * col / reps;
-    out_us[1] = 1000.0 * row / reps;
 }
 
 void forget_batches_with(unsigned long long uid)

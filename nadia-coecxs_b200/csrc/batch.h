@@ -11,7 +11,7 @@ struct Solver;
 extern std::atomic<long long> g_launches;
 
 void iterate_many(Solver *const *solvers, int count, int iterations);
-void pass_times(Solver *const *solvers, int count, int reps, double out_us[2]);
+void pass_times(Solver *const *solvers, int count, int reps, double out_us[3]);
 void forget_batches_with(unsigned long long uid);
 
 } // namespace nadia

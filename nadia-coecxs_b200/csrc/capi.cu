@@ -398,7 +398,7 @@ extern "C" int nadia_get_stream(nadia_solver *h, void **stream)
     });
 }
 
-extern "C" int nadia_pass_times(nadia_solver *const *solvers, int count, int reps, double out_us[2])
+extern "C" int nadia_pass_times(nadia_solver *const *solvers, int count, int reps, double out_us[3])
 {
     return guard([&] {
         need(solvers, "solvers");

@@ -944,7 +944,10 @@ void Fused32::Impl::check_algorithm() const
 void Fused32::Impl::prime(cudaStream_t st)
 {
     const Slot *const *sl = slot_ptr.p;
-    choice->row->row(kRowPrime, sl, 1, nx, ny, twy, st);
+    if (S.kind == NADIA_POLY)
+        prow->row(kRowPrime, sl, 1, nx / prow->L, st, twy);
+    else
+        choice->row->row(kRowPrime, sl, 1, nx, ny, twy, st);
     g_launches += 1;
     p_valid = true;
 }

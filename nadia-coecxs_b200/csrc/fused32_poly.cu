@@ -130,11 +130,7 @@ void Fused32::iterate_poly(int count)
     cudaStream_t st = I.S.st;
     const Slot *const *sl = I.slot_ptr.p;
     const int rtiles = I.nx / I.prow->L;
-    if (!I.p_valid) {
-        I.prow->row(kRowPrime, sl, 1, rtiles, st, I.twy);
-        g_launches += 1;
-        I.p_valid = true;
-    }
+    if (!I.p_valid) I.prime(st);
     auto one = [&] {
         I.pcol->col_fwd(sl, 1, I.pcols, st, I.twx);
         I.pcol->col_inv(sl, 1, I.pcols, st, I.twx);

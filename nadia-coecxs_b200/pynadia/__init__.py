@@ -367,12 +367,13 @@ def iterate_many(solvers, iterations):
 
 
 def pass_times(solvers, reps=5):
-    """Device microseconds of one column pass and one row pass for a batch."""
+    """Device microseconds of each pass for a batch: (column, second column
+    (PolyCDI only, else 0), row)."""
     lib = load()
     arr = (_H * len(solvers))(*[s.h for s in solvers])
-    out = np.zeros(2)
+    out = np.zeros(3)
     _check(lib.nadia_pass_times(arr, len(solvers), int(reps), _ptr(out)))
-    return float(out[0]), float(out[1])
+    return float(out[0]), float(out[1]), float(out[2])
 
 
 def launch_count():

@@ -229,6 +229,7 @@ def test_pass_times_and_launch_count():
     _, b = planar_pair(512)
     b.set_algorithm("HIO")
     l0 = pynadia.launch_count()
-    col, row = pynadia.pass_times([b], reps=3)
+    col, col2, row = pynadia.pass_times([b], reps=3)
+    assert col2 == 0
     assert col > 0 and row > 0
     assert pynadia.launch_count() > l0

@@ -89,3 +89,29 @@ def test_unsupported_padded_size_is_refused():
     with pytest.raises(pynadia.NadiaError) as e:
         s.set_spectrum(p.spectrum)
     assert e.value.code == 3
+
+
+def test_batched_equals_alone_and_pass_times():
+    """PolyCDI handles of one padded size step as one batch in
+    nadia_iterate_many; each ends bit for bit where it ends alone."""
+    p = synth.PolyCase(480, seed=3, padding=16, photons=1e8)
+
+    def make(seed):
+        s = pynadia.Solver("poly", 480, 480, precision=pynadia.FP32)
+        s.set_support(p.support)
+        s.set_intensity(p.intensity)
+        s.set_spectrum(p.spectrum)
+        s.initialise_estimate(seed)
+        s.set_algorithm("HIO")
+        return s
+
+    batch = [make(k) for k in range(3)]
+    alone = [make(k) for k in range(3)]
+    pynadia.iterate_many(batch, 21)
+    for s in alone:
+        s.iterate(21)
+    for a, b in zip(alone, batch):
+        assert np.array_equal(a.get_error_history(21), b.get_error_history(21))
+        assert np.array_equal(a.get_exit_surface_wave(), b.get_exit_surface_wave())
+    c1, c2, r = pynadia.pass_times(batch, reps=3)
+    assert c1 > 0 and c2 > 0 and r > 0
