@@ -7,7 +7,7 @@ threshold 0.1), on the synthetic disk object (radius 320 px, phase smoothing
 sigma 4, 1e9 photons with Poisson noise, central 8x8 beam stop unmeasured),
 run in the fused FP32 form (complex FP32 transforms and projections, FP64
 error and support reductions) through nadia_iterate_many.  The batch's
-working set (~0.8 GB for B=8) is larger than the 126 MB L2, so no flush is
+working set (~1.6 GB for B=16) is larger than the 126 MB L2, so no flush is
 needed between steps.
 
   value  -- reconstructions/s with the inputs resident on the device, timed
@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--batch", type=int, default=8)
+    p.add_argument("--batch", type=int, default=16)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--serve-requests", type=int, default=48,
                    help="requests in the saturated serving run (0 = skip serving)")
