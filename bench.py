@@ -59,6 +59,9 @@ def parse():
                    help="items in the FresnelCDI uneven-size batch report (0 = skip)")
     p.add_argument("--fresnel-only", action="store_true",
                    help="print the FresnelCDI batch report only")
+    p.add_argument("--quick-poly", action="store_true",
+                   help="device-resident FP32 PolyCDI steps only (1024^2 padded to 1080^2; "
+                        "for profiling)")
     p.add_argument("--quick", action="store_true",
                    help="device-resident steps only (for profiling): no e2e, FP64, CPU legs")
     return p.parse_args()
@@ -378,6 +381,35 @@ def fresnel_batch_report(pynadia, synth, n_items=64, iters=300):
     return out
 
 
+def quick_poly(pynadia, synth, args):
+    """`args.batch` FP32 PolyCDI reconstructions of 1024^2 padded to 1080^2
+    (10-line spectrum, 5% FWHM), HIO, stepped together; per-pass device times."""
+    import torch
+    p = synth.PolyCase(1024, seed=300, padding=28)
+    solvers = []
+    for k in range(args.batch):
+        s = pynadia.Solver("poly", 1024, 1024, precision=pynadia.FP32)
+        s.set_support(p.support)
+        s.set_intensity(p.intensity)
+        s.set_spectrum(p.spectrum)
+        s.initialise_estimate(k)
+        s.set_algorithm("HIO")
+        solvers.append(s)
+    for _ in range(args.warmup):
+        pynadia.iterate_many(solvers, 16)
+    st = torch.cuda.ExternalStream(solvers[0].stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(args.steps):
+        pynadia.iterate_many(solvers, 16)
+    b.record(st)
+    b.synchronize()
+    us = a.elapsed_time(b) * 1000.0 / (16 * args.steps)
+    c1, c2, r = pynadia.pass_times(solvers, reps=5)
+    return {"quick_poly": True, "batch": args.batch, "us_per_iteration": us,
+            "pass_us": {"column_fwd": c1, "column_inv": c2, "row": r}}
+
+
 def phase_aligned_error(x, ref):
     import numpy as np
     inner = np.vdot(x, ref)
@@ -394,6 +426,8 @@ def ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     if args.serve_only:
         return {"serving": serving_report(pynadia, synth, n_req=args.serve_requests)}
+    if args.quick_poly:
+        return quick_poly(pynadia, synth, args)
     if args.fresnel_only:
         return {"fresnel_batch": fresnel_batch_report(pynadia, synth, n_items=args.fresnel_batch)}
     dist = None
