@@ -36,7 +36,7 @@ struct Group {
     // PolyCDI groups (same grid and padding): the padded-grid passes
     const f32::PolyVariant *pcol = nullptr, *prow = nullptr;
     int pcols = 0, rtiles = 0;
-    int launches_per_iter() const { return pcol ? 3 : 2; }
+    int launches_per_iter() const { return pcol ? 4 : 2; }
     std::vector<Solver *> members;
     DevBuf<f32::Slot *> ptrs;
     const float2 *twx = nullptr, *twy = nullptr;

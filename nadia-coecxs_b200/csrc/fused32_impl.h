@@ -45,6 +45,7 @@ struct alignas(64) Slot {
     // gx/gy[l][i] are the rows/columns sampled for wavelength l at unpadded
     // row/column i (-1: outside the grid); wl[l] the normalised weights
     float *q;
+    float *ratio;           // modulus ratio per pixel of the detector window (panel layout)
     const int *gx, *gy;
     const float *wl;
     int nl, px, py, mx, my;
@@ -145,7 +146,7 @@ struct Fused32::Impl {
     bool p_valid = false;
     // PolyCDI
     int mx = 0, my = 0, pcols = 0;
-    DevBuf<float> q, wl;
+    DevBuf<float> q, wl, ratio;
     DevBuf<int> gx, gy;
     const f32::PolyVariant *pcol = nullptr, *prow = nullptr;
     cudaGraphExec_t graph_exec = nullptr;

@@ -77,7 +77,8 @@ void Fused32::set_spectrum()
     const size_t m = (size_t)mx * my;
     I.P.alloc(m);
     I.q.alloc(m);
-    I.partials.alloc(I.pcols);
+    I.ratio.alloc(I.n);
+    I.partials.alloc(kExpandBlocks); // error partials: one per expansion block
     NADIA_CUDA(cudaMemsetAsync(I.P.p, 0, I.P.bytes(), S.st));
     NADIA_CUDA(cudaMemsetAsync(I.q.p, 0, I.q.bytes(), S.st));
     const int nl = S.nlambda;
@@ -115,7 +116,8 @@ void Fused32::set_spectrum()
     h.py = S.py;
     h.mx = mx;
     h.my = my;
-    h.ncol = I.pcols;
+    h.ratio = I.ratio.p;
+    h.ncol = kExpandBlocks;
     h.s0 = (float)(1.0 / std::sqrt((double)mx * (double)my));
     I.p_valid = false;
     I.push_slot();
@@ -149,13 +151,13 @@ void Fused32::iterate_poly(int count)
         }
         while (left >= G) {
             NADIA_CUDA(cudaGraphLaunch(I.graph_exec, st));
-            g_launches += 3 * G;
+            g_launches += 4 * G;
             left -= G;
         }
     }
     for (; left > 0; --left) {
         one();
-        g_launches += 3;
+        g_launches += 4;
     }
     NADIA_CUDA(cudaGetLastError());
     I.S.iters += count;

@@ -11,17 +11,20 @@
 //   column pass 1: forward column transforms; Psi (transform order) back to P,
 //                  |Psi|^2 of the centred detector field (propagate_to_detector:
 //                  FFT then Complex_2D::invert(true)) to q
-//   column pass 2: the modulus of PolyCDI::scale_intensity (PolyCDI.c++:255-292)
-//                  against the wavelength-expanded intensity of expand_wl
-//                  (PolyCDI.c++:296-334), gathered from q, with the FP64 error
-//                  partials; inverse column transforms; the estimate's rows to P
+//   expansion:     for every measured pixel of the detector window, the
+//                  wavelength-expanded intensity of expand_wl (PolyCDI.c++:296-334)
+//                  gathered from q, the modulus ratio of PolyCDI::scale_intensity
+//                  (PolyCDI.c++:255-292) to `ratio`, and the FP64 error partials
+//                  (a light kernel at full occupancy: the gathers are latency-bound)
+//   column pass 2: Psi times the ratio, inverse column transforms; the
+//                  estimate's rows to P
 //   row pass:      inverse row transforms of those rows, the window
 //                  py..py+ny-1 combined with x and the support (the generic
 //                  combine of PolyCDI.c++:201-237, or ER), x written, forward
 //                  row transforms of the zero-padded rows to P
 //
-// The two column passes are separate launches because every expanded pixel
-// reads |Psi|^2 from other columns (q stays in L2: 4 bytes per padded pixel).
+// The passes are separate launches because every expanded pixel reads
+// |Psi|^2 from other columns (q stays in L2: 4 bytes per padded pixel).
 #pragma once
 
 #include "fused32_kernels.cuh"
@@ -61,6 +64,63 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_col_fwd(const Slot *con
     });
 }
 
+constexpr int kExpandThreads = 256;
+constexpr int kExpandBlocks = 1184; // 8 per SM
+
+// One thread per pixel of the detector window in the panel layout (lanes
+// cover 4 columns x 8 rows, so the gathered q addresses of a warp are nearly
+// contiguous).  ratio = sqrt(I)/sqrt(I_calc) (0 when I_calc = 0) for measured
+// pixels, 1 elsewhere; partials[block] = sum of (sqrt(I) - sqrt(I_calc))^2.
+__global__ void __launch_bounds__(kExpandThreads) k_poly_expand(const Slot *const *slots)
+{
+    const Slot &S = *slots[blockIdx.y];
+    const int mx = S.mx, px = S.px, py = S.py;
+    const int nx = mx - 2 * px, ny = S.my - 2 * py;
+    const int nl = S.nl;
+    const float *__restrict__ q = S.q;
+    const float *__restrict__ mI = S.mI;
+    const int *__restrict__ gx = S.gx;
+    const int *__restrict__ gy = S.gy;
+    const float *__restrict__ wl = S.wl;
+    float *__restrict__ ratio = S.ratio;
+    const size_t n = (size_t)nx * ny;
+    double diff = 0.0;
+    for (size_t a = blockIdx.x * (size_t)kExpandThreads + threadIdx.x; a < n;
+         a += (size_t)gridDim.x * kExpandThreads) {
+        const size_t t = a / kPanel;
+        const int i = (int)(t % nx), j = (int)(t / nx) * kPanel + (int)(a % kPanel);
+        const float m = __ldg(&mI[a]);
+        float r = 1.f;
+        if (!(m < 0.f)) {
+            // groups of four wavelengths: their loads issue together
+            float acc = 0.f;
+            int l = 0;
+            for (; l + 4 <= nl; l += 4) {
+                float qv[4], w[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int ga = __ldg(&gx[(l + u) * nx + i]), gb = __ldg(&gy[(l + u) * ny + j]);
+                    w[u] = (ga >= 0 && gb >= 0) ? __ldg(&wl[l + u]) : 0.f;
+                    qv[u] = (ga >= 0 && gb >= 0) ? __ldg(&q[paddr(ga, gb, mx)]) : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc += w[u] * qv[u];
+            }
+            for (; l < nl; ++l) {
+                const int ga = __ldg(&gx[l * nx + i]), gb = __ldg(&gy[l * ny + j]);
+                if (ga >= 0 && gb >= 0) acc += __ldg(&wl[l]) * __ldg(&q[paddr(ga, gb, mx)]);
+            }
+            const float calc = sqrtf(acc);
+            r = calc == 0.f ? 0.f : m / calc;
+            const double d = (double)m - (double)calc;
+            diff += d * d;
+        }
+        ratio[a] = r;
+    }
+    const double tot = block_sum<kExpandThreads>(diff);
+    if (threadIdx.x == 0) S.partials[blockIdx.x] = tot;
+}
+
 template <class C>
 __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_col_inv(const Slot *const *slots,
                                                                    const float2 *__restrict__ tw)
@@ -70,41 +130,17 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_col_inv(const Slot *con
     float2 *__restrict__ P = S.P;
     const int mx = S.mx, my = S.my, px = S.px, py = S.py;
     const int nx = mx - 2 * px, ny = my - 2 * py;
-    const int nl = S.nl;
-    const float *__restrict__ q = S.q;
-    const float *__restrict__ mI = S.mI;
-    const int *__restrict__ gx = S.gx;
-    const int *__restrict__ gy = S.gy;
-    const float *__restrict__ wl = S.wl;
+    const float *__restrict__ ratio = S.ratio;
     const int c0 = blockIdx.x * (C::L / kPanel);
     const float s02 = S.s0 * S.s0;
     float2 v[C::E];
     for_each_slot<C, true, false>([&](int e, int s, int kx) {
-        v[e] = P[paddr(kx, c0 * kPanel + s, mx)];
-    });
-    double diff = 0.0;
-    for_each_slot<C, true, false>([&](int e, int s, int kx) {
         const int ky = c0 * kPanel + s;
         const int i = centred(kx, mx) - px, j = centred(ky, my) - py;
-        float ratio = 1.f;
-        if (i >= 0 && i < nx && j >= 0 && j < ny) {
-            const float m = __ldg(&mI[paddr(i, j, nx)]);
-            if (!(m < 0.f)) {
-                float acc = 0.f;
-                for (int l = 0; l < nl; ++l) {
-                    const int a = __ldg(&gx[l * nx + i]), b = __ldg(&gy[l * ny + j]);
-                    if (a >= 0 && b >= 0) acc += __ldg(&wl[l]) * __ldg(&q[paddr(a, b, mx)]);
-                }
-                const float calc = sqrtf(acc);
-                ratio = calc == 0.f ? 0.f : m / calc;
-                const double d = (double)m - (double)calc;
-                diff += d * d;
-            }
-        }
-        v[e] = cscale(v[e], s02 * ratio);
+        float r = 1.f;
+        if (i >= 0 && i < nx && j >= 0 && j < ny) r = __ldg(&ratio[paddr(i, j, nx)]);
+        v[e] = cscale(P[paddr(kx, ky, mx)], s02 * r);
     });
-    const double tot = block_sum<C::NT>(diff);
-    if (threadIdx.x == 0) S.partials[blockIdx.x] = tot;
     transform<C, false>(v, sm, tw);
     for_each_slot<C, false, false>([&](int e, int s, int pos) {
         if (pos >= px && pos < px + nx) P[paddr(pos, c0 * kPanel + s, mx)] = v[e];
@@ -199,6 +235,7 @@ template <class C>
 void launch_poly_col_inv(const Slot *const *slots, int nslots, int tiles, cudaStream_t st,
                          const float2 *tw)
 {
+    k_poly_expand<<<dim3(kExpandBlocks, nslots), kExpandThreads, 0, st>>>(slots);
     k_poly_col_inv<C><<<dim3(tiles, nslots), C::NT, smem_bytes<C>(), st>>>(slots, tw);
 }
 

@@ -56,7 +56,7 @@ size_t footprint_bytes(int kind, int nx, int ny, int prec, int n_best, int pad_n
             const size_t m = (size_t)pad_nx * pad_ny;
             b += 8 * m + 4 * m;                                  // padded work array, |Psi|^2
             b += 4 * (size_t)nlambda * (nx + ny + 1);            // gather tables, weights
-            b += 8 * (size_t)(pad_ny / 8 + 1);                   // column-tile partials
+            b += 8 * 1184 + 4 * n;                               // error partials, ratio
         }
     }
     return b;
