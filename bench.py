@@ -503,18 +503,27 @@ def ours(args, rank, world, local_rank):
     def collect(s):
         return s.get_exit_surface_wave_f32(), s.get_error()
 
+    phase = {"readback_s": 0.0, "inputs_s": 0.0, "queue_s": 0.0, "device_wait_s": 0.0}
+
+    def timed(key, f):
+        t = time.perf_counter()
+        f()
+        phase[key] += time.perf_counter() - t
+
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
     for k in range(args.steps):
-        if dist:
-            dist.barrier()
-        t0 = time.perf_counter()
-        list(pool.map(lambda s: prepare(s, k), solvers))
-        run_program(pynadia, solvers)
-        results = list(pool.map(collect, solvers))
-        e2e_times.append(time.perf_counter() - t0)
+        timed("inputs_s", lambda: list(pool.map(lambda s: prepare(s, k), solvers)))
+        timed("queue_s", lambda: run_program(pynadia, solvers))  # returns once queued
+        timed("device_wait_s", lambda: [s.synchronize() for s in solvers])
+        timed("readback_s", lambda: list(pool.map(collect, solvers)))
+    e2e_times.append(time.perf_counter() - t0)
     pool.shutdown()
     e2e_rate = replicas.job_rate(B * args.steps, sum(e2e_times), device="cuda")
     e2e = {"value": e2e_rate, "unit": "recon/s",
-           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "host_wall_s": {k: round(v, 3) for k, v in phase.items()}}
 
     line = None
     if rank == 0:

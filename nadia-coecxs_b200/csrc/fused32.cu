@@ -662,11 +662,13 @@ void Fused32::Impl::use_choice(const f32::Choice *c)
 
 void Fused32::Impl::push_slot()
 {
-    push_slot_async(S.st);
-    NADIA_CUDA(cudaStreamSynchronize(S.st));
+    if (push_slot_async(S.st)) NADIA_CUDA(cudaStreamSynchronize(S.st));
 }
 
-void Fused32::Impl::push_slot_async(cudaStream_t st)
+// Uploads the descriptor only when it changed since the last upload: a copy
+// from pageable memory may wait for the stream's queued work, which would
+// stop the host from queueing further iterations while the device runs.
+bool Fused32::Impl::push_slot_async(cudaStream_t st)
 {
     const double *w = S.w;
     h_slot.er = (S.algorithm == NADIA_ER);
@@ -675,8 +677,12 @@ void Fused32::Impl::push_slot_async(cudaStream_t st)
     h_slot.w_ps = (float)w[PS];
     h_slot.w_psf = (float)w[PSF];
     h_slot.project = h_slot.er || w[PF] != 0 || w[PSF] != 0;
+    if (slot_uploaded && std::memcmp(&h_slot, &slot_on_device, sizeof(Slot)) == 0) return false;
     // pageable source: the copy is staged before this returns
     NADIA_CUDA(cudaMemcpyAsync(slot.p, &h_slot, sizeof(Slot), cudaMemcpyHostToDevice, st));
+    slot_on_device = h_slot;
+    slot_uploaded = true;
+    return true;
 }
 
 // Host arrays are in the reference's order (element (x, y) at x*ny + y); the

@@ -140,6 +140,8 @@ struct Fused32::Impl {
     DevBuf<f32::Slot> slot;
     DevBuf<f32::Slot *> slot_ptr;
     f32::Slot h_slot{};
+    f32::Slot slot_on_device{}; // the descriptor as last uploaded
+    bool slot_uploaded = false;
     const float2 *twx = nullptr, *twy = nullptr;
     const f32::Choice *choice = nullptr;
     std::vector<double> h_bs;
@@ -154,7 +156,7 @@ struct Fused32::Impl {
     explicit Impl(Solver &s);
     ~Impl();
     void push_slot();
-    void push_slot_async(cudaStream_t st);
+    bool push_slot_async(cudaStream_t st); // false: the device copy was current
     // the variants the next launches use (the handle's own, or a batch's);
     // sets the column-block count the row pass sums over
     void use_choice(const f32::Choice *c);
