@@ -45,7 +45,7 @@ enum {
 };
 
 /* geometries */
-enum { NADIA_PLANAR = 0, NADIA_FRESNEL = 1, NADIA_POLY = 2 };
+enum { NADIA_PLANAR = 0, NADIA_FRESNEL = 1, NADIA_POLY = 2, NADIA_FRESNEL_WF = 3 };
 
 /* arithmetic forms */
 enum { NADIA_FP64 = 0, NADIA_FP32 = 1 };
@@ -82,6 +82,24 @@ int nadia_fresnel_create(int nx, int ny, int precision, const double *white_fiel
  * set with nadia_set_relaxation_parameter. */
 int nadia_poly_create(int nx, int ny, int precision, double beta, int n_best,
                       nadia_solver **out);
+
+/* FresnelCDI_WF(initial_guess, wavelength, zone_focal_length,
+ * focal_detector_length, pixel_size, n_best) -- NADIA/src/FresnelCDI_WF.c++:17-79:
+ * recovery of the white field (the detector-plane illumination that
+ * FresnelCDI consumes) from a white-field measurement; the estimate is the
+ * detector-plane field.  FP64 form only (NADIA_FP32 returns
+ * NADIA_ERR_UNSUPPORTED).  Its algorithm is fixed (FresnelCDI_WF.c++:155-162):
+ * set_algorithm, set_custom_algorithm and set_relaxation_parameter return
+ * NADIA_ERR_UNSUPPORTED, where the reference prints a warning. */
+int nadia_fresnel_wf_create(int nx, int ny, int precision, double beam_wavelength,
+                            double zone_focal_length, double focal_detector_length,
+                            double pixel_size, int n_best, nadia_solver **out);
+
+/* FresnelCDI_WF::set_support(z_diameter, size) -- FresnelCDI_WF.c++:184-203:
+ * the disk the zone plate of diameter z_diameter projects (scaled by size,
+ * the reference's default 1.01) set to 1, then the support blurred (sigma 3,
+ * 5-pixel cut-off). */
+int nadia_fresnel_wf_set_support(nadia_solver *s, double z_diameter, double size);
 
 /* Releases the device memory and stream of a handle (NULL is accepted). */
 int nadia_destroy(nadia_solver *s);

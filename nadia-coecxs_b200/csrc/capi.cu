@@ -77,6 +77,16 @@ int create(int kind, int nx, int ny, int prec, int n_best, nadia_solver **out,
     });
 }
 
+// FresnelCDI_WF overrides the algorithm setters with warnings
+// (FresnelCDI_WF.h:147-181): its iteration is fixed
+Solver &settable(nadia_solver *h)
+{
+    Solver &s = S(h);
+    NADIA_REQUIRE(s.kind != NADIA_FRESNEL_WF, NADIA_ERR_UNSUPPORTED,
+                  "the algorithm of a FresnelCDI_WF reconstruction can not be set");
+    return s;
+}
+
 } // namespace
 
 extern "C" {
@@ -103,6 +113,20 @@ int nadia_fresnel_create(int nx, int ny, int precision, const double *white_fiel
         s.fresnel_init(white_field, beam_wavelength, focal_detector_length, focal_sample_length,
                        pixel_size, normalisation);
     });
+}
+
+int nadia_fresnel_wf_create(int nx, int ny, int precision, double beam_wavelength,
+                            double zone_focal_length, double focal_detector_length,
+                            double pixel_size, int n_best, nadia_solver **out)
+{
+    return create(NADIA_FRESNEL_WF, nx, ny, precision, n_best, out, [&](Solver &s) {
+        s.fresnel_wf_init(beam_wavelength, zone_focal_length, focal_detector_length, pixel_size);
+    });
+}
+
+int nadia_fresnel_wf_set_support(nadia_solver *h, double z_diameter, double size)
+{
+    return guard([&] { S(h).fresnel_wf_set_support(z_diameter, size); });
 }
 
 int nadia_poly_create(int nx, int ny, int precision, double beta, int n_best,
@@ -179,17 +203,17 @@ int nadia_poly_get_padding(const nadia_solver *h, int *px, int *py)
 
 int nadia_set_algorithm(nadia_solver *h, int alg)
 {
-    return guard([&] { S(h).set_algorithm(alg); });
+    return guard([&] { settable(h).set_algorithm(alg); });
 }
 
 int nadia_set_custom_algorithm(nadia_solver *h, const double m[10])
 {
-    return guard([&] { need(m, "m"); S(h).set_custom(m); });
+    return guard([&] { need(m, "m"); settable(h).set_custom(m); });
 }
 
 int nadia_set_relaxation_parameter(nadia_solver *h, double beta)
 {
-    return guard([&] { S(h).set_relaxation_parameter(beta); });
+    return guard([&] { settable(h).set_relaxation_parameter(beta); });
 }
 
 int nadia_get_algorithm_structure(const nadia_solver *h, double w[5], int *algorithm)

@@ -41,6 +41,7 @@ size_t footprint_bytes(int kind, int nx, int ny, int prec, int n_best, int pad_n
         b += 8 * 64;                   // blur kernel table
         b += (size_t)n_best * 16 * n;
         if (kind == NADIA_FRESNEL) b += 16 * n + 16 * n + 16 * (size_t)(nx / 2) * (ny / 2);
+        if (kind == NADIA_FRESNEL_WF) b += 16 * (size_t)(nx / 2) * (ny / 2);
         if (kind == NADIA_POLY)
             b += 16 * (size_t)nlambda + 16 * (size_t)pad_nx * pad_ny + 8 * n +
                  16 * (size_t)(pad_nx + pad_ny);

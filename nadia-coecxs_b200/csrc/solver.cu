@@ -82,7 +82,10 @@ double host_max(const double *a, size_t n)
 Solver::Solver(int kind_, int nx_, int ny_, int prec_, int n_best_)
     : kind(kind_), nx(nx_), ny(ny_), prec(prec_), n_best(n_best_)
 {
-    NADIA_REQUIRE(kind >= NADIA_PLANAR && kind <= NADIA_POLY, NADIA_ERR_INVALID, "unknown kind");
+    NADIA_REQUIRE(kind >= NADIA_PLANAR && kind <= NADIA_FRESNEL_WF, NADIA_ERR_INVALID,
+                  "unknown kind");
+    NADIA_REQUIRE(kind != NADIA_FRESNEL_WF || prec == NADIA_FP64, NADIA_ERR_UNSUPPORTED,
+                  "FresnelCDI_WF runs in the FP64 form");
     NADIA_REQUIRE(prec == NADIA_FP64 || prec == NADIA_FP32, NADIA_ERR_INVALID,
                   "unknown precision");
     NADIA_REQUIRE(nx >= 2 && ny >= 2 && nx % 2 == 0 && ny % 2 == 0, NADIA_ERR_INVALID,
@@ -330,6 +333,59 @@ void Solver::fresnel_set_experimental_parameters(double wl, double zfd_, double 
     }
 }
 
+// FresnelCDI_WF::FresnelCDI_WF, FresnelCDI_WF.c++:31-79: the quarter table
+// of the zone-plate-to-detector factor, (sin phi, -cos phi) / sqrt(nx*ny),
+// computed on the host in the reference's operation order (pow(x, 2) included)
+void Solver::fresnel_wf_init(double wl, double zone_focal, double focal_detector, double pixel_)
+{
+    AllocScope scope(st);
+    NADIA_REQUIRE(kind == NADIA_FRESNEL_WF, NADIA_ERR_INVALID, "needs a FresnelCDI_WF handle");
+    NADIA_REQUIRE(wl > 0 && zone_focal != 0 && focal_detector != 0 && pixel_ > 0,
+                  NADIA_ERR_INVALID, "FresnelCDI_WF needs a wavelength, non-zero distances and "
+                                     "a pixel size");
+    wavelength = wl;
+    z12 = zone_focal;
+    z23 = focal_detector;
+    pixel = pixel_;
+    const int qy = ny / 2;
+    const double x_mid = (nx - 1) / 2.0, y_mid = (ny - 1) / 2.0;
+    const double scaling_x = wl * z23 / (pixel * nx);
+    const double scaling_y = wl * z23 / (pixel * ny);
+    const double nrm = 1 / (sqrt(nx * ny));
+    std::vector<double2> hc((size_t)(nx / 2) * qy);
+    for (int i = 0; i < nx / 2; i++)
+        for (int j = 0; j < qy; j++) {
+            double rho_2 = pow(scaling_x * (x_mid - i), 2) + pow(scaling_y * (y_mid - j), 2);
+            double phi = rho_2 / z12 + rho_2 / z23;
+            phi *= M_PI / wl;
+            hc[(size_t)i * qy + j] = make_double2(sin(phi) * nrm, -cos(phi) * nrm);
+        }
+    coef.alloc(hc.size());
+    h2d(coef.p, hc.data(), coef.bytes(), st);
+}
+
+// FresnelCDI_WF::set_support(z_diameter, size), FresnelCDI_WF.c++:184-203:
+// the projected zone-plate disk (centre (nx-1)/2 in integer arithmetic, on
+// both axes) set to 1 over the current support, then convolve(support, 3, 5)
+void Solver::fresnel_wf_set_support(double z_diameter, double size)
+{
+    AllocScope scope(st);
+    NADIA_REQUIRE(kind == NADIA_FRESNEL_WF, NADIA_ERR_INVALID, "needs a FresnelCDI_WF handle");
+    if (!h_support_valid) get_support(h_support.data());
+    const double center_pixel = (nx - 1) / 2;
+    const double delta_z = (z12 / z23) * pixel;
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++) {
+            double i_ = i - center_pixel;
+            double j_ = j - center_pixel;
+            double r = delta_z * sqrt(i_ * i_ + j_ * j_);
+            if (r < size * z_diameter / 2.0) h_support[(size_t)i * ny + j] = 1;
+        }
+    upload_support();
+    plain_convolve(support.p, 3, 5);
+    h_support_valid = false;
+}
+
 // FresnelCDI::set_norm, FresnelCDI.c++:139-148
 void Solver::fresnel_set_norm(double nn)
 {
@@ -433,6 +489,16 @@ void Solver::initialise_estimate(int seed)
     }
     if (!h_support_valid) {
         get_support(h_support.data());
+    }
+    if (kind == NADIA_FRESNEL_WF) {
+        // FresnelCDI_WF::initialise_estimate, FresnelCDI_WF.c++:134-152: sqrt(I)
+        // inside the support, 0 outside (the seed is not used)
+        for (size_t k = 0; k < n; ++k) {
+            h[2 * k] = h_support[k] ? h_isqrt[k] : 0;
+            h[2 * k + 1] = 0;
+        }
+        set_esw(h.data());
+        return;
     }
     int max_value = (int)host_max(h_isqrt.data(), n);
     for (size_t k = 0; k < n; ++k) {
@@ -542,7 +608,13 @@ void Solver::get_illumination_at_sample(double *h)
 void Solver::plain_propagate_to(double2 *c, bool pg)
 {
     AllocScope scope(st);
-    if (kind == NADIA_FRESNEL) {
+    if (kind == NADIA_FRESNEL_WF) {
+        // FresnelCDI_WF::propagate_to_detector, FresnelCDI_WF.c++:176-182
+        fft.exec(c, true, st);
+        plain::multiply_factors(c, coef.p, nx, ny, -1, st);
+        plain::invert(c, nx, ny, true, st);
+        fft.exec(c, true, st);
+    } else if (kind == NADIA_FRESNEL) {
         // FresnelCDI::propagate_to_detector, FresnelCDI.c++:245-250
         plain::invert(c, nx, ny, true, st);
         fft.exec(c, true, st);
@@ -561,7 +633,13 @@ void Solver::plain_propagate_to(double2 *c, bool pg)
 void Solver::plain_propagate_from(double2 *c, bool pg)
 {
     AllocScope scope(st);
-    if (kind == NADIA_FRESNEL) {
+    if (kind == NADIA_FRESNEL_WF) {
+        // FresnelCDI_WF::propagate_from_detector, FresnelCDI_WF.c++:165-173
+        fft.exec(c, false, st);
+        plain::invert(c, nx, ny, true, st);
+        plain::multiply_factors(c, coef.p, nx, ny, +1, st);
+        fft.exec(c, false, st);
+    } else if (kind == NADIA_FRESNEL) {
         // FresnelCDI::propagate_from_detector, FresnelCDI.c++:238-243
         plain::multiply_factors(c, coef.p, nx, ny, +1, st);
         fft.exec(c, false, st);
@@ -626,6 +704,14 @@ void Solver::plain_iterate_once()
 {
     AllocScope scope(st);
     const size_t nb = n * sizeof(double2);
+    if (kind == NADIA_FRESNEL_WF) {
+        // FresnelCDI_WF::iterate, FresnelCDI_WF.c++:155-162: a fixed algorithm
+        plain_propagate_from(x.p, false);
+        plain::support_constraint(x.p, support.p, n, st);
+        plain_propagate_to(x.p, false);
+        plain_scale(x.p);
+        return;
+    }
     if (algorithm == NADIA_ER) {
         plain_project(x.p);
         plain::support_constraint(x.p, support.p, n, st);
@@ -706,7 +792,8 @@ void Solver::iterate(int count)
         else
             f32->iterate(1);
         if (prec == NADIA_FP64) record_error();
-        update_n_best();
+        if (kind != NADIA_FRESNEL_WF) update_n_best(); // FresnelCDI_WF::iterate keeps none
+
     }
     NADIA_CUDA(cudaGetLastError());
 }

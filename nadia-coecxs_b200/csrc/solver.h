@@ -60,6 +60,7 @@ struct Solver {
     // FresnelCDI
     std::vector<double> h_illum; // detector white field x norm (interleaved)
     double norm = 1, wavelength = 0, zfd = 0, zfs = 0, pixel = 0;
+    double z12 = 0, z23 = 0; // FresnelCDI_WF: zone plate to focus, focus to detector
     DevBuf<double2> illum, illum_sample, coef;
 
     // PolyCDI
@@ -86,6 +87,8 @@ struct Solver {
     void fresnel_set_experimental_parameters(double wl, double zfd, double zfs, double pixel);
     void fresnel_set_norm(double nn);
     void fresnel_auto_set_norm();
+    void fresnel_wf_init(double wl, double zone_focal, double focal_detector, double pixel);
+    void fresnel_wf_set_support(double z_diameter, double size);
 
     // algorithm
     void set_algorithm(int alg);

@@ -22,9 +22,9 @@ LIB_PATH = os.path.join(PKG, "libnadia_b200.so")
 ER, BIO, BOO, HIO, DM, SF, ASR, HPR, RAAR, CUSTOM = range(10)
 ALGORITHMS = {"ER": ER, "BIO": BIO, "BOO": BOO, "HIO": HIO, "DM": DM, "SF": SF, "ASR": ASR,
               "HPR": HPR, "RAAR": RAAR}
-PLANAR, FRESNEL, POLY = 0, 1, 2
+PLANAR, FRESNEL, POLY, FRESNEL_WF = 0, 1, 2, 3
 FP64, FP32 = 0, 1
-KINDS = {"planar": PLANAR, "fresnel": FRESNEL, "poly": POLY}
+KINDS = {"planar": PLANAR, "fresnel": FRESNEL, "poly": POLY, "fresnel_wf": FRESNEL_WF}
 
 STATUS = {0: "OK", 1: "INVALID", 2: "STATE", 3: "UNSUPPORTED", 4: "CUDA", 5: "NOMEM",
           6: "RANGE"}
@@ -67,6 +67,9 @@ _PROTOS = {
                                   ctypes.c_double, ctypes.c_double, ctypes.c_double, _I,
                                   ctypes.POINTER(_H)]),
     "nadia_poly_create": (_I, [_I, _I, _I, ctypes.c_double, _I, ctypes.POINTER(_H)]),
+    "nadia_fresnel_wf_create": (_I, [_I, _I, _I, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_double, _I, ctypes.POINTER(_H)]),
+    "nadia_fresnel_wf_set_support": (_I, [_H, ctypes.c_double, ctypes.c_double]),
     "nadia_destroy": (_I, [_H]),
     "nadia_get_size": (_I, [_H, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "nadia_set_support": (_I, [_H, _D, _I]),
@@ -168,11 +171,12 @@ def custom_weights(m):
 
 
 class Solver:
-    """One reconstruction on the GPU (PlanarCDI / FresnelCDI / PolyCDI)."""
+    """One reconstruction on the GPU (PlanarCDI / FresnelCDI / PolyCDI /
+    FresnelCDI_WF)."""
 
     def __init__(self, kind, nx, ny, precision=FP64, n_best=0, white_field=None,
                  wavelength=None, focal_detector_length=None, focal_sample_length=None,
-                 pixel_size=None, normalisation=1.0, beta=0.9):
+                 pixel_size=None, normalisation=1.0, beta=0.9, zone_focal_length=None):
         self.lib = load()
         self.kind = kind
         self.nx, self.ny = int(nx), int(ny)
@@ -189,6 +193,10 @@ class Solver:
                                                  ctypes.byref(h)))
         elif kind == "poly":
             _check(self.lib.nadia_poly_create(nx, ny, precision, beta, n_best, ctypes.byref(h)))
+        elif kind == "fresnel_wf":
+            _check(self.lib.nadia_fresnel_wf_create(nx, ny, precision, wavelength,
+                                                    zone_focal_length, focal_detector_length,
+                                                    pixel_size, n_best, ctypes.byref(h)))
         else:
             raise ValueError(kind)
         self.h = h
@@ -215,6 +223,10 @@ class Solver:
 
     def set_intensity(self, i):
         _check(self.lib.nadia_set_intensity(self.h, _ptr(self._real(i))))
+
+    def set_wf_support(self, z_diameter, size=1.01):
+        """FresnelCDI_WF::set_support(z_diameter, size)."""
+        _check(self.lib.nadia_fresnel_wf_set_support(self.h, float(z_diameter), float(size)))
 
     def set_beam_stop(self, b):
         _check(self.lib.nadia_set_beam_stop(self.h, _ptr(self._real(b))))

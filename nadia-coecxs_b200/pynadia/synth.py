@@ -17,7 +17,11 @@ objects with the shapes and value distributions of the benchmark workloads:
   |propagate_to_detector((T-1) L) + W|^2 (FresnelCDI.c++:217-250, 253-283);
 * Poly: a Gaussian spectrum of lines listed longest wavelength first, and
   the polychromatic intensity sum_l w_l |Psi(lf*(i-n/2)+n/2, ...)|^2 of
-  PolyCDI::expand_wl (NADIA/src/PolyCDI.c++:296-334).
+  PolyCDI::expand_wl (NADIA/src/PolyCDI.c++:296-334);
+* FresnelCDI_WF: a zone-plate-plane field (a disk with a smooth phase
+  aberration) carried to the detector by FresnelCDI_WF::propagate_to_detector
+  (NADIA/src/FresnelCDI_WF.c++:176-182), whose intensity is the white-field
+  measurement.
 
 Random numbers come from numpy's Philox counter-based generator (Philox4x64-10,
 Salmon et al. SC'11) and its Poisson sampler (PTRS for large means); every
@@ -232,3 +236,52 @@ class PolyCase:
         self.intensity = poisson_scale(I, photons, seed) if photons else I
         self.support = square_support(n, n, int(2.5 * radius_frac * n))
         self.padding = padding
+
+
+# ------------------------------------------------------------- FresnelCDI_WF
+
+def fresnel_wf_factor(nx, ny, wavelength, z12, z23, pixel):
+    """The zone-plate-to-detector factor of FresnelCDI_WF.c++:31-79 on the full
+    grid, at the folded indices of multiply_factors (FresnelCDI_WF.c++:98-124)."""
+    x_mid, y_mid = (nx - 1) / 2.0, (ny - 1) / 2.0
+    sx = wavelength * z23 / (pixel * nx)
+    sy = wavelength * z23 / (pixel * ny)
+    i_ = np.trunc(x_mid - np.abs(x_mid - np.arange(nx))).astype(int)
+    j_ = np.trunc(y_mid - np.abs(y_mid - np.arange(ny))).astype(int)
+    rho2 = (sx * (x_mid - i_))[:, None] ** 2 + (sy * (y_mid - j_))[None, :] ** 2
+    phi = (rho2 / z12 + rho2 / z23) * math.pi / wavelength
+    return (np.sin(phi) - 1j * np.cos(phi)) / math.sqrt(nx * ny)
+
+
+def fresnel_wf_to_detector(x, coef):
+    """FresnelCDI_WF::propagate_to_detector: FFT, x conj(coef), swap+scale, FFT."""
+    nx, ny = x.shape
+    y = np.fft.fft2(x) * np.conj(coef)
+    y = np.fft.fftshift(y) / math.sqrt(nx * ny)
+    return np.fft.fft2(y)
+
+
+class FresnelWFCase:
+    """A FresnelCDI_WF problem with the reference example's geometry
+    (wavelength 4.892e-10 m, zone plate 16.353 mm before focus, detector
+    0.909513 m after the zone plate, 13.5 um pixels); the zone-plate diameter
+    is scaled so that its projected disk has radius `radius_frac` of the grid."""
+
+    def __init__(self, n, seed, radius_frac=0.3, wavelength=4.892e-10, z12=16.353e-3,
+                 z23=0.909513 - 16.353e-3, pixel=13.5e-6, photons=None):
+        self.nx = self.ny = n
+        self.wavelength, self.z12, self.z23, self.pixel = wavelength, z12, z23, pixel
+        delta_z = (z12 / z23) * pixel
+        self.z_diameter = 2.0 * radius_frac * n * delta_z / 1.01
+        r = radius_frac * n
+        g = rng(seed)
+        ph = gaussian_filter(g.uniform(-np.pi, np.pi, (n, n)), 3.0, mode="wrap")
+        i = np.arange(n)[:, None] - (n - 1) // 2
+        j = np.arange(n)[None, :] - (n - 1) // 2
+        aberration = 0.5 * ((i * i + j * j) / (r * r)) ** 2
+        self.zone_field = disk_mask(n, n, 0.95 * r) * np.exp(1j * (ph + aberration))
+        coef = fresnel_wf_factor(n, n, wavelength, z12, z23, pixel)
+        self.white_field = fresnel_wf_to_detector(self.zone_field, coef)
+        I = np.abs(self.white_field) ** 2
+        self.intensity = poisson_scale(I, photons, seed) if photons else I
+

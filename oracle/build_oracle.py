@@ -29,6 +29,7 @@ REF_SOURCES = [
     "src/BaseCDI.c++",
     "src/PlanarCDI.c++",
     "src/FresnelCDI.c++",
+    "src/FresnelCDI_WF.c++",
     "src/PolyCDI.c++",
     "src/TransmissionConstraint.c++",
     "src/io_spec.c",

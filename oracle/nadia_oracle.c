@@ -29,7 +29,7 @@ CANON_FFT_DEFINE(d, double)
 
 enum { PSF, PFS, PS, PF, PI_ }; /* NADIA/include/BaseCDI.h:32 (term order) */
 enum { ER, BIO, BOO, HIO, DM, SF, ASR, HPR, RAAR, CUSTOM }; /* BaseCDI.h:37 */
-enum { KIND_PLANAR = 0, KIND_FRESNEL = 1, KIND_POLY = 2 };
+enum { KIND_PLANAR = 0, KIND_FRESNEL = 1, KIND_POLY = 2, KIND_FRESNEL_WF = 3 };
 
 typedef struct orc_solver {
     int kind, nx, ny;
@@ -51,6 +51,8 @@ typedef struct orc_solver {
     double *illum_sample;  /* illumination propagated to the sample plane */
     double *coef;          /* (nx/2)*(ny/2)*2 quarter table */
     double norm, wavelength, pixel, zfd, zfs;
+    /* FresnelCDI_WF: zone-plate-to-focus and focus-to-detector distances */
+    double z12, z23;
     /* PolyCDI */
     double *spectrum;      /* nlambda*2: (wavelength, weight) */
     int nlambda, px, py;
@@ -255,7 +257,13 @@ static void multiply_factors(orc_solver *s, double *c, int direction)
 
 static void propagate_to_detector(orc_solver *s, double *c)
 {
-    if (s->kind == KIND_FRESNEL) {
+    if (s->kind == KIND_FRESNEL_WF) {
+        /* FresnelCDI_WF::propagate_to_detector, FresnelCDI_WF.c++:176-182 */
+        canon_fft2d_execd(s->fft, (canon_cd *)c, 1);
+        multiply_factors(s, c, -1);
+        invert(c, s->nx, s->ny, 1);
+        canon_fft2d_execd(s->fft, (canon_cd *)c, 1);
+    } else if (s->kind == KIND_FRESNEL) {
         /* FresnelCDI::propagate_to_detector, FresnelCDI.c++:245-250 */
         invert(c, s->nx, s->ny, 1);
         canon_fft2d_execd(s->fft, (canon_cd *)c, 1);
@@ -273,7 +281,13 @@ static void propagate_to_detector(orc_solver *s, double *c)
 
 static void propagate_from_detector(orc_solver *s, double *c)
 {
-    if (s->kind == KIND_FRESNEL) {
+    if (s->kind == KIND_FRESNEL_WF) {
+        /* FresnelCDI_WF::propagate_from_detector, FresnelCDI_WF.c++:165-173 */
+        canon_fft2d_execd(s->fft, (canon_cd *)c, 0);
+        invert(c, s->nx, s->ny, 1);
+        multiply_factors(s, c, +1);
+        canon_fft2d_execd(s->fft, (canon_cd *)c, 0);
+    } else if (s->kind == KIND_FRESNEL) {
         /* FresnelCDI::propagate_from_detector, FresnelCDI.c++:238-243 */
         multiply_factors(s, c, +1);
         canon_fft2d_execd(s->fft, (canon_cd *)c, 0);
@@ -451,6 +465,15 @@ void orc_iterate(orc_solver *s)
 {
     size_t n = (size_t)s->nx * s->ny, nb = sizeof(double) * 2 * n;
     double *x = s->complex_;
+    if (s->kind == KIND_FRESNEL_WF) {
+        /* FresnelCDI_WF::iterate, FresnelCDI_WF.c++:155-162: a fixed algorithm
+         * on the detector-plane field, no n-best bookkeeping */
+        propagate_from_detector(s, x);
+        apply_support(s, x);
+        propagate_to_detector(s, x);
+        scale_intensity(s, x);
+        return;
+    }
     if (s->algorithm == ER) {
         project(s, x);
         apply_support(s, x);
@@ -532,6 +555,53 @@ static orc_solver *base_create(int kind, int nx, int ny, int n_best)
 orc_solver *orc_planar_create(int nx, int ny, int n_best)
 {
     return base_create(KIND_PLANAR, nx, ny, n_best);
+}
+
+/* FresnelCDI_WF::FresnelCDI_WF, FresnelCDI_WF.c++:31-79: the quarter table of
+ * the zone-plate-to-detector propagation factor, (sin phi, -cos phi)/sqrt(N) */
+orc_solver *orc_fresnel_wf_create(int nx, int ny, double wavelength, double zone_focal_length,
+                                  double focal_detector_length, double pixel_size, int n_best)
+{
+    orc_solver *s = base_create(KIND_FRESNEL_WF, nx, ny, n_best);
+    s->wavelength = wavelength;
+    s->z12 = zone_focal_length;
+    s->z23 = focal_detector_length;
+    s->pixel = pixel_size;
+    int qy = ny / 2;
+    s->coef = zd((size_t)2 * (nx / 2) * qy);
+    double x_mid = (nx - 1) / 2.0, y_mid = (ny - 1) / 2.0;
+    double z12 = s->z12, z23 = s->z23;
+    double scaling_x = wavelength * z23 / (pixel_size * nx);
+    double scaling_y = wavelength * z23 / (pixel_size * ny);
+    double norm = 1 / (sqrt(nx * ny));
+    for (int i = 0; i < nx / 2; i++)
+        for (int j = 0; j < qy; j++) {
+            double rho_2 = pow(scaling_x * (x_mid - i), 2) + pow(scaling_y * (y_mid - j), 2);
+            double phi = rho_2 / z12 + rho_2 / z23;
+            phi *= M_PI / wavelength;
+            s->coef[2 * ((size_t)i * qy + j)] = sin(phi) * norm;
+            s->coef[2 * ((size_t)i * qy + j) + 1] = -cos(phi) * norm;
+        }
+    return s;
+}
+
+/* FresnelCDI_WF::set_support(z_diameter, size), FresnelCDI_WF.c++:184-203: a
+ * disk of the zone plate's projected size (the centre is (nx-1)/2 in integer
+ * arithmetic, on both axes), then convolve(support, 3, 5); pixels outside the
+ * disk keep their earlier support values */
+void orc_fresnel_wf_set_support(orc_solver *s, double z_diameter, double size)
+{
+    int nx = s->nx, ny = s->ny;
+    double center_pixel = (nx - 1) / 2;
+    double delta_z = (s->z12 / s->z23) * s->pixel;
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++) {
+            double i_ = i - center_pixel;
+            double j_ = j - center_pixel;
+            double r = delta_z * sqrt(i_ * i_ + j_ * j_);
+            if (r < size * z_diameter / 2.0) s->support[(size_t)i * ny + j] = 1;
+        }
+    convolve(s->support, nx, ny, 3, 5);
 }
 
 /* FresnelCDI::set_experimental_parameters, FresnelCDI.c++:57-95 */
@@ -748,6 +818,15 @@ void orc_initialise_estimate(orc_solver *s, int seed)
 {
     size_t n = (size_t)s->nx * s->ny;
     srand(seed);
+    if (s->kind == KIND_FRESNEL_WF) {
+        /* FresnelCDI_WF::initialise_estimate, FresnelCDI_WF.c++:134-152:
+         * sqrt(I) inside the support, 0 outside (the seed is unused) */
+        for (size_t k = 0; k < n; ++k) {
+            s->complex_[2 * k] = s->support[k] ? s->isqrt[k] : 0;
+            s->complex_[2 * k + 1] = 0;
+        }
+        return;
+    }
     if (s->kind == KIND_FRESNEL) {
         double *t = zd(2 * n);
         for (size_t k = 0; k < n; ++k) {

@@ -42,6 +42,9 @@ _PROTOS = {
     "fresnel_create": (_V, [ctypes.c_int, ctypes.c_int, _D, ctypes.c_double, ctypes.c_double,
                             ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
     "poly_create": (_V, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+    "fresnel_wf_create": (_V, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                               ctypes.c_double, ctypes.c_double, ctypes.c_int]),
+    "fresnel_wf_set_support": (None, [_V, ctypes.c_double, ctypes.c_double]),
     "destroy": (None, [_V]),
     "set_support": (None, [_V, _D, ctypes.c_int]),
     "set_intensity": (None, [_V, _D]),
@@ -142,11 +145,12 @@ def read_spec(path, capacity=4096):
 
 
 class _Solver:
-    """One reconstruction (PlanarCDI / FresnelCDI / PolyCDI) on a CPU library."""
+    """One reconstruction (PlanarCDI / FresnelCDI / PolyCDI / FresnelCDI_WF) on a
+    CPU library."""
 
     def __init__(self, lib, kind, nx, ny, n_best=0, white_field=None, wavelength=None,
                  focal_detector_length=None, focal_sample_length=None, pixel_size=None,
-                 normalisation=1.0, beta=0.9):
+                 normalisation=1.0, beta=0.9, zone_focal_length=None):
         self.L = lib
         self.kind = kind
         self.nx, self.ny = nx, ny
@@ -158,6 +162,9 @@ class _Solver:
                                         focal_sample_length, pixel_size, normalisation, n_best)
         elif kind == "poly":
             self.h = lib.poly_create(nx, ny, beta, n_best)
+        elif kind == "fresnel_wf":
+            self.h = lib.fresnel_wf_create(nx, ny, wavelength, zone_focal_length,
+                                           focal_detector_length, pixel_size, n_best)
         else:
             raise ValueError(kind)
 
@@ -229,6 +236,10 @@ class _Solver:
         out = np.zeros((self.nx, self.ny), dtype=np.complex128)
         self.L.get_illumination_at_sample(self.h, _ptr(out))
         return out
+
+    def set_wf_support(self, z_diameter, size=1.01):
+        """FresnelCDI_WF::set_support(z_diameter, size)."""
+        self.L.fresnel_wf_set_support(self.h, z_diameter, size)
 
     def auto_set_norm(self):
         self.L.fresnel_auto_set_norm(self.h)

@@ -16,11 +16,12 @@
 #include <BaseCDI.h>
 #include <PlanarCDI.h>
 #include <FresnelCDI.h>
+#include <FresnelCDI_WF.h>
 #include <PolyCDI.h>
 
 namespace {
 
-enum { KIND_PLANAR = 0, KIND_FRESNEL = 1, KIND_POLY = 2 };
+enum { KIND_PLANAR = 0, KIND_FRESNEL = 1, KIND_POLY = 2, KIND_FRESNEL_WF = 3 };
 
 struct RefSolver {
     int kind, nx, ny;
@@ -69,6 +70,23 @@ void *ref_planar_create(int nx, int ny, int n_best)
     s->wf = 0;
     s->cdi = new PlanarCDI(*s->esw, n_best);
     return s;
+}
+
+void *ref_fresnel_wf_create(int nx, int ny, double wavelength, double zone_focal_length,
+                            double focal_detector_length, double pixel, int n_best)
+{
+    RefSolver *s = new RefSolver();
+    s->kind = KIND_FRESNEL_WF; s->nx = nx; s->ny = ny;
+    s->esw = new Complex_2D(nx, ny);
+    s->wf = 0;
+    s->cdi = new FresnelCDI_WF(*s->esw, wavelength, zone_focal_length, focal_detector_length,
+                               pixel, n_best);
+    return s;
+}
+
+void ref_fresnel_wf_set_support(void *h, double z_diameter, double size)
+{
+    static_cast<FresnelCDI_WF *>(S(h)->cdi)->set_support(z_diameter, size);
 }
 
 void *ref_fresnel_create(int nx, int ny, const double *white_field, double wavelength,

@@ -6,7 +6,7 @@
 // estimate read back every 10 iterations), reading inputs from and writing
 // results to raw little-endian float64 files in a directory.
 //
-//   cdi_program <planar|fresnel|poly|example> <nx> <ny> <dir> [padding]
+//   cdi_program <planar|fresnel|poly|example|wf> <nx> <ny> <dir> [padding]
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -17,6 +17,7 @@
 #include <Complex_2D.h>
 #include <Double_2D.h>
 #include <FresnelCDI.h>
+#include <FresnelCDI_WF.h>
 #include <PlanarCDI.h>
 #include <PolyCDI.h>
 
@@ -190,6 +191,31 @@ static int poly(int nx, int ny, int padding)
     return 0;
 }
 
+// FresnelCDI_WF: the sequence of tests/scenarios.py's fresnel_wf_mixed
+static int white_field(int nx, int ny)
+{
+    std::vector<double> p = load("params.bin", 5);
+    Complex_2D wf(nx, ny);
+    FresnelCDI_WF proj(wf, p[0], p[1], p[2], p[3]);
+    proj.set_support(p[4]);
+    proj.set_intensity(real_2d("intensity.bin", nx, ny));
+    proj.initialise_estimate(0);
+    save_complex("init.bin", wf);
+    save_real("support0.bin", proj.get_support());
+    proj.set_algorithm(HIO); // prints the reference's warning and changes nothing
+    std::vector<double> errs;
+    const int iterations = 12;
+    for (int it = 0; it < iterations; ++it) {
+        proj.iterate();
+        errs.push_back(proj.get_error());
+        if (it == iterations / 2) proj.apply_shrinkwrap(1.5, 0.1);
+    }
+    save("errors.bin", errs);
+    save_complex("esw.bin", wf);
+    save_real("support_out.bin", proj.get_support());
+    return 0;
+}
+
 // the flow of the reference's PlanarCDI example, two short cycles
 static int example(int nx, int ny)
 {
@@ -253,6 +279,7 @@ int main(int argc, char **argv)
         if (mode == "fresnel") return fresnel(nx, ny);
         if (mode == "poly") return poly(nx, ny, argc > 5 ? std::atoi(argv[5]) : 0);
         if (mode == "example") return example(nx, ny);
+        if (mode == "wf") return white_field(nx, ny);
     } catch (const nadia_cxx::Failure &e) {
         std::cerr << "failure " << e.code << ": " << e.what() << std::endl;
         return 4;

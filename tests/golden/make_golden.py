@@ -1,13 +1,13 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
 The reference's own hot-path sources (NADIA/src/{Complex_2D,BaseCDI,PlanarCDI,
-FresnelCDI,PolyCDI}.c++), compiled unmodified in their double build against
+FresnelCDI,FresnelCDI_WF,PolyCDI}.c++), compiled unmodified in their double build against
 the FFTW shim by oracle/build_oracle.py, run the scenarios of tests/scenarios.py
 on the synthetic inputs of pynadia.synth.  Each fixture stores the outputs
 and a digest of the inputs it was made from.
 
 Run (needs the reference sources, i.e. in the build container):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 """
 import hashlib
 import os
@@ -29,6 +29,7 @@ CASES = {
     "planar_custom_32": (sc.planar_custom, dict(n=32)),
     "fresnel_mixed_32": (sc.fresnel_mixed, dict(n=32)),
     "poly_mixed_32": (sc.poly_mixed, dict(n=32, padding=2)),
+    "fresnel_wf_mixed_32": (sc.fresnel_wf_mixed, dict(n=32)),
 }
 
 
@@ -39,6 +40,9 @@ def input_digest(name):
     if name.startswith("planar"):
         c = sc.planar_inputs(n, ny=kw.get("ny"), beam_stop=0 if "custom" in name else 4)
         arrs = [c.intensity, c.support]
+    elif name.startswith("fresnel_wf"):
+        f = sc.fresnel_wf_inputs(n)
+        arrs = [f.intensity, np.array([f.z_diameter, f.wavelength, f.z12, f.z23, f.pixel])]
     elif name.startswith("fresnel"):
         f = sc.fresnel_inputs(n)
         arrs = [f.intensity, f.support, f.white_field]
@@ -54,10 +58,12 @@ def reference_factory(kind, nx, ny, **kw):
     return po.Reference(kind, nx, ny, variant="64", **kw)
 
 
-def main():
+def main(names=None):
     if not po.reference_available("64"):
         sys.exit("oracle/_ref not built (python oracle/build_oracle.py with the reference present)")
     for name, (fn, kw) in CASES.items():
+        if names and name not in names:
+            continue
         res = fn(reference_factory, **kw)
         out = {k: v for k, v in res.items() if v is not None}
         out["input_digest"] = np.array(input_digest(name))
@@ -66,4 +72,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -156,3 +156,33 @@ def rel_err(a, b):
     d = np.abs(a - b).max()
     m = np.abs(b).max()
     return d / m if m else d
+
+
+def fresnel_wf_inputs(n, seed=6):
+    return synth.FresnelWFCase(n, seed=seed)
+
+
+def fresnel_wf_mixed(make, n=32, seed=6, iterations=12):
+    """FresnelCDI_WF: the projected zone-plate support, sqrt(I) initial
+    estimate, the fixed algorithm, a shrinkwrap, and the single operators."""
+    f = fresnel_wf_inputs(n, seed)
+    s = make("fresnel_wf", n, n, wavelength=f.wavelength, zone_focal_length=f.z12,
+             focal_detector_length=f.z23, pixel_size=f.pixel)
+    s.set_wf_support(f.z_diameter)
+    s.set_intensity(f.intensity)
+    s.initialise_estimate(0)
+    out = {"init": s.get_exit_surface_wave(), "support0": s.get_support()}
+    errs = []
+    for it in range(iterations):
+        s.iterate()
+        errs.append(s.get_error())
+        if it == iterations // 2:
+            s.apply_shrinkwrap(1.5, 0.1)
+    out["errors"] = np.array(errs)
+    out["esw"] = s.get_exit_surface_wave()
+    out["support"] = s.get_support()
+    g = np.random.default_rng(seed)
+    field = g.standard_normal((n, n)) + 1j * g.standard_normal((n, n))
+    out["to_detector"] = s.propagate_to_detector(field)
+    out["from_detector"] = s.propagate_from_detector(field)
+    return out

@@ -154,6 +154,23 @@ def test_poly(programs, tmp_path, double):
     assert sc.rel_err(got, out_round(double, ref["esw"])) <= (1e-10 if double else 1e-6)
 
 
+@pytest.mark.parametrize("double", [True, False])
+def test_fresnel_wf(programs, tmp_path, double):
+    n = 64
+    f = sc.fresnel_wf_inputs(n)
+    put(tmp_path, "intensity.bin", f.intensity)
+    put(tmp_path, "params.bin", [f.wavelength, f.z12, f.z23, f.pixel, f.z_diameter])
+    run(programs[double], "wf", n, n, tmp_path)
+    ref = sc.fresnel_wf_mixed(oracle_factory(double), n=n)
+    assert_errors(get(tmp_path, "errors.bin"), ref["errors"])
+    for key in ("init", "esw"):
+        got = get(tmp_path, key + ".bin", (n, n), cplx=True)
+        assert np.array_equal(got, out_round(double, ref[key])), key
+    assert np.array_equal(get(tmp_path, "support0.bin", (n, n)), out_round(double, ref["support0"]))
+    assert np.array_equal(get(tmp_path, "support_out.bin", (n, n)),
+                          out_round(double, ref["support"]))
+
+
 def example_oracle(make, nx, ny, intensity, support):
     s = make("planar", nx, ny, n_best=4)
     s.set_support(support)

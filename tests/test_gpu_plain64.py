@@ -46,7 +46,7 @@ def compare(a, b, exact_keys=(), tol=TOL):
 
 
 @pytest.mark.parametrize("name", ["planar_mixed_32", "planar_mixed_32x48", "planar_custom_32",
-                                  "fresnel_mixed_32", "poly_mixed_32"])
+                                  "fresnel_mixed_32", "poly_mixed_32", "fresnel_wf_mixed_32"])
 def test_golden(name):
     g = np.load(os.path.join(GOLDEN, name + ".npz"))
     import importlib.util
@@ -57,7 +57,8 @@ def test_golden(name):
     fn, kw = mg.CASES[name]
     res = fn(gpu, **kw)
     exact = () if name.startswith("poly") else ("esw", "support", "init", "transmission", "best",
-                                                 "illum")
+                                                 "illum", "support0", "to_detector",
+                                                 "from_detector")
     compare(res, g, exact_keys=exact)
 
 
@@ -65,6 +66,26 @@ def test_golden(name):
 def test_planar_vs_oracle(n, ny):
     compare(sc.planar_mixed(gpu, n=n, ny=ny), sc.planar_mixed(orc, n=n, ny=ny),
             exact_keys=("esw", "support", "init", "best"))
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_fresnel_wf_vs_oracle(n):
+    compare(sc.fresnel_wf_mixed(gpu, n=n), sc.fresnel_wf_mixed(orc, n=n),
+            exact_keys=("esw", "support", "init", "support0", "to_detector", "from_detector"))
+
+
+def test_fresnel_wf_fixed_algorithm_and_fp64_only():
+    f = sc.fresnel_wf_inputs(32)
+    kw = dict(wavelength=f.wavelength, zone_focal_length=f.z12, focal_detector_length=f.z23,
+              pixel_size=f.pixel)
+    s = gpu("fresnel_wf", 32, 32, **kw)
+    for call in (lambda: s.set_algorithm("HIO"), lambda: s.set_relaxation_parameter(0.5)):
+        with pytest.raises(pynadia.NadiaError) as e:
+            call()
+        assert e.value.code == 3
+    with pytest.raises(pynadia.NadiaError) as e:
+        pynadia.Solver("fresnel_wf", 32, 32, precision=pynadia.FP32, **kw)
+    assert e.value.code == 3
 
 
 def test_fresnel_vs_oracle():

@@ -43,6 +43,11 @@ def test_fresnel():
     same(sc.fresnel_mixed(orc, n=64), sc.fresnel_mixed(ref, n=64))
 
 
+@pytest.mark.parametrize("n", [32, 64])
+def test_fresnel_wf(n):
+    same(sc.fresnel_wf_mixed(orc, n=n), sc.fresnel_wf_mixed(ref, n=n))
+
+
 @pytest.mark.parametrize("n,padding", [(48, 3), (64, 4)])
 def test_poly(n, padding):
     same(sc.poly_mixed(orc, n=n, padding=padding), sc.poly_mixed(ref, n=n, padding=padding))
