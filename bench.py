@@ -59,6 +59,8 @@ def parse():
                    help="items in the FresnelCDI uneven-size batch report (0 = skip)")
     p.add_argument("--fresnel-only", action="store_true",
                    help="print the FresnelCDI batch report only")
+    p.add_argument("--no-wf", action="store_true", help="skip the FresnelCDI_WF report")
+    p.add_argument("--wf-only", action="store_true", help="print the FresnelCDI_WF report only")
     p.add_argument("--quick-poly", action="store_true",
                    help="device-resident FP32 PolyCDI steps only (1024^2 padded to 1080^2; "
                         "for profiling)")
@@ -381,6 +383,54 @@ def fresnel_batch_report(pynadia, synth, n_items=64, iters=300):
     return out
 
 
+def white_field_report(pynadia, synth, n=2048, iters=26):
+    """FresnelCDI_WF at the reference example's size (1024^2 data padded by
+    512 on each side), 26 iterations: the FP64 form on the GPU (CUDA events)
+    against the reference's float build on one host core (one timed
+    iteration).  Algorithmic bytes of the FP64 form per pixel and iteration:
+    four 2-D transforms of two passes (4 x 2 x 32), two quadrant swaps (2 x
+    32), two factor multiplies (2 x 32), the support (40) and the modulus (40)
+    = 464."""
+    import torch
+    f = synth.FresnelWFCase(n, seed=21)
+    kw = dict(wavelength=f.wavelength, zone_focal_length=f.z12, focal_detector_length=f.z23,
+              pixel_size=f.pixel)
+    s = pynadia.Solver("fresnel_wf", n, n, precision=pynadia.FP64, **kw)
+    s.set_wf_support(f.z_diameter)
+    s.set_intensity(f.intensity)
+    s.initialise_estimate(0)
+    s.iterate(2)
+    s.synchronize()
+    st = torch.cuda.ExternalStream(s.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    s.iterate(iters)
+    b.record(st)
+    b.synchronize()
+    sec = a.elapsed_time(b) / 1000.0
+    err = s.get_error()
+    s.close()
+    peak, _ = measured_peak()
+    gbs = 464.0 * n * n * iters / sec / 1e9
+    out = {"grid": [n, n], "iterations": iters, "gpu_fp64_ms_per_iteration": 1000.0 * sec / iters,
+           "gpu_fp64_recon_per_s": 1.0 / sec, "final_error": err,
+           "hbm_gbs_algorithmic": gbs, "roofline_frac": gbs / peak}
+    sys.path.insert(0, ORACLE)
+    import pyoracle as po
+    if po.reference_available("32_fast"):
+        r = po.Reference("fresnel_wf", n, n, variant="32_fast", **kw)
+        r.set_wf_support(f.z_diameter)
+        r.set_intensity(f.intensity)
+        r.initialise_estimate(0)
+        t = time.perf_counter()
+        r.iterate(1)
+        cpu = time.perf_counter() - t
+        out["cpu_reference_float_s_per_iteration"] = cpu
+        out["cpu_reference_recon_per_s_one_core"] = 1.0 / (cpu * iters)
+        out["gpu_over_cpu_one_core"] = (cpu * iters) / sec
+    return out
+
+
 def quick_poly(pynadia, synth, args):
     """`args.batch` FP32 PolyCDI reconstructions of 1024^2 padded to 1080^2
     (10-line spectrum, 5% FWHM), HIO, stepped together; per-pass device times."""
@@ -428,6 +478,8 @@ def ours(args, rank, world, local_rank):
         return {"serving": serving_report(pynadia, synth, n_req=args.serve_requests)}
     if args.quick_poly:
         return quick_poly(pynadia, synth, args)
+    if args.wf_only:
+        return {"white_field": white_field_report(pynadia, synth)}
     if args.fresnel_only:
         return {"fresnel_batch": fresnel_batch_report(pynadia, synth, n_items=args.fresnel_batch)}
     dist = None
@@ -603,6 +655,8 @@ def ours(args, rank, world, local_rank):
         if args.fresnel_batch > 0:
             fresnel_batch = fresnel_batch_report(pynadia, synth, n_items=args.fresnel_batch)
 
+        white_field = white_field_report(pynadia, synth) if not args.no_wf else None
+
         serving = None
         if args.serve_requests > 0:
             serving = serving_report(pynadia, synth, n_req=args.serve_requests)
@@ -629,7 +683,7 @@ def ours(args, rank, world, local_rank):
                            "note": "per reconstruction in a batch = its batch's step time"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": launches, "fp64_plain": fp64, "accuracy": accuracy,
-            "serving": serving, "fresnel_batch": fresnel_batch,
+            "serving": serving, "fresnel_batch": fresnel_batch, "white_field": white_field,
         }
     if dist:
         dist.barrier()

@@ -11,7 +11,9 @@
 //   - propagate_to_detector / propagate_from_detector / scale_intensity /
 //     apply_support / project_intensity on a caller's field run in FP64 and
 //     are not available on FP32 reconstructions;
-//   - set_complex_constraint (TransmissionConstraint) is not provided.
+//   - a TransmissionConstraint given to set_complex_constraint runs in the
+//     FP64 form only, and is read when iterate() or apply_support() next runs
+//     (changes to it after that are picked up at the following call).
 #ifndef NADIA_DROPIN_BASECDI_H
 #define NADIA_DROPIN_BASECDI_H
 
@@ -23,6 +25,7 @@
 
 #include "Complex_2D.h"
 #include "Double_2D.h"
+#include "TransmissionConstraint.h"
 #include "types.h"
 
 #define NALGORITHMS 9
@@ -43,9 +46,17 @@ public:
         }
     }
 
+    // BaseCDI::set_complex_constraint (BaseCDI.h:471-473)
+    virtual void set_complex_constraint(TransmissionConstraint &trans_constraint)
+    {
+        transmission_constraint = &trans_constraint;
+        trans_constraint.push_to(h, nx, ny, true);
+    }
+
     // BaseCDI::iterate (BaseCDI.c++:297-387): one iteration on the GPU
     virtual int iterate()
     {
+        if (transmission_constraint) transmission_constraint->push_to(h, nx, ny);
         complex.push();
         nadia_cxx::check(nadia_iterate(h, 1));
         complex.device_newer = true;
@@ -55,6 +66,7 @@ public:
     // several iterations without returning to the host in between
     int iterate(int n)
     {
+        if (transmission_constraint) transmission_constraint->push_to(h, nx, ny);
         complex.push();
         nadia_cxx::check(nadia_iterate(h, n));
         complex.device_newer = true;
@@ -254,6 +266,7 @@ protected:
     Complex_2D &complex;
     int nx, ny;
     int n_best;
+    TransmissionConstraint *transmission_constraint = nullptr;
     nadia_solver *h = nullptr;
     Double_2D support;
     std::vector<std::unique_ptr<Complex_2D>> best;

@@ -133,6 +133,34 @@ int nadia_poly_set_spectrum_file(nadia_solver *s, const char *path);
 /* The padding PolyCDI derived from its spectrum (PolyCDI.c++:86-87). */
 int nadia_poly_get_padding(const nadia_solver *s, int *px, int *py);
 
+/* ---- transmission constraint ------------------------------------------------ */
+
+/* BaseCDI::set_complex_constraint (NADIA/include/BaseCDI.h:471-473) with a
+ * TransmissionConstraint (NADIA/include/TransmissionConstraint.h:200-375):
+ * applied after every support projection (BaseCDI::apply_support,
+ * BaseCDI.c++:130-134) -- to the estimate, or for FresnelCDI to its
+ * transmission function (FresnelCDI.c++:203-215, and in get_transmission).
+ * enforce_unity: magnitudes above 1 set to 1; charge_flip with flip_sign
+ * (+1 or -1): imaginary parts with flip_sign*imag > 0 negated; nregions (at
+ * most 16) ComplexConstraint regions, given as nregions masks of nx*ny
+ * (a pixel belongs to the first region whose mask is > 0 there), alpha as
+ * nregions pairs (alpha1, alpha2), fixed_c as nregions values (NaN = c_mean
+ * measured each time; NULL = all measured).  FP64 form only. */
+int nadia_set_transmission_constraint(nadia_solver *s, int enforce_unity, int charge_flip,
+                                      int flip_sign, int nregions, const double *regions,
+                                      const double *alpha, const double *fixed_c);
+
+/* TransmissionConstraint::set_custom_constraint (TransmissionConstraint.h:
+ * 357-359): fn is called on the host with the constrained transmission
+ * (interleaved complex, x*ny+y) after the built-in steps and may change it;
+ * NULL removes it.  Needs a constraint set first. */
+int nadia_set_transmission_custom(nadia_solver *s,
+                                  void (*fn)(double *transmission, int nx, int ny, void *user),
+                                  void *user);
+
+/* Removes the transmission constraint (BaseCDI without one). */
+int nadia_clear_transmission_constraint(nadia_solver *s);
+
 /* ---- algorithm ---------------------------------------------------------- */
 
 /* BaseCDI::set_algorithm -- BaseCDI.c++:192-237.  Returns early when the

@@ -129,6 +129,28 @@ int nadia_fresnel_wf_set_support(nadia_solver *h, double z_diameter, double size
     return guard([&] { S(h).fresnel_wf_set_support(z_diameter, size); });
 }
 
+int nadia_set_transmission_constraint(nadia_solver *h, int enforce_unity, int charge_flip,
+                                      int flip_sign, int nregions, const double *regions,
+                                      const double *alpha, const double *fixed_c)
+{
+    return guard([&] {
+        S(h).set_transmission_constraint(enforce_unity, charge_flip, flip_sign, nregions, regions,
+                                         alpha, fixed_c);
+    });
+}
+
+int nadia_set_transmission_custom(nadia_solver *h,
+                                  void (*fn)(double *transmission, int nx, int ny, void *user),
+                                  void *user)
+{
+    return guard([&] { S(h).set_transmission_custom(fn, user); });
+}
+
+int nadia_clear_transmission_constraint(nadia_solver *h)
+{
+    return guard([&] { S(h).clear_transmission_constraint(); });
+}
+
 int nadia_poly_create(int nx, int ny, int precision, double beta, int n_best,
                       nadia_solver **out)
 {

@@ -714,9 +714,87 @@ void fresnel_get_transmission(const double2 *esw, const double2 *ill, double2 *o
     k_fresnel_get_t<<<grid_of(n), kThreads, 0, s>>>(esw, ill, out, n);
 }
 
+// TransmissionConstraint::apply_constraint, TransmissionConstraint.c++:76-172
+__global__ void k_tc_sums(const double2 *__restrict__ t, const int *__restrict__ region, size_t n,
+                          int R, double *partials)
+{
+    double lnA[kMaxRegions], ph[kMaxRegions];
+    for (int r = 0; r < R; ++r) lnA[r] = ph[r] = 0;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const int r = region[k];
+        if (r > 0) {
+            const double2 v = t[k];
+            ph[r - 1] += fabs(atan2(v.y, v.x));
+            lnA[r - 1] += fabs(log(mag_of(v)));
+        }
+    }
+    for (int r = 0; r < R; ++r) {
+        double a = lnA[r], b = ph[r];
+        block_sum2(a, b);
+        if (threadIdx.x == 0) {
+            partials[2 * ((size_t)blockIdx.x * R + r)] = a;
+            partials[2 * ((size_t)blockIdx.x * R + r) + 1] = b;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_tc_cmean(const double *partials, int nblocks, int R, const double *params,
+                           double *cmean)
+{
+    const int r = threadIdx.x;
+    if (r >= R) return;
+    double a = 0, b = 0;
+    for (int blk = 0; blk < nblocks; ++blk) {
+        a += partials[2 * ((size_t)blk * R + r)];
+        b += partials[2 * ((size_t)blk * R + r) + 1];
+    }
+    cmean[r] = params[4 * r + 2] != 0 ? params[4 * r + 3] : a / b;
+}
+
+__global__ void k_tc_apply(double2 *t, const int *__restrict__ region, size_t n, int R,
+                           const double *__restrict__ params, const double *__restrict__ cmean,
+                           int flip, int flip_sign, int unity)
+{
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        double2 v = t[k];
+        const double phase_old = atan2(v.y, v.x);
+        double mag_old = mag_of(v);
+        const int r = R > 0 ? region[k] : 0;
+        if (r > 0) {
+            const double a1 = params[4 * (r - 1)], a2 = params[4 * (r - 1) + 1];
+            const double cm = cmean[r - 1];
+            const double mag_new = exp((1 - a1) * log(mag_old) + a1 * cm * phase_old);
+            const double phase_new = (1 - a2) * phase_old + a2 * log(mag_old) / cm;
+            v = set_mag(v, mag_new);
+            const double m = mag_of(v); // Complex_2D::set_phase keeps the current magnitude
+            v = make_double2(m * cos(phase_new), m * sin(phase_new));
+            mag_old = mag_new;
+        }
+        if (flip && flip_sign * v.y > 0) v.y = -1 * v.y;
+        if (unity && mag_old > 1) v = set_mag(v, 1);
+        t[k] = v;
+    }
+}
+
 void autocorr_fill(const double *isqrt, double2 *t, size_t n, cudaStream_t s)
 {
     k_autocorr_fill<<<grid_of(n), kThreads, 0, s>>>(isqrt, t, n);
+}
+
+void transmission_constraint(double2 *t, const int *region, size_t n, int nregions,
+                             const double *params, double *partials, double *cmean,
+                             int charge_flip, int flip_sign, int enforce_unity, cudaStream_t s)
+{
+    if (nregions > 0) {
+        k_tc_sums<<<kRedBlocks, kThreads, 0, s>>>(t, region, n, nregions, partials);
+        k_tc_cmean<<<1, 32, 0, s>>>(partials, kRedBlocks, nregions, params, cmean);
+    }
+    if (nregions > 0 || charge_flip || enforce_unity)
+        k_tc_apply<<<grid_of(n), kThreads, 0, s>>>(t, region, n, nregions, params, cmean,
+                                                    charge_flip, flip_sign, enforce_unity);
 }
 
 } // namespace plain

@@ -98,5 +98,14 @@ void fresnel_get_transmission(const double2 *esw, const double2 *ill, double2 *o
 // PlanarCDI::get_intensity_autocorrelation, first loop (PlanarCDI.c++:18-25).
 void autocorr_fill(const double *isqrt, double2 *t, size_t n, cudaStream_t s);
 
+// TransmissionConstraint::apply_constraint (TransmissionConstraint.c++:76-172)
+// on the device.  region[k] is 0 or the 1-based region of pixel k; params
+// holds (alpha1, alpha2, c fixed?, fixed c) per region.  Region sums are
+// reduced in a fixed order (kRedBlocks blocks, then one thread per region).
+constexpr int kMaxRegions = 16;
+void transmission_constraint(double2 *t, const int *region, size_t n, int nregions,
+                             const double *params, double *partials, double *cmean,
+                             int charge_flip, int flip_sign, int enforce_unity, cudaStream_t s);
+
 } // namespace plain
 } // namespace nadia

@@ -333,6 +333,96 @@ void Solver::fresnel_set_experimental_parameters(double wl, double zfd_, double 
     }
 }
 
+// BaseCDI::apply_support (BaseCDI.c++:130-134) and FresnelCDI::apply_support
+// (FresnelCDI.c++:203-215): the support, then the transmission constraint --
+// on the estimate itself, or for FresnelCDI on its transmission function
+// (get_transmission_function applies the constraint, set_transmission_function
+// writes the estimate back)
+void Solver::plain_apply_support(double2 *c)
+{
+    AllocScope scope(st);
+    plain::support_constraint(c, support.p, n, st);
+    if (!tc.active) return;
+    if (kind == NADIA_FRESNEL) {
+        plain::fresnel_get_transmission(c, illum_sample.p, tc.tbuf.p, n, st);
+        apply_transmission_constraint(tc.tbuf.p);
+        plain::fresnel_set_transmission(tc.tbuf.p, illum_sample.p, c, nx, ny, st);
+    } else {
+        apply_transmission_constraint(c);
+    }
+}
+
+// TransmissionConstraint::apply_constraint (TransmissionConstraint.c++:76-172),
+// ending with the caller's custom function, run on the host copy
+void Solver::apply_transmission_constraint(double2 *t)
+{
+    plain::transmission_constraint(t, tc.region.p, n, tc.nregions, tc.params.p, tc.partials.p,
+                                   tc.cmean.p, tc.flip, tc.flip_sign, tc.unity, st);
+    if (tc.custom) {
+        std::vector<double> h(2 * n);
+        d2h(h.data(), t, n * sizeof(double2), st);
+        tc.custom(h.data(), nx, ny, tc.user);
+        h2d(t, h.data(), n * sizeof(double2), st);
+    }
+}
+
+// BaseCDI::set_complex_constraint (BaseCDI.h:471-473) with a
+// TransmissionConstraint built as TransmissionConstraint.c++:20-73 builds it:
+// regions in order, the earlier region keeping a shared pixel; fixed_c NaN
+// leaves a region's c_mean free (ComplexConstraint::set_fixed_c otherwise)
+void Solver::set_transmission_constraint(int unity, int flip, int flip_sign, int nregions,
+                                         const double *regions, const double *alpha,
+                                         const double *fixed_c)
+{
+    AllocScope scope(st);
+    NADIA_REQUIRE(prec == NADIA_FP64, NADIA_ERR_UNSUPPORTED,
+                  "transmission constraints run in the FP64 form");
+    NADIA_REQUIRE(nregions >= 0 && nregions <= plain::kMaxRegions, NADIA_ERR_INVALID,
+                  "between 0 and 16 complex-constraint regions");
+    NADIA_REQUIRE(nregions == 0 || (regions && alpha), NADIA_ERR_INVALID,
+                  "complex-constraint regions need their masks and alphas");
+    NADIA_CUDA(cudaStreamSynchronize(st)); // buffers of an earlier constraint may be replaced
+    tc.active = true;
+    tc.unity = unity ? 1 : 0;
+    tc.flip = flip ? 1 : 0;
+    tc.flip_sign = flip_sign > 0 ? 1 : -1;
+    tc.nregions = nregions;
+    std::vector<int> map(n, 0);
+    std::vector<double> prm(4 * (size_t)std::max(nregions, 1), 0.0);
+    for (int r = 0; r < nregions; ++r) {
+        for (size_t k = 0; k < n; ++k)
+            if (regions[(size_t)r * n + k] > 0 && map[k] == 0) map[k] = r + 1;
+        prm[4 * r] = alpha[2 * r];
+        prm[4 * r + 1] = alpha[2 * r + 1];
+        const bool fixed = fixed_c && fixed_c[r] == fixed_c[r];
+        prm[4 * r + 2] = fixed ? 1.0 : 0.0;
+        prm[4 * r + 3] = fixed ? fixed_c[r] : 0.0;
+    }
+    tc.region.alloc(n);
+    tc.params.alloc(prm.size());
+    tc.partials.alloc(2 * (size_t)plain::kRedBlocks * std::max(nregions, 1));
+    tc.cmean.alloc(std::max(nregions, 1));
+    if (kind == NADIA_FRESNEL && !tc.tbuf) tc.tbuf.alloc(n);
+    h2d(tc.region.p, map.data(), n * sizeof(int), st);
+    h2d(tc.params.p, prm.data(), prm.size() * sizeof(double), st);
+}
+
+void Solver::set_transmission_custom(void (*fn)(double *, int, int, void *), void *user)
+{
+    NADIA_REQUIRE(tc.active, NADIA_ERR_STATE, "set a transmission constraint first");
+    tc.custom = fn;
+    tc.user = user;
+}
+
+void Solver::clear_transmission_constraint()
+{
+    NADIA_CUDA(cudaStreamSynchronize(st));
+    tc.active = false;
+    tc.custom = nullptr;
+    tc.user = nullptr;
+    tc.nregions = 0;
+}
+
 // FresnelCDI_WF::FresnelCDI_WF, FresnelCDI_WF.c++:31-79: the quarter table
 // of the zone-plate-to-detector factor, (sin phi, -cos phi) / sqrt(nx*ny),
 // computed on the host in the reference's operation order (pow(x, 2) included)
@@ -480,7 +570,7 @@ void Solver::initialise_estimate(int seed)
             DevBuf<double2> t(n);
             h2d(t.p, h.data(), t.bytes(), st);
             plain::fresnel_set_transmission(t.p, illum_sample.p, x.p, nx, ny, st);
-            plain::support_constraint(x.p, support.p, n, st);
+            plain_apply_support(x.p); // FresnelCDI.c++:199 (apply_support)
             sync();
         } else {
             f32->fresnel_initialise(h.data());
@@ -587,6 +677,7 @@ void Solver::get_transmission(double *h)
     if (prec == NADIA_FP64) {
         DevBuf<double2> t(n);
         plain::fresnel_get_transmission(x.p, illum_sample.p, t.p, n, st);
+        if (tc.active) apply_transmission_constraint(t.p); // FresnelCDI.c++:352-353
         d2h(h, t.p, t.bytes(), st);
     } else {
         f32->fresnel_get_transmission(h);
@@ -707,20 +798,20 @@ void Solver::plain_iterate_once()
     if (kind == NADIA_FRESNEL_WF) {
         // FresnelCDI_WF::iterate, FresnelCDI_WF.c++:155-162: a fixed algorithm
         plain_propagate_from(x.p, false);
-        plain::support_constraint(x.p, support.p, n, st);
+        plain_apply_support(x.p);
         plain_propagate_to(x.p, false);
         plain_scale(x.p);
         return;
     }
     if (algorithm == NADIA_ER) {
         plain_project(x.p);
-        plain::support_constraint(x.p, support.p, n, st);
+        plain_apply_support(x.p);
         return;
     }
     ensure_temps();
     if (w[PFS] != 0) {
         NADIA_CUDA(cudaMemcpyAsync(tPFS.p, x.p, nb, cudaMemcpyDeviceToDevice, st));
-        plain::support_constraint(tPFS.p, support.p, n, st);
+        plain_apply_support(tPFS.p);
         plain_project(tPFS.p);
     }
     if (w[PF] != 0) {
@@ -729,16 +820,16 @@ void Solver::plain_iterate_once()
     }
     if (w[PS] != 0) {
         NADIA_CUDA(cudaMemcpyAsync(tPS.p, x.p, nb, cudaMemcpyDeviceToDevice, st));
-        plain::support_constraint(tPS.p, support.p, n, st);
+        plain_apply_support(tPS.p);
     }
     if (w[PSF] != 0) {
         if (w[PF] != 0) {
             NADIA_CUDA(cudaMemcpyAsync(tPSF.p, tPF.p, nb, cudaMemcpyDeviceToDevice, st));
-            plain::support_constraint(tPSF.p, support.p, n, st);
+            plain_apply_support(tPSF.p);
         } else {
             NADIA_CUDA(cudaMemcpyAsync(tPSF.p, x.p, nb, cudaMemcpyDeviceToDevice, st));
             plain_project(tPSF.p);
-            plain::support_constraint(tPSF.p, support.p, n, st);
+            plain_apply_support(tPSF.p);
         }
     }
     plain::combine(x.p, w[PFS] != 0 ? tPFS.p : nullptr, w[PF] != 0 ? tPF.p : nullptr,
@@ -890,7 +981,7 @@ void Solver::single_op(int op, double *field)
     case 0: plain_propagate_to(c.p, false); break;
     case 1: plain_propagate_from(c.p, false); break;
     case 2: plain_scale(c.p); break;
-    case 3: plain::support_constraint(c.p, support.p, n, st); break;
+    case 3: plain_apply_support(c.p); break;
     case 4: plain_project(c.p); break;
     default: throw Error(NADIA_ERR_INVALID, "unknown operator");
     }

@@ -72,6 +72,19 @@ struct Solver {
     DevBuf<double2> padded;
     plain::Fft2d fft_pad;
 
+    // TransmissionConstraint set by BaseCDI::set_complex_constraint (FP64 form)
+    struct TransConstraint {
+        bool active = false;
+        int unity = 0, flip = 0, flip_sign = 1, nregions = 0;
+        DevBuf<int> region;       // n: 0 or the 1-based region of each pixel
+        DevBuf<double> params;    // per region: alpha1, alpha2, c fixed?, fixed c
+        DevBuf<double> partials;  // region sums per reduction block
+        DevBuf<double> cmean;     // per region
+        DevBuf<double2> tbuf;     // FresnelCDI: the transmission function being constrained
+        void (*custom)(double *, int, int, void *) = nullptr;
+        void *user = nullptr;
+    } tc;
+
     std::unique_ptr<Fused32> f32;
 
     Solver(int kind, int nx, int ny, int prec, int n_best);
@@ -89,6 +102,11 @@ struct Solver {
     void fresnel_auto_set_norm();
     void fresnel_wf_init(double wl, double zone_focal, double focal_detector, double pixel);
     void fresnel_wf_set_support(double z_diameter, double size);
+    void set_transmission_constraint(int unity, int flip, int flip_sign, int nregions,
+                                     const double *regions, const double *alpha,
+                                     const double *fixed_c);
+    void set_transmission_custom(void (*fn)(double *, int, int, void *), void *user);
+    void clear_transmission_constraint();
 
     // algorithm
     void set_algorithm(int alg);
@@ -124,6 +142,8 @@ struct Solver {
     void plain_propagate_from(double2 *c, bool padded_grid);
     void plain_scale(double2 *c);
     void plain_convolve(double *arr, double gauss_width, int cut);
+    void plain_apply_support(double2 *c);
+    void apply_transmission_constraint(double2 *t);
     void ensure_temps();
     void update_n_best();
     void record_error();

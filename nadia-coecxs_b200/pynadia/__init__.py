@@ -70,6 +70,9 @@ _PROTOS = {
     "nadia_fresnel_wf_create": (_I, [_I, _I, _I, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_double, ctypes.c_double, _I, ctypes.POINTER(_H)]),
     "nadia_fresnel_wf_set_support": (_I, [_H, ctypes.c_double, ctypes.c_double]),
+    "nadia_set_transmission_constraint": (_I, [_H, _I, _I, _I, _I, _D, _D, _D]),
+    "nadia_set_transmission_custom": (_I, [_H, ctypes.c_void_p, ctypes.c_void_p]),
+    "nadia_clear_transmission_constraint": (_I, [_H]),
     "nadia_destroy": (_I, [_H]),
     "nadia_get_size": (_I, [_H, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "nadia_set_support": (_I, [_H, _D, _I]),
@@ -223,6 +226,41 @@ class Solver:
 
     def set_intensity(self, i):
         _check(self.lib.nadia_set_intensity(self.h, _ptr(self._real(i))))
+
+    def set_transmission_constraint(self, enforce_unity=True, charge_flip=True, flip_sign=1,
+                                    regions=(), alphas=(), fixed_c=None):
+        """BaseCDI::set_complex_constraint with a TransmissionConstraint
+        (nadia_set_transmission_constraint)."""
+        nr = len(regions)
+        reg = np.ascontiguousarray(np.array(regions, dtype=np.float64).reshape(nr, self.nx, self.ny)
+                                   if nr else np.zeros(1))
+        al = np.ascontiguousarray(np.array(alphas, dtype=np.float64).reshape(-1)
+                                  if nr else np.zeros(2))
+        fc = None if fixed_c is None else np.ascontiguousarray(fixed_c, dtype=np.float64)
+        _check(self.lib.nadia_set_transmission_constraint(
+            self.h, int(enforce_unity), int(charge_flip), int(flip_sign), nr, _ptr(reg), _ptr(al),
+            _ptr(fc) if fc is not None else None))
+
+    def set_transmission_custom(self, fn):
+        """A Python function f(transmission) changing the (nx, ny) complex128
+        array in place, called after the built-in constraint steps."""
+        if fn is None:
+            self._custom = None
+            _check(self.lib.nadia_set_transmission_custom(self.h, None, None))
+            return
+        proto = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                 ctypes.c_int, ctypes.c_void_p)
+
+        def tramp(p, nx, ny, user):
+            a = np.ctypeslib.as_array(p, shape=(nx * ny * 2,)).view(np.complex128)
+            fn(a.reshape(nx, ny))
+
+        self._custom = proto(tramp)   # kept alive with the handle
+        _check(self.lib.nadia_set_transmission_custom(
+            self.h, ctypes.cast(self._custom, ctypes.c_void_p), None))
+
+    def clear_transmission_constraint(self):
+        _check(self.lib.nadia_clear_transmission_constraint(self.h))
 
     def set_wf_support(self, z_diameter, size=1.01):
         """FresnelCDI_WF::set_support(z_diameter, size)."""

@@ -31,6 +31,19 @@ enum { PSF, PFS, PS, PF, PI_ }; /* NADIA/include/BaseCDI.h:32 (term order) */
 enum { ER, BIO, BOO, HIO, DM, SF, ASR, HPR, RAAR, CUSTOM }; /* BaseCDI.h:37 */
 enum { KIND_PLANAR = 0, KIND_FRESNEL = 1, KIND_POLY = 2, KIND_FRESNEL_WF = 3 };
 
+/* TransmissionConstraint (NADIA/include/TransmissionConstraint.h:200-375,
+ * NADIA/src/TransmissionConstraint.c++) with its ComplexConstraint regions */
+typedef struct orc_tc {
+    int active;
+    int enforce_unity, charge_flip, flip_sign;
+    int nregions;
+    double *region_map;    /* nx*ny: 0, or the 1-based region that claimed the pixel */
+    double *alpha1, *alpha2, *c_mean;
+    int *fixed_c;
+    void (*custom)(double *t, int nx, int ny, void *user);
+    void *user;
+} orc_tc;
+
 typedef struct orc_solver {
     int kind, nx, ny;
     double beta;
@@ -60,6 +73,7 @@ typedef struct orc_solver {
     double *isqrt_calc;    /* nx*ny */
     canon_ctxd *fft_pad;   /* padded transform */
     int pnx, pny;
+    orc_tc tc;
 } orc_solver;
 
 static double *zd(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
@@ -395,7 +409,125 @@ static void project(orc_solver *s, double *c)
 
 /* apply_support: BaseCDI.c++:130-134 and FresnelCDI.c++:203-215 (no complex
  * constraint attached) */
-static void apply_support(orc_solver *s, double *c) { support_constraint(s, c); }
+/* TransmissionConstraint::apply_constraint, TransmissionConstraint.c++:76-172:
+ * per-region c_mean = sum|ln|T|| / sum|arg T| (unless fixed), then per pixel
+ * the region update (ComplexConstraint::get_new_mag / get_new_phase,
+ * TransmissionConstraint.h:100-118) applied with set_mag then set_phase,
+ * charge flipping, unit magnitude, and the caller's custom function */
+static void apply_constraint(orc_solver *s, double *t)
+{
+    orc_tc *tc = &s->tc;
+    int nx = s->nx, ny = s->ny;
+    int regions = tc->nregions;
+    if (regions > 0) {
+        double *mean_lnA = zd((size_t)regions), *mean_phase = zd((size_t)regions);
+        for (int i = 0; i < nx; i++)
+            for (int j = 0; j < ny; j++) {
+                double rm = tc->region_map[(size_t)i * ny + j];
+                if (rm > 0) {
+                    int r = (int)rm - 1;
+                    double *p = t + 2 * ((size_t)i * ny + j);
+                    mean_phase[r] += fabs(atan2(p[1], p[0]));
+                    mean_lnA[r] += fabs(log(mag_of(p)));
+                }
+            }
+        for (int r = 0; r < regions; r++)
+            if (!tc->fixed_c[r]) tc->c_mean[r] = mean_lnA[r] / mean_phase[r];
+        free(mean_lnA);
+        free(mean_phase);
+    }
+    if (regions > 0 || tc->charge_flip || tc->enforce_unity) {
+        for (int i = 0; i < nx; i++)
+            for (int j = 0; j < ny; j++) {
+                double *p = t + 2 * ((size_t)i * ny + j);
+                double phase_old = atan2(p[1], p[0]);
+                double mag_old = mag_of(p);
+                double rm = regions > 0 ? tc->region_map[(size_t)i * ny + j] : 0;
+                if (regions > 0 && rm > 0) {
+                    int r = (int)rm - 1;
+                    double a1 = tc->alpha1[r], a2 = tc->alpha2[r], cm = tc->c_mean[r];
+                    double mag_new = exp((1 - a1) * log(mag_old) + a1 * cm * phase_old);
+                    double phase_new = (1 - a2) * phase_old + a2 * log(mag_old) / cm;
+                    set_mag(p, mag_new);
+                    double m = mag_of(p);             /* Complex_2D::set_phase */
+                    p[0] = m * cos(phase_new);
+                    p[1] = m * sin(phase_new);
+                    mag_old = mag_new;
+                }
+                if (tc->charge_flip && tc->flip_sign * p[1] > 0) p[1] = -1 * p[1];
+                if (tc->enforce_unity && mag_old > 1) set_mag(p, 1);
+            }
+    }
+    if (tc->custom) tc->custom(t, nx, ny, tc->user);
+}
+
+static void fresnel_set_transmission(orc_solver *s, const double *t, double *esw);
+static void fresnel_get_transmission(orc_solver *s, const double *esw, double *res);
+
+/* BaseCDI::apply_support, BaseCDI.c++:130-134; FresnelCDI::apply_support,
+ * FresnelCDI.c++:203-215 (the constraint acts on the transmission function) */
+static void apply_support(orc_solver *s, double *c)
+{
+    support_constraint(s, c);
+    if (!s->tc.active) return;
+    if (s->kind == KIND_FRESNEL) {
+        double *t = zd(2 * (size_t)s->nx * s->ny);
+        fresnel_get_transmission(s, c, t);
+        fresnel_set_transmission(s, t, c);
+        free(t);
+    } else {
+        apply_constraint(s, c);
+    }
+}
+
+/* BaseCDI::set_complex_constraint (BaseCDI.h:471-473) with a
+ * TransmissionConstraint built as TransmissionConstraint.c++:20-73 does:
+ * regions added in order, a pixel claimed by an earlier region stays with it;
+ * fixed_c[r] is NaN for a free c_mean (ComplexConstraint::set_fixed_c). */
+void orc_set_transmission_constraint(orc_solver *s, int enforce_unity, int charge_flip,
+                                     int flip_sign, int nregions, const double *regions,
+                                     const double *alpha, const double *fixed_c)
+{
+    orc_tc *tc = &s->tc;
+    size_t n = (size_t)s->nx * s->ny;
+    free(tc->region_map); free(tc->alpha1); free(tc->alpha2); free(tc->c_mean); free(tc->fixed_c);
+    memset(tc, 0, sizeof(*tc));
+    tc->active = 1;
+    tc->enforce_unity = enforce_unity;
+    tc->charge_flip = charge_flip;
+    tc->flip_sign = flip_sign > 0 ? 1 : -1;
+    tc->nregions = nregions;
+    if (nregions > 0) {
+        tc->region_map = zd(n);
+        tc->alpha1 = zd((size_t)nregions);
+        tc->alpha2 = zd((size_t)nregions);
+        tc->c_mean = zd((size_t)nregions);
+        tc->fixed_c = (int *)calloc((size_t)nregions, sizeof(int));
+        for (int r = 0; r < nregions; ++r) {
+            for (size_t k = 0; k < n; ++k)
+                if (regions[r * n + k] > 0 && !(tc->region_map[k] > 0)) tc->region_map[k] = r + 1;
+            tc->alpha1[r] = alpha[2 * r];
+            tc->alpha2[r] = alpha[2 * r + 1];
+            if (fixed_c && fixed_c[r] == fixed_c[r]) {
+                tc->fixed_c[r] = 1;
+                tc->c_mean[r] = fixed_c[r];
+            }
+        }
+    }
+}
+
+void orc_set_transmission_custom(orc_solver *s, void (*f)(double *, int, int, void *), void *user)
+{
+    s->tc.custom = f;
+    s->tc.user = user;
+}
+
+void orc_clear_transmission_constraint(orc_solver *s)
+{
+    orc_tc *tc = &s->tc;
+    free(tc->region_map); free(tc->alpha1); free(tc->alpha2); free(tc->c_mean); free(tc->fixed_c);
+    memset(tc, 0, sizeof(*tc));
+}
 
 /* set_custom_algorithm, BaseCDI.c++:240-255 */
 static void set_custom(orc_solver *s, const double *m)
@@ -697,6 +829,7 @@ static void fresnel_get_transmission(orc_solver *s, const double *esw, double *r
             res[2 * k + 1] = 0.0;
         }
     }
+    if (s->tc.active) apply_constraint(s, res); /* FresnelCDI.c++:352-353 */
 }
 
 /* PolyCDI::PolyCDI, PolyCDI.c++:25-35 (its own `beta` member never reaches
@@ -792,6 +925,7 @@ void orc_destroy(orc_solver *s)
     canon_ctx_destroyd(s->fft); canon_ctx_destroyd(s->fft_pad);
     free(s->illum); free(s->illum_sample); free(s->coef);
     free(s->spectrum); free(s->isqrt_calc);
+    orc_clear_transmission_constraint(s);
     free(s);
 }
 

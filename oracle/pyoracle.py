@@ -45,6 +45,8 @@ _PROTOS = {
     "fresnel_wf_create": (_V, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                ctypes.c_double, ctypes.c_double, ctypes.c_int]),
     "fresnel_wf_set_support": (None, [_V, ctypes.c_double, ctypes.c_double]),
+    "set_transmission_constraint": (None, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, _D, _D, _D]),
     "destroy": (None, [_V]),
     "set_support": (None, [_V, _D, ctypes.c_int]),
     "set_intensity": (None, [_V, _D]),
@@ -240,6 +242,36 @@ class _Solver:
     def set_wf_support(self, z_diameter, size=1.01):
         """FresnelCDI_WF::set_support(z_diameter, size)."""
         self.L.fresnel_wf_set_support(self.h, z_diameter, size)
+
+    def set_transmission_constraint(self, enforce_unity=True, charge_flip=True, flip_sign=1,
+                                    regions=(), alphas=(), fixed_c=None):
+        """BaseCDI::set_complex_constraint with a TransmissionConstraint: the
+        unit-magnitude and charge-flipping switches and ComplexConstraint
+        regions (masks, (alpha1, alpha2) each, optional fixed c; NaN = free)."""
+        nr = len(regions)
+        reg = np.ascontiguousarray(np.array(regions, dtype=np.float64).reshape(nr, self.nx, self.ny)
+                                   if nr else np.zeros(1))
+        al = np.ascontiguousarray(np.array(alphas, dtype=np.float64).reshape(-1)
+                                  if nr else np.zeros(2))
+        fc = None if fixed_c is None else np.ascontiguousarray(fixed_c, dtype=np.float64)
+        self.L.set_transmission_constraint(self.h, int(enforce_unity), int(charge_flip),
+                                           int(flip_sign), nr, _ptr(reg), _ptr(al),
+                                           _ptr(fc) if fc is not None else None)
+
+    def set_transmission_custom(self, fn):
+        """Oracle only: a Python function changing the transmission in place."""
+        proto = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                 ctypes.c_int, ctypes.c_void_p)
+
+        def tramp(p, nx, ny, user):
+            a = np.ctypeslib.as_array(p, shape=(nx * ny * 2,)).view(np.complex128)
+            fn(a.reshape(nx, ny))
+
+        self._custom = proto(tramp)
+        f = self.L.lib.orc_set_transmission_custom
+        f.argtypes = [_V, ctypes.c_void_p, ctypes.c_void_p]
+        f.restype = None
+        f(self.h, ctypes.cast(self._custom, ctypes.c_void_p), None)
 
     def auto_set_norm(self):
         self.L.fresnel_auto_set_norm(self.h)

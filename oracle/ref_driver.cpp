@@ -18,6 +18,8 @@
 #include <FresnelCDI.h>
 #include <FresnelCDI_WF.h>
 #include <PolyCDI.h>
+#include <TransmissionConstraint.h>
+#include <vector>
 
 namespace {
 
@@ -28,6 +30,10 @@ struct RefSolver {
     Complex_2D *esw;
     Complex_2D *wf;
     BaseCDI *cdi;
+    // a transmission constraint and its regions (they must outlive the solver's use)
+    TransmissionConstraint *tc = nullptr;
+    std::vector<Double_2D *> regions;
+    std::vector<ComplexConstraint *> constraints;
 };
 
 void to_real(Double_2D &d, const double *a, int nx, int ny)
@@ -70,6 +76,27 @@ void *ref_planar_create(int nx, int ny, int n_best)
     s->wf = 0;
     s->cdi = new PlanarCDI(*s->esw, n_best);
     return s;
+}
+
+void ref_set_transmission_constraint(void *h, int enforce_unity, int charge_flip, int flip_sign,
+                                     int nregions, const double *regions, const double *alpha,
+                                     const double *fixed_c)
+{
+    RefSolver *s = S(h);
+    size_t n = (size_t)s->nx * s->ny;
+    s->tc = new TransmissionConstraint();
+    s->tc->set_enforce_unity(enforce_unity != 0);
+    s->tc->set_charge_flipping(charge_flip != 0, flip_sign);
+    for (int r = 0; r < nregions; ++r) {
+        Double_2D *d = new Double_2D(s->nx, s->ny);
+        to_real(*d, regions + r * n, s->nx, s->ny);
+        ComplexConstraint *c = new ComplexConstraint(*d, alpha[2 * r], alpha[2 * r + 1]);
+        if (fixed_c && fixed_c[r] == fixed_c[r]) c->set_fixed_c(fixed_c[r]);
+        s->regions.push_back(d);
+        s->constraints.push_back(c);
+        s->tc->add_complex_constraint(*c);
+    }
+    s->cdi->set_complex_constraint(*s->tc);
 }
 
 void *ref_fresnel_wf_create(int nx, int ny, double wavelength, double zone_focal_length,
@@ -117,6 +144,9 @@ void ref_destroy(void *h)
     delete s->cdi;
     delete s->esw;
     delete s->wf;
+    delete s->tc;
+    for (ComplexConstraint *c : s->constraints) delete c;
+    for (Double_2D *d : s->regions) delete d;
     delete s;
 }
 

@@ -191,6 +191,37 @@ static int poly(int nx, int ny, int padding)
     return 0;
 }
 
+// PlanarCDI with a TransmissionConstraint: tests/scenarios.py's
+// planar_constrained with ER only
+static int constrained(int nx, int ny)
+{
+    Complex_2D object_estimate(nx, ny);
+    PlanarCDI planar(object_estimate);
+    planar.set_support(real_2d("support.bin", nx, ny));
+    planar.set_intensity(real_2d("intensity.bin", nx, ny));
+    std::vector<double> p = load("tc_params.bin", 9); // (alpha1, alpha2, fixed c or NaN) x 3
+    Double_2D r0 = real_2d("region0.bin", nx, ny), r1 = real_2d("region1.bin", nx, ny),
+              r2 = real_2d("region2.bin", nx, ny);
+    ComplexConstraint c0(r0, p[0], p[1]), c1(r1, p[3], p[4]), c2(r2, p[6], p[7]);
+    if (p[5] == p[5]) c1.set_fixed_c(p[5]);
+    TransmissionConstraint tc;
+    tc.set_enforce_unity(true);
+    tc.set_charge_flipping(true, -1);
+    tc.add_complex_constraint(c0);
+    tc.add_complex_constraint(c1);
+    tc.add_complex_constraint(c2);
+    planar.set_complex_constraint(tc);
+    planar.initialise_estimate(3);
+    std::vector<double> errs;
+    for (int it = 0; it < 12; ++it) {
+        planar.iterate();
+        errs.push_back(planar.get_error());
+    }
+    save("errors.bin", errs);
+    save_complex("esw.bin", object_estimate);
+    return 0;
+}
+
 // FresnelCDI_WF: the sequence of tests/scenarios.py's fresnel_wf_mixed
 static int white_field(int nx, int ny)
 {
@@ -280,6 +311,7 @@ int main(int argc, char **argv)
         if (mode == "poly") return poly(nx, ny, argc > 5 ? std::atoi(argv[5]) : 0);
         if (mode == "example") return example(nx, ny);
         if (mode == "wf") return white_field(nx, ny);
+        if (mode == "tc") return constrained(nx, ny);
     } catch (const nadia_cxx::Failure &e) {
         std::cerr << "failure " << e.code << ": " << e.what() << std::endl;
         return 4;

@@ -186,3 +186,61 @@ def fresnel_wf_mixed(make, n=32, seed=6, iterations=12):
     out["to_detector"] = s.propagate_to_detector(field)
     out["from_detector"] = s.propagate_from_detector(field)
     return out
+
+
+def constraint_regions(n, ny=None):
+    """Three ComplexConstraint regions inside the central support: two
+    disjoint blocks and a third that overlaps the first (the earlier region
+    keeps the shared pixels)."""
+    ny = ny or n
+    c0, c1 = n // 2, ny // 2
+    q = max(2, n // 10)
+    a = np.zeros((n, ny))
+    b = np.zeros((n, ny))
+    c = np.zeros((n, ny))
+    a[c0 - q:c0, c1 - q:c1] = 1
+    b[c0:c0 + q, c1:c1 + q] = 1
+    c[c0 - q // 2:c0 + q // 2, c1 - q:c1] = 1
+    return [a, b, c], [(0.5, 0.4), (0.3, 0.6), (0.8, 0.1)], np.array([np.nan, 0.7, np.nan])
+
+
+def planar_constrained(make, n=32, seed=3, iterations=12, hio_from=3):
+    """PlanarCDI with a transmission constraint on the exit-surface wave:
+    unit magnitude, charge flipping (sign -1) and three complex-constraint
+    regions, through ER and (from iteration hio_from; None = never) HIO."""
+    c = planar_inputs(n, beam_stop=0)
+    s = make("planar", n, n)
+    s.set_support(c.support)
+    s.set_intensity(c.intensity)
+    regions, alphas, fixed = constraint_regions(n)
+    s.set_transmission_constraint(True, True, -1, regions, alphas, fixed)
+    s.initialise_estimate(seed)
+    errs = []
+    for it in range(iterations):
+        if it == hio_from:
+            s.set_algorithm(HIO)
+        s.iterate()
+        errs.append(s.get_error())
+    return {"errors": np.array(errs), "esw": s.get_exit_surface_wave()}
+
+
+def fresnel_constrained(make, n=32, seed=2, iterations=12, hio_from=4):
+    """FresnelCDI with a transmission constraint on the transmission function
+    (FresnelCDI::apply_support and get_transmission_function)."""
+    f = fresnel_inputs(n)
+    s = make("fresnel", n, n, white_field=f.white_field, wavelength=f.wavelength,
+             focal_detector_length=f.zfd, focal_sample_length=f.zfs, pixel_size=f.pixel,
+             normalisation=0.97)
+    s.set_support(f.support)
+    s.set_intensity(f.intensity)
+    regions, alphas, fixed = constraint_regions(n)
+    s.set_transmission_constraint(True, True, 1, regions[:2], alphas[:2], fixed[:2])
+    s.initialise_estimate(seed)
+    errs = []
+    for it in range(iterations):
+        if it == hio_from:
+            s.set_algorithm(HIO)
+        s.iterate()
+        errs.append(s.get_error())
+    return {"errors": np.array(errs), "esw": s.get_exit_surface_wave(),
+            "transmission": s.get_transmission()}

@@ -171,6 +171,25 @@ def test_fresnel_wf(programs, tmp_path, double):
                           out_round(double, ref["support"]))
 
 
+def test_transmission_constraint(programs, tmp_path):
+    """Double build: a PlanarCDI with a TransmissionConstraint (unit
+    magnitude, charge flipping, three complex-constraint regions) over ER
+    iterations, against the oracle to the 1e-10 bar (the constraint's maths
+    functions come from the device library)."""
+    n = 32
+    c = sc.planar_inputs(n, beam_stop=0)
+    regions, alphas, fixed = sc.constraint_regions(n)
+    put(tmp_path, "support.bin", c.support)
+    put(tmp_path, "intensity.bin", c.intensity)
+    for r in range(3):
+        put(tmp_path, "region%d.bin" % r, regions[r])
+    put(tmp_path, "tc_params.bin", [v for (a1, a2), fc in zip(alphas, fixed) for v in (a1, a2, fc)])
+    run(programs[True], "tc", n, n, tmp_path)
+    ref = sc.planar_constrained(oracle_factory(True), n=n, hio_from=None)
+    assert sc.rel_err(get(tmp_path, "errors.bin"), ref["errors"]) <= 1e-10
+    assert sc.rel_err(get(tmp_path, "esw.bin", (n, n), cplx=True), ref["esw"]) <= 1e-10
+
+
 def example_oracle(make, nx, ny, intensity, support):
     s = make("planar", nx, ny, n_best=4)
     s.set_support(support)

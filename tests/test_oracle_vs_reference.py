@@ -44,6 +44,16 @@ def test_fresnel():
 
 
 @pytest.mark.parametrize("n", [32, 64])
+def test_planar_transmission_constraint(n):
+    same(sc.planar_constrained(orc, n=n), sc.planar_constrained(ref, n=n))
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_fresnel_transmission_constraint(n):
+    same(sc.fresnel_constrained(orc, n=n), sc.fresnel_constrained(ref, n=n))
+
+
+@pytest.mark.parametrize("n", [32, 64])
 def test_fresnel_wf(n):
     same(sc.fresnel_wf_mixed(orc, n=n), sc.fresnel_wf_mixed(ref, n=n))
 
