@@ -11,6 +11,9 @@
 //   - propagate_to_detector / propagate_from_detector / scale_intensity /
 //     apply_support / project_intensity on a caller's field run in FP64 and
 //     are not available on FP32 reconstructions;
+//   - set_algorithm, set_custom_algorithm, set_relaxation_parameter and
+//     print_algorithm are virtual, so FresnelCDI_WF's versions (a warning:
+//     its algorithm is fixed) answer calls through a BaseCDI pointer too;
 //   - a TransmissionConstraint given to set_complex_constraint runs in the
 //     FP64 form only, and is read when iterate() or apply_support() next runs
 //     (changes to it after that are picked up at the following call).
@@ -113,7 +116,7 @@ public:
         std::vector<double> d = to_double(beam_stop_region);
         nadia_cxx::check(nadia_set_beam_stop(h, d.data()));
     }
-    void set_relaxation_parameter(double relaxation_parameter)
+    virtual void set_relaxation_parameter(double relaxation_parameter)
     {
         nadia_cxx::check(nadia_set_relaxation_parameter(h, relaxation_parameter));
     }
@@ -131,14 +134,14 @@ public:
         complex.push();
     }
 
-    void set_algorithm(int alg) { nadia_cxx::check(nadia_set_algorithm(h, alg)); }
-    void set_custom_algorithm(double m1, double m2, double m3, double m4, double m5, double m6,
+    virtual void set_algorithm(int alg) { nadia_cxx::check(nadia_set_algorithm(h, alg)); }
+    virtual void set_custom_algorithm(double m1, double m2, double m3, double m4, double m5, double m6,
                               double m7, double m8, double m9, double m10)
     {
         const double m[10] = {m1, m2, m3, m4, m5, m6, m7, m8, m9, m10};
         nadia_cxx::check(nadia_set_custom_algorithm(h, m));
     }
-    void print_algorithm()
+    virtual void print_algorithm()
     {
         double w[5];
         int alg = 0;

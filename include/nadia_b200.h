@@ -130,6 +130,12 @@ int nadia_poly_set_spectrum(nadia_solver *s, const double *wl_weight, int nlambd
  * energy stored as its reciprocal, values pass through float). */
 int nadia_poly_set_spectrum_file(nadia_solver *s, const char *path);
 
+/* read_spec (NADIA/src/io_spec.c:61-133) on its own: parses the file into
+ * rows of (1/energy, weight), writes min(*nrows, capacity) of them to rows
+ * (2 doubles each; rows may be NULL when capacity is 0) and sets *nrows to
+ * the number in the file.  Needs no GPU. */
+int nadia_read_spec(const char *path, double *rows, int capacity, int *nrows);
+
 /* The padding PolyCDI derived from its spectrum (PolyCDI.c++:86-87). */
 int nadia_poly_get_padding(const nadia_solver *s, int *px, int *py);
 

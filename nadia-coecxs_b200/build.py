@@ -68,5 +68,31 @@ def build(force=False, verbose=False):
     return LIB
 
 
+CLI_SRC = os.path.join(HERE, "cli", "CDI_reconstruction.cpp")
+BIN = os.path.join(HERE, "bin")
+
+
+def build_cli(force=False):
+    """Compile the reconstruction tool twice (float and DOUBLE_PRECISION
+    builds) against the drop-in headers and libnadia_b200.so; returns the
+    paths of bin/CDI_reconstruction and bin/CDI_reconstruction_double."""
+    lib = build(force)
+    os.makedirs(BIN, exist_ok=True)
+    deps = [CLI_SRC, lib] + [os.path.join(ROOT, "include", "nadia", f)
+                             for f in os.listdir(os.path.join(ROOT, "include", "nadia"))]
+    outs = []
+    for name, flags in (("CDI_reconstruction", []), ("CDI_reconstruction_double", ["-DDOUBLE_PRECISION"])):
+        out = os.path.join(BIN, name)
+        outs.append(out)
+        if not force and os.path.exists(out) and all(os.path.getmtime(d) <= os.path.getmtime(out)
+                                                     for d in deps):
+            continue
+        _run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", *flags,
+              "-I", os.path.join(ROOT, "include", "nadia"), "-I", os.path.join(ROOT, "include"),
+              CLI_SRC, "-L", HERE, "-lnadia_b200", "-Wl,-rpath,$ORIGIN/..", "-o", out])
+    return outs
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build_cli(force="--force" in sys.argv))

@@ -211,6 +211,20 @@ int nadia_poly_set_spectrum_file(nadia_solver *h, const char *path)
     });
 }
 
+int nadia_read_spec(const char *path, double *rows, int capacity, int *nrows)
+{
+    return guard([&] {
+        need(path, "path");
+        need(nrows, "nrows");
+        NADIA_REQUIRE(capacity >= 0, NADIA_ERR_INVALID, "negative capacity");
+        if (capacity > 0) need(rows, "rows");
+        std::vector<double> sp = nadia::read_spec_file(path);
+        const int n = (int)(sp.size() / 2);
+        std::copy(sp.begin(), sp.begin() + 2 * (size_t)std::min(n, capacity), rows);
+        *nrows = n;
+    });
+}
+
 int nadia_poly_get_padding(const nadia_solver *h, int *px, int *py)
 {
     return guard([&] {

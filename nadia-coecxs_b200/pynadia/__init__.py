@@ -80,6 +80,7 @@ _PROTOS = {
     "nadia_set_beam_stop": (_I, [_H, _D]),
     "nadia_poly_set_spectrum": (_I, [_H, _D, _I]),
     "nadia_poly_set_spectrum_file": (_I, [_H, ctypes.c_char_p]),
+    "nadia_read_spec": (_I, [ctypes.c_char_p, _D, _I, ctypes.POINTER(_I)]),
     "nadia_poly_get_padding": (_I, [_H, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "nadia_set_algorithm": (_I, [_H, _I]),
     "nadia_set_custom_algorithm": (_I, [_H, _D]),
@@ -162,6 +163,17 @@ def _check(rc):
 
 def _ptr(a):
     return a.ctypes.data_as(_D)
+
+
+def read_spec(path):
+    """read_spec (NADIA/src/io_spec.c:61-133): the file's rows of
+    (1/energy, weight) as an (n, 2) array.  Needs no GPU."""
+    lib = load()
+    n = ctypes.c_int()
+    _check(lib.nadia_read_spec(path.encode(), None, 0, ctypes.byref(n)))
+    out = np.zeros((n.value, 2))
+    _check(lib.nadia_read_spec(path.encode(), _ptr(out), n.value, ctypes.byref(n)))
+    return out
 
 
 def custom_weights(m):

@@ -8,6 +8,9 @@ against the FFTW shim:
   oracle/_ref/libnadia_ref64.so       -DDOUBLE_PRECISION, -O2 -fno-fast-math  (parity)
   oracle/_ref/libnadia_ref64_fast.so  -DDOUBLE_PRECISION, -O3 -ffast-math     (timing)
   oracle/_ref/libnadia_ref32_fast.so  float build,        -O3 -ffast-math     (timing)
+  oracle/_ref/libnadia_ref_io.a       io_*.c + Config.c++ (+ Complex_2D.c++), double build
+  oracle/_ref/CDI_reconstruction_ref  NADIA/tools/CDI_reconstruction.c, double build
+(libtiff, libhdf4 and LAPACK are not linked: ref_stubs.cpp stands in for them).
 The reference flags are those of NADIA/configure.in:11 (-O3 -fPIC -ffast-math).
 
 The reference headers are copied into oracle/_ref/include and three
@@ -133,10 +136,72 @@ def build_reference(force=False):
     return outs
 
 
+# the file helpers and configuration reader (test of include/nadia/io.h and
+# Config.h) and the reconstruction tool (test of the CLI)
+IO_SOURCES = [
+    "src/Complex_2D.c++",
+    "src/io_cplx.c",
+    "src/io_dbin.c",
+    "src/io_ppm.c",
+    "src/io_spec.c",
+    "src/Config.c++",
+]
+CLI_SOURCES = REF_SOURCES + [s for s in IO_SOURCES if s not in REF_SOURCES] + [
+    "src/utils.c",
+    "src/PartialCDI.c++",
+    "src/PartialCharCDI.c++",
+    "tools/CDI_reconstruction.c",
+]
+
+
+def _objects(nadia, inc, sources, objdir, flags, extra_own=()):
+    os.makedirs(objdir, exist_ok=True)
+    common = ["-fPIC", "-w", "-I", os.path.join(HERE, "shim"), "-I", inc, *flags]
+    objs = []
+    for s in sources:
+        o = os.path.join(objdir, s.replace("/", "_").replace(".", "_") + ".o")
+        _run(["g++", "-x", "c++", "-c", *common, os.path.join(nadia, s), "-o", o])
+        objs.append(o)
+    for f in extra_own:
+        o = os.path.join(objdir, os.path.basename(f).replace(".", "_") + ".o")
+        if f.endswith(".c"):
+            _run(["gcc", "-c", "-fPIC", "-w", *flags, f, "-o", o])
+        else:
+            _run(["g++", "-c", *common, f, "-o", o])
+        objs.append(o)
+    return objs
+
+
+def build_reference_tools(force=False):
+    """oracle/_ref/libnadia_ref_io.a (the reference's io_*.c, Config.c++ and
+    Complex_2D.c++, double build) and oracle/_ref/CDI_reconstruction_ref (the
+    reference's tool, double build, parity flags).  Needs the sources."""
+    nadia = reference_root()
+    if nadia is None:
+        return None
+    os.makedirs(REF_OUT, exist_ok=True)
+    inc = _copy_headers(nadia)
+    flags = ["-DDOUBLE_PRECISION", *PARITY_FLAGS]
+    stubs = os.path.join(HERE, "ref_stubs.cpp")
+    lib = os.path.join(REF_OUT, "libnadia_ref_io.a")
+    cli = os.path.join(REF_OUT, "CDI_reconstruction_ref")
+    own = [stubs, os.path.join(HERE, "fftw_shim.c")]
+    if force or _stale(lib, [os.path.join(nadia, s) for s in IO_SOURCES] + own):
+        objs = _objects(nadia, inc, IO_SOURCES, os.path.join(REF_OUT, "obj_io"), flags, own)
+        if os.path.exists(lib):
+            os.remove(lib)
+        _run(["ar", "rcs", lib, *objs])
+    if force or _stale(cli, [os.path.join(nadia, s) for s in CLI_SOURCES] + own):
+        objs = _objects(nadia, inc, CLI_SOURCES, os.path.join(REF_OUT, "obj_cli"), flags, own)
+        _run(["g++", "-o", cli, *objs, "-lm"])
+    return {"io": lib, "cli": cli, "include": inc}
+
+
 def main():
     force = "--force" in sys.argv
     print(build_oracle(force))
     print(build_reference(force))
+    print(build_reference_tools(force))
 
 
 if __name__ == "__main__":

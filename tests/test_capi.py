@@ -35,3 +35,15 @@ def test_custom_weights_host_only():
     assert np.allclose(w, [1.9, 0, -1, -0.9, 0])
     w = pynadia.custom_weights([0, 1, 0.8, 0, 0, 0, 0, 0, 0.2, 0])
     assert np.allclose(w, [1.8, 0, -0.8, -0.8, -0.2])
+
+
+def test_read_spec_host_only(tmp_path):
+    import pyoracle
+    p = tmp_path / "spec.txt"
+    p.write_text("Energy\tF.Density\n1200\t1.336e+15\n1208\t1.439e+15\n1216\t2e+15\n")
+    got = pynadia.read_spec(str(p))
+    assert np.array_equal(got, pyoracle.read_spec(str(p)))
+    assert got.shape == (3, 2)
+    import pytest
+    with pytest.raises(pynadia.NadiaError):
+        pynadia.read_spec(str(tmp_path / "missing.txt"))
