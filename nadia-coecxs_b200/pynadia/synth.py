@@ -174,6 +174,52 @@ class FresnelCase:
         self.support = disk_mask(n, ny, R * 1.1).astype(float)
 
 
+
+class PhaseDiverseCase:
+    """Phase-diverse Fresnel frames of one extended object: frame k sees the
+    n x n window of a global transmission function at its position
+    (positions[k]: the x, y given to PhaseDiverseCDI::add_new_position; the
+    window starts at global index -position - x_min with x_min = -position of
+    frame 0, PhaseDiverseCDI.h:380-397) under its own illumination -- a
+    different focus-to-sample distance per frame (the phase diversity)."""
+
+    def __init__(self, n, positions=((0, 0), (5, -3), (-4, 6)), seed=11, energy_kev=8.0,
+                 zfd=1.0, zfs=(1.0e-3, 0.97e-3, 1.04e-3), pixel=13.5e-6, photons=None):
+        self.n = n
+        self.positions = [tuple(float(v) for v in p) for p in positions]
+        self.wavelength = FresnelCase.HC_KEV_M / energy_kev
+        self.zfd, self.pixel = zfd, pixel
+        self.zfs = [zfs[k % len(zfs)] for k in range(len(positions))]
+        xmin = int(-self.positions[0][0])
+        ymin = int(-self.positions[0][1])
+        starts = [(int(-x - xmin), int(-y - ymin)) for x, y in self.positions]
+        lo_x = min(sx for sx, _ in starts)
+        lo_y = min(sy for _, sy in starts)
+        span_x = max(sx for sx, _ in starts) - lo_x + n
+        span_y = max(sy for _, sy in starts) - lo_y + n
+        g = rng(seed)
+        amp = gaussian_filter(g.uniform(0.75, 1.0, (span_x, span_y)), 1.5)
+        ph = gaussian_filter(g.uniform(-np.pi / 3, np.pi / 3, (span_x, span_y)), 2.0)
+        self.object = amp * np.exp(1j * ph)
+        i = np.arange(n)[:, None] - n / 2.0
+        j = np.arange(n)[None, :] - n / 2.0
+        r2 = i * i + j * j
+        rf = 0.42 * n
+        wamp = gaussian_filter((r2 <= rf * rf).astype(float), 2.0)
+        alpha = (math.pi / 8) / (2 * rf)
+        self.white_fields, self.intensities, self.windows = [], [], []
+        for k, (sx, sy) in enumerate(starts):
+            wf = wamp * np.exp(1j * alpha * r2 * (1 + 0.1 * k)) * 100.0
+            coef = fresnel_factor(n, n, self.wavelength, zfd, self.zfs[k], pixel)
+            illum = fresnel_from_detector(wf, coef)
+            T = self.object[sx - lo_x:sx - lo_x + n, sy - lo_y:sy - lo_y + n]
+            esw = (T - 1) * illum
+            I = np.abs(fresnel_to_detector(esw, coef) + wf) ** 2
+            self.white_fields.append(wf)
+            self.intensities.append(poisson_scale(I, photons, seed + k) if photons else I)
+            self.windows.append(T)
+        self.support = disk_mask(n, n, 0.36 * n).astype(float)
+
 # --------------------------------------------------------------------- Poly
 
 def gaussian_spectrum(nlines, fwhm_frac, lambda_ref, padding, n):

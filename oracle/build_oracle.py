@@ -35,7 +35,12 @@ REF_SOURCES = [
     "src/FresnelCDI_WF.c++",
     "src/PolyCDI.c++",
     "src/TransmissionConstraint.c++",
+    "src/PhaseDiverseCDI.c++",
+    "src/utils.c",
     "src/io_spec.c",
+    "src/io_cplx.c",
+    "src/io_dbin.c",
+    "src/io_ppm.c",
 ]
 
 # (file, 1-based line that closes an assignment operator without a return)
@@ -111,7 +116,7 @@ def build_reference(force=False):
     }
     srcs = [os.path.join(nadia, s) for s in REF_SOURCES]
     own = [os.path.join(HERE, f) for f in ("fftw_shim.c", "canon_fft.h", "ref_driver.cpp",
-                                           "shim/fftw3.h")]
+                                           "ref_stubs.cpp", "shim/fftw3.h")]
     outs = {}
     for name, flags in variants.items():
         out = os.path.join(REF_OUT, name)
@@ -128,6 +133,9 @@ def build_reference(force=False):
             objs.append(o)
         o = os.path.join(objdir, "ref_driver.o")
         _run(["g++", "-c", *common, os.path.join(HERE, "ref_driver.cpp"), "-o", o])
+        objs.append(o)
+        o = os.path.join(objdir, "ref_stubs.o")
+        _run(["g++", "-c", *common, os.path.join(HERE, "ref_stubs.cpp"), "-o", o])
         objs.append(o)
         o = os.path.join(objdir, "fftw_shim.o")
         _run(["gcc", "-c", "-fPIC", "-w", *flags, os.path.join(HERE, "fftw_shim.c"), "-o", o])
@@ -147,7 +155,6 @@ IO_SOURCES = [
     "src/Config.c++",
 ]
 CLI_SOURCES = REF_SOURCES + [s for s in IO_SOURCES if s not in REF_SOURCES] + [
-    "src/utils.c",
     "src/PartialCDI.c++",
     "src/PartialCharCDI.c++",
     "tools/CDI_reconstruction.c",

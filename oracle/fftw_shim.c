@@ -5,8 +5,12 @@
  * reference sources can be compiled and run here as a CPU oracle and as the
  * timed CPU baseline.  fftw_malloc returns zeroed memory; that neutralises the
  * uninitialised padding rows that Complex_2D::get_padded leaves
- * (NADIA/src/Complex_2D.c++:421-433).  The real-to-complex plans are not used
- * by the phase-retrieval loop and abort if executed.
+ * (NADIA/src/Complex_2D.c++:421-433).  The real-to-complex plans (used only by
+ * the image alignment of PhaseDiverseCDI, NADIA/src/utils.c:1151-1300) go
+ * through the same complex transform: r2c keeps columns 0..ny/2 of the
+ * transform of (x, 0) in FFTW's n0 x (n1/2+1) layout; c2r extends the half
+ * spectrum by Hermitian symmetry, runs the backward transform and keeps the
+ * real part (both unnormalised, as FFTW).
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -16,6 +20,7 @@
 CANON_FFT_DEFINE(d, double)
 CANON_FFT_DEFINE(f, float)
 
+/* real: 0 complex-to-complex, 1 r2c, 2 c2r */
 struct nadia_shim_plan_d { canon_ctxd *ctx; fftw_complex *in, *out; int nx, ny, fwd, real; };
 struct nadia_shim_plan_f { canon_ctxf *ctx; fftwf_complex *in, *out; int nx, ny, fwd, real; };
 
@@ -37,20 +42,63 @@ fftw_plan fftw_plan_dft_2d(int n0, int n1, fftw_complex *in, fftw_complex *out, 
     p->in = in; p->out = out; p->nx = n0; p->ny = n1; p->fwd = (sign == FFTW_FORWARD);
     return p;
 }
+static fftw_plan shim_real_pland(int n0, int n1, void *in, void *out, int kind)
+{
+    fftw_plan p = (fftw_plan)calloc(1, sizeof(*p));
+    p->ctx = canon_ctx_created(n0, n1);
+    if (!p->ctx) { fprintf(stderr, "fftw shim: unsupported size %dx%d\n", n0, n1); abort(); }
+    p->in = (fftw_complex *)in; p->out = (fftw_complex *)out;
+    p->nx = n0; p->ny = n1; p->real = kind;
+    return p;
+}
 fftw_plan fftw_plan_dft_r2c_2d(int n0, int n1, double *in, fftw_complex *out, unsigned flags)
 {
-    (void)in; (void)out; (void)flags;
-    fftw_plan p = (fftw_plan)calloc(1, sizeof(*p));
-    p->nx = n0; p->ny = n1; p->real = 1;
-    return p;
+    (void)flags;
+    return shim_real_pland(n0, n1, in, out, 1);
 }
 fftw_plan fftw_plan_dft_c2r_2d(int n0, int n1, fftw_complex *in, double *out, unsigned flags)
 {
-    return fftw_plan_dft_r2c_2d(n0, n1, (double *)in, (fftw_complex *)out, flags);
+    (void)flags;
+    return shim_real_pland(n0, n1, in, out, 2);
+}
+
+static void shim_real_execd(fftw_plan p)
+{
+    const int nx = p->nx, ny = p->ny, h = ny / 2 + 1;
+    canon_cd *t = (canon_cd *)zalloc(sizeof(canon_cd) * (size_t)nx * ny);
+    if (p->real == 1) {
+        const double *in = (const double *)p->in;
+        double *out = (double *)p->out;
+        for (size_t k = 0; k < (size_t)nx * ny; ++k) { t[k].re = in[k]; t[k].im = 0; }
+        canon_fft2d_execd(p->ctx, t, 1);
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < h; ++y) {
+                out[2 * ((size_t)x * h + y)] = t[(size_t)x * ny + y].re;
+                out[2 * ((size_t)x * h + y) + 1] = t[(size_t)x * ny + y].im;
+            }
+    } else {
+        const double *in = (const double *)p->in;
+        double *out = (double *)p->out;
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y) {
+                canon_cd *d = &t[(size_t)x * ny + y];
+                if (y < h) {
+                    d->re = in[2 * ((size_t)x * h + y)];
+                    d->im = in[2 * ((size_t)x * h + y) + 1];
+                } else {
+                    const size_t k = (size_t)((nx - x) % nx) * h + (ny - y);
+                    d->re = in[2 * k];
+                    d->im = -in[2 * k + 1];
+                }
+            }
+        canon_fft2d_execd(p->ctx, t, 0);
+        for (size_t k = 0; k < (size_t)nx * ny; ++k) out[k] = t[k].re;
+    }
+    free(t);
 }
 void fftw_execute(const fftw_plan p)
 {
-    if (p->real) { fprintf(stderr, "fftw shim: r2c/c2r not provided\n"); abort(); }
+    if (p->real) { shim_real_execd(p); return; }
     if (p->out != p->in) memcpy(p->out, p->in, sizeof(fftw_complex) * (size_t)p->nx * p->ny);
     canon_fft2d_execd(p->ctx, (canon_cd *)p->out, p->fwd);
 }
@@ -70,20 +118,63 @@ fftwf_plan fftwf_plan_dft_2d(int n0, int n1, fftwf_complex *in, fftwf_complex *o
     p->in = in; p->out = out; p->nx = n0; p->ny = n1; p->fwd = (sign == FFTW_FORWARD);
     return p;
 }
+static fftwf_plan shim_real_planf(int n0, int n1, void *in, void *out, int kind)
+{
+    fftwf_plan p = (fftwf_plan)calloc(1, sizeof(*p));
+    p->ctx = canon_ctx_createf(n0, n1);
+    if (!p->ctx) { fprintf(stderr, "fftw shim: unsupported size %dx%d\n", n0, n1); abort(); }
+    p->in = (fftwf_complex *)in; p->out = (fftwf_complex *)out;
+    p->nx = n0; p->ny = n1; p->real = kind;
+    return p;
+}
 fftwf_plan fftwf_plan_dft_r2c_2d(int n0, int n1, float *in, fftwf_complex *out, unsigned flags)
 {
-    (void)in; (void)out; (void)flags;
-    fftwf_plan p = (fftwf_plan)calloc(1, sizeof(*p));
-    p->nx = n0; p->ny = n1; p->real = 1;
-    return p;
+    (void)flags;
+    return shim_real_planf(n0, n1, in, out, 1);
 }
 fftwf_plan fftwf_plan_dft_c2r_2d(int n0, int n1, fftwf_complex *in, float *out, unsigned flags)
 {
-    return fftwf_plan_dft_r2c_2d(n0, n1, (float *)in, (fftwf_complex *)out, flags);
+    (void)flags;
+    return shim_real_planf(n0, n1, in, out, 2);
+}
+
+static void shim_real_execf(fftwf_plan p)
+{
+    const int nx = p->nx, ny = p->ny, h = ny / 2 + 1;
+    canon_cf *t = (canon_cf *)zalloc(sizeof(canon_cf) * (size_t)nx * ny);
+    if (p->real == 1) {
+        const float *in = (const float *)p->in;
+        float *out = (float *)p->out;
+        for (size_t k = 0; k < (size_t)nx * ny; ++k) { t[k].re = in[k]; t[k].im = 0; }
+        canon_fft2d_execf(p->ctx, t, 1);
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < h; ++y) {
+                out[2 * ((size_t)x * h + y)] = t[(size_t)x * ny + y].re;
+                out[2 * ((size_t)x * h + y) + 1] = t[(size_t)x * ny + y].im;
+            }
+    } else {
+        const float *in = (const float *)p->in;
+        float *out = (float *)p->out;
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y) {
+                canon_cf *d = &t[(size_t)x * ny + y];
+                if (y < h) {
+                    d->re = in[2 * ((size_t)x * h + y)];
+                    d->im = in[2 * ((size_t)x * h + y) + 1];
+                } else {
+                    const size_t k = (size_t)((nx - x) % nx) * h + (ny - y);
+                    d->re = in[2 * k];
+                    d->im = -in[2 * k + 1];
+                }
+            }
+        canon_fft2d_execf(p->ctx, t, 0);
+        for (size_t k = 0; k < (size_t)nx * ny; ++k) out[k] = t[k].re;
+    }
+    free(t);
 }
 void fftwf_execute(const fftwf_plan p)
 {
-    if (p->real) { fprintf(stderr, "fftw shim: r2c/c2r not provided\n"); abort(); }
+    if (p->real) { shim_real_execf(p); return; }
     if (p->out != p->in) memcpy(p->out, p->in, sizeof(fftwf_complex) * (size_t)p->nx * p->ny);
     canon_fft2d_execf(p->ctx, (canon_cf *)p->out, p->fwd);
 }

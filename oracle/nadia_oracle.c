@@ -1084,3 +1084,641 @@ int orc_padding(orc_solver *s, int *px, int *py)
     *py = s->py;
     return 0;
 }
+
+/* ===================== PhaseDiverseCDI (NADIA/src/PhaseDiverseCDI.c++) =====================
+ *
+ * Frames are orc_solver reconstructions (Fresnel: the transmission function is
+ * exchanged, PhaseDiverseCDI.c++:330-345; others: the exit-surface wave) placed
+ * at (x, y) on a global object.  remove_positions forgets the frames only; the
+ * positions, scalings, weights and per-frame results stay indexed as before
+ * (PhaseDiverseCDI.c++:60-66).  Arrays the reference leaves uninitialised
+ * (new Complex_2D) are zero here, as under the FFTW shim's fftw_malloc. */
+
+typedef struct orc_pd {
+    double beta, gamma;
+    int parallel, scale;
+    int nframes;            /* singleCDI.size() */
+    int npos, cap;          /* x_position.size() and capacity */
+    orc_solver **frame;
+    double *xpos, *ypos, *alpha;
+    double **result;        /* single_result: lnx*lny*2 each */
+    double **weight;        /* weights: lnx*lny each */
+    int *rnx, *rny;         /* sizes of result/weight n */
+    double *object;         /* nx*ny*2, NULL before the first position */
+    int nx, ny, x_min, y_min;
+    int iterations_per_cycle;
+    int weights_set;
+} orc_pd;
+
+orc_pd *orc_pd_create(double beta, double gamma, int parallel, int granularity)
+{
+    orc_pd *p = (orc_pd *)calloc(1, sizeof(orc_pd));
+    p->beta = beta;
+    p->gamma = gamma;
+    p->parallel = parallel != 0;
+    p->scale = granularity;
+    p->iterations_per_cycle = 1;
+    return p;
+}
+
+void orc_pd_destroy(orc_pd *p)
+{
+    if (!p) return;
+    for (int n = 0; n < p->npos; ++n) {
+        free(p->result[n]);
+        free(p->weight[n]);
+    }
+    free(p->frame); free(p->xpos); free(p->ypos); free(p->alpha);
+    free(p->result); free(p->weight); free(p->rnx); free(p->rny);
+    free(p->object);
+    free(p);
+}
+
+/* the get_global/local_x/y_pos helpers, PhaseDiverseCDI.h:380-397 (int results) */
+static inline int pd_gx(const orc_pd *p, int x, double off) { return (int)(x - off - p->x_min); }
+static inline int pd_gy(const orc_pd *p, int y, double off) { return (int)(y - off - p->y_min); }
+static inline int pd_lx(const orc_pd *p, int x, double off) { return (int)(x + off + p->x_min); }
+static inline int pd_ly(const orc_pd *p, int y, double off) { return (int)(y + off + p->y_min); }
+
+/* reallocate_object_memory, PhaseDiverseCDI.c++:68-75 */
+static void pd_realloc_object(orc_pd *p, int nx, int ny)
+{
+    free(p->object);
+    p->object = zd(2 * (size_t)nx * ny);
+    p->nx = nx;
+    p->ny = ny;
+}
+
+/* add_new_position, PhaseDiverseCDI.c++:104-160 */
+void orc_pd_add_position(orc_pd *p, orc_solver *frame, double x, double y, double alpha)
+{
+    p->weights_set = 0;
+    const int lnx = frame->nx, lny = frame->ny;
+    if (p->nframes >= p->cap || p->npos >= p->cap) {
+        int cap = p->cap ? 2 * p->cap : 8;
+        p->frame = (orc_solver **)realloc(p->frame, cap * sizeof(void *));
+        p->xpos = (double *)realloc(p->xpos, cap * sizeof(double));
+        p->ypos = (double *)realloc(p->ypos, cap * sizeof(double));
+        p->alpha = (double *)realloc(p->alpha, cap * sizeof(double));
+        p->result = (double **)realloc(p->result, cap * sizeof(double *));
+        p->weight = (double **)realloc(p->weight, cap * sizeof(double *));
+        p->rnx = (int *)realloc(p->rnx, cap * sizeof(int));
+        p->rny = (int *)realloc(p->rny, cap * sizeof(int));
+        p->cap = cap;
+    }
+    p->frame[p->nframes++] = frame;
+    const int k = p->npos++;
+    p->xpos[k] = x;
+    p->ypos[k] = y;
+    p->alpha[k] = alpha;
+    p->result[k] = zd(2 * (size_t)lnx * lny);
+    p->weight[k] = zd((size_t)lnx * lny);
+    p->rnx[k] = lnx;
+    p->rny[k] = lny;
+    if (!p->object) {
+        p->x_min = (int)(-x);
+        p->y_min = (int)(-y);
+        pd_realloc_object(p, lnx * p->scale, lny * p->scale);
+    }
+    int extra_x = 0, extra_y = 0;
+    const int gx0 = pd_gx(p, 0, x) * p->scale, gy0 = pd_gy(p, 0, y) * p->scale;
+    const int gx1 = pd_gx(p, lnx, x) * p->scale, gy1 = pd_gy(p, lny, y) * p->scale;
+    if (gx0 < 0) {
+        p->x_min = (int)(-x);
+        extra_x += -gx0;
+    }
+    if (gy0 < 0) {
+        p->y_min = (int)(-y);
+        extra_y += -gy0;
+    }
+    if (gx1 > p->nx) extra_x += gx1 - p->nx;
+    if (gy1 > p->ny) extra_y += gy1 - p->ny;
+    if (extra_x || extra_y) pd_realloc_object(p, p->nx + extra_x, p->ny + extra_y);
+}
+
+void orc_pd_remove_positions(orc_pd *p) { p->nframes = 0; }
+
+/* set_up_weights, PhaseDiverseCDI.c++:450-530 */
+static void pd_set_up_weights(orc_pd *p)
+{
+    if (p->weights_set) return;
+    p->weights_set = 1;
+    const int frames = p->nframes;
+    for (int n = 0; n < frames; ++n) {
+        const int lnx = p->rnx[n], lny = p->rny[n];
+        orc_solver *f = p->frame[n];
+        double *illum_mag = NULL, max = 0;
+        if (f->kind == KIND_FRESNEL) {
+            /* the frame's size is the result's size for the frames added since
+             * the last remove_positions; the reference reads illum by the
+             * result's size too */
+            illum_mag = zd((size_t)lnx * lny);
+            for (size_t k = 0; k < (size_t)lnx * lny; ++k) illum_mag[k] = mag_of(f->illum_sample + 2 * k);
+            max = illum_mag[0];
+            for (size_t k = 0; k < (size_t)lnx * lny; ++k)
+                if (illum_mag[k] > max) max = illum_mag[k];
+        }
+        for (int i = 0; i < lnx; ++i)
+            for (int j = 0; j < lny; ++j) {
+                double value = f->kind == KIND_FRESNEL ? illum_mag[(size_t)i * lny + j] / max : 1;
+                value = p->alpha[n] * pow(value, p->gamma);
+                if (f->support[(size_t)i * f->ny + j] <= 0.0) value = 0;
+                if (!p->parallel) value *= p->beta;
+                p->weight[n][(size_t)i * lny + j] = value;
+            }
+        free(illum_mag);
+    }
+    if (!p->parallel) return;
+    double *norm = zd((size_t)p->nx * p->ny);
+    for (int n = 0; n < frames; ++n)
+        for (int i_ = 0; i_ < p->rnx[n]; ++i_)
+            for (int j_ = 0; j_ < p->rny[n]; ++j_) {
+                const int i = pd_gx(p, i_, p->xpos[n]), j = pd_gy(p, j_, p->ypos[n]);
+                if (i >= 0 && j >= 0 && i < p->nx && j < p->ny) {
+                    const double w = p->weight[n][(size_t)i_ * p->rny[n] + j_];
+                    double *t = &norm[(size_t)i * p->ny + j];
+                    *t = n == 0 ? w : w + *t;
+                }
+            }
+    for (int n = 0; n < frames; ++n)
+        for (int i_ = 0; i_ < p->rnx[n]; ++i_)
+            for (int j_ = 0; j_ < p->rny[n]; ++j_) {
+                const int i = pd_gx(p, i_, p->xpos[n]), j = pd_gy(p, j_, p->ypos[n]);
+                if (i >= 0 && j >= 0 && i < p->nx && j < p->ny) {
+                    double *w = &p->weight[n][(size_t)i_ * p->rny[n] + j_];
+                    const double nn = norm[(size_t)i * p->ny + j];
+                    *w = nn <= 0 ? 0 : p->beta * *w / nn;
+                }
+            }
+    free(norm);
+}
+
+/* get_result / set_result, PhaseDiverseCDI.c++:330-345 */
+static void pd_get_result(orc_solver *f, double *r) { orc_get_transmission(f, r); }
+static void pd_set_result(orc_solver *f, const double *r) { orc_set_transmission(f, r); }
+
+/* add_to_object, PhaseDiverseCDI.c++:537-640 */
+static void pd_add_to_object(orc_pd *p, int n)
+{
+    pd_get_result(p->frame[n], p->result[n]);
+    pd_set_up_weights(p);
+    const double xo = p->xpos[n], yo = p->ypos[n];
+    const double *small = p->result[n], *w = p->weight[n];
+    const int lnx = p->rnx[n], lny = p->rny[n], sc = p->scale;
+    double *sub = zd(sc);
+    for (int d = 0; d < sc; ++d) sub[d] = (d + 0.5 * ((sc + 1) % 2)) / ((double)sc);
+    double *o = p->object;
+    for (int i_ = 1; i_ < lnx - 1; ++i_)
+        for (int j_ = 1; j_ < lny - 1; ++j_) {
+            const double wt = w[(size_t)i_ * lny + j_];
+            if (wt == 0) continue;
+            const int i = pd_gx(p, i_, xo) * sc, j = pd_gy(p, j_, yo) * sc;
+            if (!(i >= 0 && j >= 0 && i < p->nx && j < p->ny)) continue;
+            const double *f00 = small + 2 * ((size_t)i_ * lny + j_);
+            if (sc != 1) {
+                const double *f10 = small + 2 * ((size_t)(i_ + 1) * lny + j_);
+                const double *f01 = small + 2 * ((size_t)i_ * lny + j_ + 1);
+                const double *f11 = small + 2 * ((size_t)(i_ + 1) * lny + j_ + 1);
+                for (int di = 0; di < sc; ++di)
+                    for (int dj = 0; dj < sc; ++dj) {
+                        const double x = sub[di], y = sub[dj], x1 = 1 - x, y1 = 1 - y;
+                        const double vr = f00[0] * (x1) * (y1) + f10[0] * x * (y1) + f01[0] * (x1) * y + f11[0] * x * y;
+                        const double vi = f00[1] * (x1) * (y1) + f10[1] * x * (y1) + f01[1] * (x1) * y + f11[1] * x * y;
+                        const int ni = (int)((i_ + 0.5 - xo - p->x_min) * sc + di);
+                        const int nj = (int)((j_ + 0.5 - yo - p->y_min) * sc + dj);
+                        double *t = o + 2 * ((size_t)ni * p->ny + nj);
+                        double nr = wt * vr + t[0];
+                        double nim = wt * vi + t[1];
+                        if (!p->parallel) {
+                            nr -= wt * t[0];
+                            nim -= wt * t[1];
+                        }
+                        t[0] = nr;
+                        t[1] = nim;
+                    }
+            } else {
+                double *t = o + 2 * ((size_t)i * p->ny + j);
+                double nr = wt * f00[0] + t[0];
+                double nim = wt * f00[1] + t[1];
+                if (!p->parallel) {
+                    nr -= wt * t[0];
+                    nim -= wt * t[1];
+                }
+                t[0] = nr;
+                t[1] = nim;
+            }
+        }
+    free(sub);
+}
+
+/* update_from_object, PhaseDiverseCDI.c++:664-711 */
+static void pd_update_from_object(orc_pd *p, int n)
+{
+    pd_set_up_weights(p);
+    const double xo = p->xpos[n], yo = p->ypos[n];
+    double *small = p->result[n];
+    const double *w = p->weight[n];
+    const int lnx = p->rnx[n], lny = p->rny[n], sc = p->scale;
+    const double *o = p->object;
+    for (int i_ = 0; i_ < lnx; ++i_)
+        for (int j_ = 0; j_ < lny; ++j_) {
+            if (w[(size_t)i_ * lny + j_] == 0) continue;
+            const int i = pd_gx(p, i_, xo) * sc, j = pd_gy(p, j_, yo) * sc;
+            if (!(i >= 0 && j >= 0 && i < p->nx && j < p->ny)) continue;
+            double *s = small + 2 * ((size_t)i_ * lny + j_);
+            if (sc != 1) {
+                double re = 0, im = 0;
+                for (int di = 0; di < sc; ++di)
+                    for (int dj = 0; dj < sc; ++dj) {
+                        re += o[2 * ((size_t)(i + di) * p->ny + j + dj)];
+                        im += o[2 * ((size_t)(i + di) * p->ny + j + dj) + 1];
+                    }
+                const double norm = 1 / ((double)(sc * sc));
+                s[0] = re * norm;
+                s[1] = im * norm;
+            } else {
+                s[0] = o[2 * ((size_t)i * p->ny + j)];
+                s[1] = o[2 * ((size_t)i * p->ny + j) + 1];
+            }
+        }
+    pd_set_result(p->frame[n], small);
+}
+
+/* scale_object, PhaseDiverseCDI.c++:290-325 */
+static void pd_scale_object(orc_pd *p, double factor)
+{
+    pd_set_up_weights(p);
+    for (int i = 0; i < p->nx; ++i)
+        for (int j = 0; j < p->ny; ++j) {
+            int inside = 0;
+            for (int n = 0; n < p->nframes; ++n) {
+                const int i_ = pd_lx(p, i / p->scale, p->xpos[n]);
+                const int j_ = pd_ly(p, j / p->scale, p->ypos[n]);
+                if (i_ >= 0 && j_ >= 0 && i_ < p->rnx[n] && j_ < p->rny[n]) {
+                    inside = p->weight[n][(size_t)i_ * p->rny[n] + j_] != 0;
+                    if (inside) break;
+                }
+            }
+            double *t = p->object + 2 * ((size_t)i * p->ny + j);
+            if (!inside) {
+                t[0] = 1.0;
+                t[1] = 0.0;
+            } else {
+                t[0] = factor * t[0];
+                t[1] = factor * t[1];
+            }
+        }
+}
+
+/* initialise_estimate, PhaseDiverseCDI.c++:163-177 */
+void orc_pd_initialise_estimate(orc_pd *p)
+{
+    if (!p->object) return; /* no position yet (the reference dereferences null) */
+    for (size_t k = 0; k < (size_t)p->nx * p->ny; ++k) {
+        p->object[2 * k] = 1;
+        p->object[2 * k + 1] = 0;
+    }
+    for (int n = 0; n < p->nframes; ++n) pd_add_to_object(p, n);
+}
+
+/* iterate, PhaseDiverseCDI.c++:180-230 (the reference also prints the
+ * iteration count and each frame's error) */
+void orc_pd_iterate(orc_pd *p)
+{
+    for (int n = 0; n < p->nframes; ++n) {
+        pd_update_from_object(p, n);
+        for (int k = 0; k < p->iterations_per_cycle; ++k) orc_iterate(p->frame[n]);
+        if (!p->parallel) pd_add_to_object(p, n);
+    }
+    if (p->parallel) {
+        pd_scale_object(p, 1 - p->beta);
+        for (int n = 0; n < p->nframes; ++n) pd_add_to_object(p, n);
+    }
+}
+
+void orc_pd_set_iterations_per_cycle(orc_pd *p, int n) { p->iterations_per_cycle = n; }
+void orc_pd_set_feedback_parameter(orc_pd *p, double b) { p->beta = b; p->weights_set = 0; }
+void orc_pd_set_amplification_factor(orc_pd *p, double g) { p->gamma = g; p->weights_set = 0; }
+/* set_probe_scaling, PhaseDiverseCDI.h:214-226: returns 0 when n is too large */
+int orc_pd_set_probe_scaling(orc_pd *p, int n, double alpha)
+{
+    int ok = n >= 0 && n < p->npos;
+    if (ok) p->alpha[n] = alpha;
+    p->weights_set = 0;
+    return ok;
+}
+void orc_pd_get_size(orc_pd *p, int *nx, int *ny)
+{
+    *nx = p->object ? p->nx : 0;
+    *ny = p->object ? p->ny : 0;
+}
+void orc_pd_get_transmission(orc_pd *p, double *out)
+{
+    memcpy(out, p->object, sizeof(double) * 2 * (size_t)p->nx * p->ny);
+}
+/* set_transmission, PhaseDiverseCDI.c++:81-101: returns 0 on a size mismatch */
+int orc_pd_set_transmission(orc_pd *p, int nx, int ny, const double *t)
+{
+    if (!p->object) pd_realloc_object(p, nx, ny);
+    if (nx != p->nx || ny != p->ny) return 0;
+    memcpy(p->object, t, sizeof(double) * 2 * (size_t)nx * ny);
+    return 1;
+}
+double orc_pd_get_x(orc_pd *p, int n) { return p->xpos[n]; }
+double orc_pd_get_y(orc_pd *p, int n) { return p->ypos[n]; }
+
+/* ---- image alignment (NADIA/src/utils.c:1151-1300) ---- */
+
+/* real-to-complex / complex-to-real transforms in FFTW's layout: r2c keeps
+ * columns 0..ny/2 of the transform of (x, 0); c2r extends by Hermitian
+ * symmetry and keeps the real part of the backward transform (unnormalised) */
+static void pd_r2c(const double *in, double *half, int nx, int ny)
+{
+    const int h = ny / 2 + 1;
+    double *t = zd(2 * (size_t)nx * ny);
+    for (size_t k = 0; k < (size_t)nx * ny; ++k) t[2 * k] = in[k];
+    canon_ctxd *c = canon_ctx_created(nx, ny);
+    canon_fft2d_execd(c, (canon_cd *)t, 1);
+    canon_ctx_destroyd(c);
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < h; ++y) {
+            half[2 * ((size_t)x * h + y)] = t[2 * ((size_t)x * ny + y)];
+            half[2 * ((size_t)x * h + y) + 1] = t[2 * ((size_t)x * ny + y) + 1];
+        }
+    free(t);
+}
+
+static void pd_c2r(const double *half, double *out, int nx, int ny)
+{
+    const int h = ny / 2 + 1;
+    double *t = zd(2 * (size_t)nx * ny);
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y) {
+            double *d = t + 2 * ((size_t)x * ny + y);
+            if (y < h) {
+                d[0] = half[2 * ((size_t)x * h + y)];
+                d[1] = half[2 * ((size_t)x * h + y) + 1];
+            } else {
+                const size_t k = (size_t)((nx - x) % nx) * h + (ny - y);
+                d[0] = half[2 * k];
+                d[1] = -half[2 * k + 1];
+            }
+        }
+    canon_ctxd *c = canon_ctx_created(nx, ny);
+    canon_fft2d_execd(c, (canon_cd *)t, 0);
+    canon_ctx_destroyd(c);
+    for (size_t k = 0; k < (size_t)nx * ny; ++k) out[k] = t[2 * k];
+    free(t);
+}
+
+/* c2r(conj(r2c(a)) * r2c(b)) with Complex_2D::multiply's operation order
+ * (Complex_2D.c++:203-228): the unnormalised cross-correlation */
+static void pd_correlate(const double *a, const double *b, double *out, int nx, int ny)
+{
+    const int h = ny / 2 + 1;
+    double *fa = zd(2 * (size_t)nx * h), *fb = zd(2 * (size_t)nx * h);
+    pd_r2c(a, fa, nx, ny);
+    pd_r2c(b, fb, nx, ny);
+    for (size_t k = 0; k < (size_t)nx * h; ++k) {
+        const double ar = fa[2 * k], ai = -1 * fa[2 * k + 1];
+        const double br = fb[2 * k], bi = fb[2 * k + 1];
+        const double nr = br * ar - bi * ai;
+        const double ni = br * ai + bi * ar;
+        fa[2 * k] = 1 * nr;
+        fa[2 * k + 1] = 1 * ni;
+    }
+    pd_c2r(fa, out, nx, ny);
+    free(fa);
+    free(fb);
+}
+
+/* align, utils.c:1151-1300 (with its default overlap fraction 0.2 passed in) */
+void orc_align(const double *first, int nx_1, int ny_1, const double *second, int nx_2, int ny_2,
+               int *offset_x, int *offset_y, int min_x, int max_x, int min_y, int max_y,
+               const double *first_w, const double *second_w, double overlap_fraction)
+{
+    const int nx = nx_1 > nx_2 ? nx_1 * 2 : nx_2 * 2;
+    const int ny = ny_1 > ny_2 ? ny_1 * 2 : ny_2 * 2;
+    if (min_x == max_x || min_y == max_y) {
+        min_x = (int)(1 - nx / 2.0);
+        max_x = (int)(nx / 2.0);
+        min_y = (int)(1 - ny / 2.0);
+        max_y = (int)(ny / 2.0);
+    }
+    const size_t N = (size_t)nx * ny;
+    double *img1 = zd(N), *img2 = zd(N), *w1 = zd(N), *w2 = zd(N);
+    double weight_sum = 0;
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            if (!(i >= 0.5 * (nx - nx_1) && i < 0.5 * (nx + nx_1) && j >= 0.5 * (ny - ny_1) &&
+                  j < 0.5 * (ny + ny_1)))
+                continue;
+            const int i_ = (int)(i - 0.5 * (nx - nx_1)), j_ = (int)(j - 0.5 * (ny - ny_1));
+            const size_t k = (size_t)i * ny + j;
+            if (!first_w || first_w[(size_t)i_ * ny_1 + j_] > 0) {
+                img1[k] = first[(size_t)i_ * ny_1 + j_];
+                w1[k] = 1.0;
+            }
+            if (i_ < nx_2 && j_ < ny_2 && (!second_w || second_w[(size_t)i_ * ny_2 + j_] > 0)) {
+                img2[k] = second[(size_t)i_ * ny_2 + j_];
+                w2[k] = 1.0;
+            }
+            if (nx_1 * ny_1 < nx_2 * ny_2)
+                weight_sum += w1[k];
+            else
+                weight_sum += w2[k];
+        }
+    double *corr = zd(N), *overlap = zd(N);
+    pd_correlate(img1, img2, corr, nx, ny);
+    pd_correlate(w1, w2, overlap, nx, ny);
+    double max = 0;
+    const double overlap_factor = weight_sum * nx * ny;
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            const size_t k = (size_t)i * ny + j;
+            if (!(overlap[k] / overlap_factor > overlap_fraction)) continue;
+            if (!(corr[k] / overlap[k] > max)) continue;
+            int ti = -i, tj = -j;
+            if (i >= nx / 2.0) ti = -i + nx;
+            if (j >= ny / 2.0) tj = -j + ny;
+            if (ti >= min_x && ti < max_x && tj >= min_y && tj < max_y) {
+                max = corr[k] / overlap[k];
+                *offset_x = ti;
+                *offset_y = tj;
+            }
+        }
+    free(img1); free(img2); free(w1); free(w2); free(corr); free(overlap);
+}
+
+/* interpolate(Double_2D, Double_2D), utils.c:1305-1352 (bilinear, border left 0) */
+static void pd_interpolate(const double *a, int nx, int ny, double *big, int sc)
+{
+    const int bny = ny * sc;
+    for (int i = 1; i < nx - 1; ++i)
+        for (int j = 1; j < ny - 1; ++j) {
+            const double f00 = a[(size_t)i * ny + j], f10 = a[(size_t)(i + 1) * ny + j];
+            const double f01 = a[(size_t)i * ny + j + 1], f11 = a[(size_t)(i + 1) * ny + j + 1];
+            const double ni = (i + 0.5) * sc, nj = (j + 0.5) * sc;
+            for (int di = 0; di < sc; ++di)
+                for (int dj = 0; dj < sc; ++dj) {
+                    const double x = (di + 0.5 * ((sc + 1) % 2)) / ((double)sc);
+                    const double y = (dj + 0.5 * ((sc + 1) % 2)) / ((double)sc);
+                    const double x1 = 1 - x, y1 = 1 - y;
+                    const double v = f00 * (x1) * (y1) + f10 * x * (y1) + f01 * (x1) * y + f11 * x * y;
+                    big[(size_t)(int)(ni + di) * bny + (int)(nj + dj)] = v;
+                }
+        }
+}
+
+/* check_position, PhaseDiverseCDI.c++:395-447 */
+static int pd_check_position(orc_pd *p, int n, double step, int min_x, int max_x, int min_y,
+                             int max_y, int tries)
+{
+    const double x = p->xpos[n], y = p->ypos[n];
+    if (step < 1.0 / p->scale) return 1;
+    if (tries > 10 || x < (x + min_x) || x > (x + max_x) || y < (y + min_y) || y > (y + max_y))
+        return 0;
+    orc_solver *single = p->frame[n];
+    double best_x = x, best_y = y, best_error = 100;
+    const size_t on = 2 * (size_t)p->nx * p->ny, sn = 2 * (size_t)p->rnx[n] * p->rny[n];
+    double *object_copy = zd(on), *single_copy = zd(sn);
+    memcpy(object_copy, p->object, on * sizeof(double));
+    memcpy(single_copy, p->result[n], sn * sizeof(double));
+    p->beta = 0.5;
+    p->weights_set = 0;
+    for (int i = -1; i < 2; ++i)
+        for (int j = -1; j < 2; ++j) {
+            const double nx_ = x + i * step, ny_ = y + j * step;
+            p->xpos[n] = nx_;
+            p->ypos[n] = ny_;
+            pd_add_to_object(p, n);
+            pd_update_from_object(p, n);
+            orc_iterate(single);
+            if (orc_get_error(single) < best_error) {
+                best_error = orc_get_error(single);
+                best_x = nx_;
+                best_y = ny_;
+            }
+            memcpy(p->object, object_copy, on * sizeof(double));
+            pd_set_result(single, single_copy);
+            memcpy(p->result[n], single_copy, sn * sizeof(double));
+        }
+    free(object_copy);
+    free(single_copy);
+    p->xpos[n] = best_x;
+    p->ypos[n] = best_y;
+    if (best_x == x && best_y == y) step = step / 2.0;
+    if (!pd_check_position(p, n, step, min_x, max_x, min_y, max_y, ++tries)) {
+        p->xpos[n] = x;
+        p->ypos[n] = y;
+        return 0;
+    }
+    p->beta = 1.0;
+    p->weights_set = 0;
+    return 1;
+}
+
+/* adjust_positions, PhaseDiverseCDI.c++:232-392; returns 0 for an unknown type */
+int orc_pd_adjust_positions(orc_pd *p, int type, int forward, int min_x, int max_x, int min_y,
+                            int max_y, double step_size)
+{
+    if (type != 0 && type != 1) return 0;
+    const int parallel_c = p->parallel;
+    double *saved_object = p->object;
+    const int nx_c = p->nx, ny_c = p->ny, x_min_c = p->x_min, y_min_c = p->y_min;
+    const double beta_c = p->beta;
+    const int sc = p->scale;
+    p->parallel = 0;
+    int n = 1, limit = p->nframes;
+    if (!forward) {
+        n = p->nframes - 2;
+        limit = -1;
+    }
+    double *temp_object = zd(2 * (size_t)p->nx * p->ny);
+    for (size_t k = 0; k < (size_t)p->nx * p->ny; ++k) temp_object[2 * k] = 1;
+    p->object = temp_object;
+    p->beta = 1.0;
+    p->weights_set = 0;
+    const int first = forward ? 0 : p->nframes - 1;
+    orc_iterate(p->frame[first]);
+    pd_get_result(p->frame[first], p->result[first]);
+    pd_add_to_object(p, first);
+    while (n != limit) {
+        const double bx = p->xpos[n], by = p->ypos[n];
+        const int lnx = p->rnx[0], lny = p->rny[0];
+        orc_iterate(p->frame[n]);
+        pd_get_result(p->frame[n], p->result[n]);
+        const int bnx = lnx * sc, bny = lny * sc;
+        if (type == 0) { /* CROSS_CORRELATION */
+            double *single = zd((size_t)lnx * lny), *others = zd((size_t)bnx * bny);
+            for (int i = 0; i < bnx; ++i)
+                for (int j = 0; j < bny; ++j) {
+                    const int i_ = (int)(i - bx * sc - p->x_min * sc);
+                    const int j_ = (int)(j - by * sc - p->y_min * sc);
+                    if (i_ >= 0 && j_ >= 0 && i_ < p->nx && j_ < p->ny) {
+                        const double m = mag_of(p->object + 2 * ((size_t)i_ * p->ny + j_));
+                        if (m < 1) others[(size_t)i * bny + j] = 1 - m;
+                    }
+                    if (i < lnx && j < lny) {
+                        const double m = mag_of(p->result[n] + 2 * ((size_t)i * p->rny[n] + j));
+                        if (m < 1) single[(size_t)i * lny + j] = 1 - m;
+                    }
+                }
+            double *single_int, *weight_int = zd((size_t)bnx * bny);
+            orc_solver *f = p->frame[n];
+            if (sc == 1) {
+                single_int = single;
+                memcpy(weight_int, f->support, sizeof(double) * (size_t)bnx * bny);
+            } else {
+                single_int = zd((size_t)bnx * bny);
+                pd_interpolate(single, lnx, lny, single_int, sc);
+                pd_interpolate(f->support, f->nx, f->ny, weight_int, sc);
+            }
+            int new_x = 0, new_y = 0;
+            orc_align(single_int, bnx, bny, others, bnx, bny, &new_x, &new_y, min_x, max_x, min_y,
+                      max_y, weight_int, others, 0.2);
+            p->xpos[n] = bx + new_x / ((double)sc);
+            p->ypos[n] = by + new_y / ((double)sc);
+            if (single_int != single) free(single_int);
+            free(single);
+            free(others);
+            free(weight_int);
+        } else { /* MINIMUM_ERROR */
+            double *temp = zd(2 * (size_t)bnx * bny);
+            for (int i = 0; i < bnx; ++i)
+                for (int j = 0; j < bny; ++j) {
+                    const int i_ = (int)(i - bx * sc - p->x_min * sc);
+                    const int j_ = (int)(j - by * sc - p->y_min * sc);
+                    if (i_ >= 0 && j_ >= 0 && i_ < p->nx && j_ < p->ny) {
+                        temp[2 * ((size_t)i * bny + j)] = p->object[2 * ((size_t)i_ * p->ny + j_)];
+                        temp[2 * ((size_t)i * bny + j) + 1] = p->object[2 * ((size_t)i_ * p->ny + j_) + 1];
+                    }
+                }
+            p->object = temp;
+            p->nx = bnx;
+            p->ny = bny;
+            p->x_min = (int)(-p->xpos[n]);
+            p->y_min = (int)(-p->ypos[n]);
+            pd_check_position(p, n, step_size, min_x, max_x, min_y, max_y, 0);
+            free(temp);
+            p->object = temp_object;
+            p->nx = nx_c;
+            p->ny = ny_c;
+            p->x_min = x_min_c;
+            p->y_min = y_min_c;
+        }
+        p->weights_set = 0;
+        pd_add_to_object(p, n);
+        n += forward ? 1 : -1;
+    }
+    free(temp_object);
+    p->object = saved_object;
+    p->nx = nx_c;
+    p->ny = ny_c;
+    p->x_min = x_min_c;
+    p->y_min = y_min_c;
+    p->parallel = parallel_c;
+    p->beta = beta_c;
+    p->weights_set = 0;
+    return 1;
+}

@@ -326,3 +326,107 @@ def Oracle(kind, nx, ny, **kw):
 
 def Reference(kind, nx, ny, variant="64", **kw):
     return _Solver(reference_lib(variant), kind, nx, ny, **kw)
+
+
+_PD_PROTOS = {
+    "pd_create": (_V, [ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
+    "pd_destroy": (None, [_V]),
+    "pd_add_position": (None, [_V, _V, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+    "pd_remove_positions": (None, [_V]),
+    "pd_initialise_estimate": (None, [_V]),
+    "pd_iterate": (None, [_V]),
+    "pd_set_iterations_per_cycle": (None, [_V, ctypes.c_int]),
+    "pd_set_feedback_parameter": (None, [_V, ctypes.c_double]),
+    "pd_set_amplification_factor": (None, [_V, ctypes.c_double]),
+    "pd_set_probe_scaling": (None, [_V, ctypes.c_int, ctypes.c_double]),
+    "pd_get_size": (None, [_V, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "pd_get_transmission": (None, [_V, _D]),
+    "pd_set_transmission": (None, [_V, ctypes.c_int, ctypes.c_int, _D]),
+    "pd_adjust_positions": (None, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_double]),
+    "pd_get_x": (ctypes.c_double, [_V, ctypes.c_int]),
+    "pd_get_y": (ctypes.c_double, [_V, ctypes.c_int]),
+}
+
+
+class _PhaseDiverse:
+    """PhaseDiverseCDI (NADIA/include/PhaseDiverseCDI.h) over frames made by
+    the same library's Oracle / Reference factory."""
+
+    CROSS_CORRELATION, MINIMUM_ERROR = 0, 1
+
+    def __init__(self, L, beta=1.0, gamma=1.0, parallel=False, granularity=1):
+        self.L = L
+        self.f = {}
+        for name, (res, args) in _PD_PROTOS.items():
+            fn = getattr(L.lib, L.prefix + name)
+            fn.restype = res
+            fn.argtypes = args
+            self.f[name] = fn
+        self.h = self.f["pd_create"](beta, gamma, int(bool(parallel)), granularity)
+        self.frames = []
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.f["pd_destroy"](self.h)
+            self.h = None
+
+    def add_new_position(self, frame, x=0.0, y=0.0, alpha=1.0):
+        assert frame.L is self.L
+        self.frames.append(frame)
+        self.f["pd_add_position"](self.h, frame.h, x, y, alpha)
+
+    def remove_positions(self):
+        self.f["pd_remove_positions"](self.h)
+
+    def initialise_estimate(self):
+        self.f["pd_initialise_estimate"](self.h)
+
+    def iterate(self):
+        self.f["pd_iterate"](self.h)
+
+    def set_iterations_per_cycle(self, n):
+        self.f["pd_set_iterations_per_cycle"](self.h, n)
+
+    def set_feedback_parameter(self, b):
+        self.f["pd_set_feedback_parameter"](self.h, b)
+
+    def set_amplification_factor(self, g):
+        self.f["pd_set_amplification_factor"](self.h, g)
+
+    def set_probe_scaling(self, n, alpha):
+        self.f["pd_set_probe_scaling"](self.h, n, alpha)
+
+    def size(self):
+        nx, ny = ctypes.c_int(), ctypes.c_int()
+        self.f["pd_get_size"](self.h, ctypes.byref(nx), ctypes.byref(ny))
+        return nx.value, ny.value
+
+    def get_transmission(self):
+        nx, ny = self.size()
+        out = np.empty((nx, ny), dtype=np.complex128)
+        self.f["pd_get_transmission"](self.h, _ptr(out))
+        return out
+
+    def set_transmission(self, t):
+        t = np.ascontiguousarray(t, dtype=np.complex128)
+        self.f["pd_set_transmission"](self.h, t.shape[0], t.shape[1], _ptr(t))
+
+    def adjust_positions(self, type=0, forward=True, x_min=-50, x_max=50, y_min=-50, y_max=50,
+                         step_size=4.0):
+        self.f["pd_adjust_positions"](self.h, type, int(bool(forward)), x_min, x_max, y_min,
+                                      y_max, step_size)
+
+    def get_final_x_position(self, n):
+        return self.f["pd_get_x"](self.h, n)
+
+    def get_final_y_position(self, n):
+        return self.f["pd_get_y"](self.h, n)
+
+
+def OraclePD(**kw):
+    return _PhaseDiverse(oracle_lib(), **kw)
+
+
+def ReferencePD(variant="64", **kw):
+    return _PhaseDiverse(reference_lib(variant), **kw)

@@ -19,6 +19,7 @@
 #include <FresnelCDI_WF.h>
 #include <PolyCDI.h>
 #include <TransmissionConstraint.h>
+#include <PhaseDiverseCDI.h>
 #include <vector>
 
 namespace {
@@ -316,5 +317,84 @@ void ref_get_intensity_autocorrelation(void *h, double *a)
 }
 
 int ref_precision_bytes(void) { return (int)sizeof(((Double_2D *)0)->get(0, 0)); }
+
+/* ---- PhaseDiverseCDI (NADIA/include/PhaseDiverseCDI.h) over RefSolver frames */
+
+void *ref_pd_create(double beta, double gamma, int parallel, int granularity)
+{
+    return new PhaseDiverseCDI(beta, gamma, parallel != 0, granularity);
+}
+
+void ref_pd_destroy(void *pd) { delete static_cast<PhaseDiverseCDI *>(pd); }
+
+void ref_pd_add_position(void *pd, void *frame, double x, double y, double alpha)
+{
+    static_cast<PhaseDiverseCDI *>(pd)->add_new_position(S(frame)->cdi, x, y, alpha);
+}
+
+void ref_pd_remove_positions(void *pd) { static_cast<PhaseDiverseCDI *>(pd)->remove_positions(); }
+
+void ref_pd_initialise_estimate(void *pd)
+{
+    static_cast<PhaseDiverseCDI *>(pd)->initialise_estimate();
+}
+
+void ref_pd_iterate(void *pd) { static_cast<PhaseDiverseCDI *>(pd)->iterate(); }
+
+void ref_pd_set_iterations_per_cycle(void *pd, int n)
+{
+    static_cast<PhaseDiverseCDI *>(pd)->set_iterations_per_cycle(n);
+}
+
+void ref_pd_set_feedback_parameter(void *pd, double b)
+{
+    static_cast<PhaseDiverseCDI *>(pd)->set_feedback_parameter(b);
+}
+
+void ref_pd_set_amplification_factor(void *pd, double g)
+{
+    static_cast<PhaseDiverseCDI *>(pd)->set_amplification_factor(g);
+}
+
+void ref_pd_set_probe_scaling(void *pd, int n, double alpha)
+{
+    static_cast<PhaseDiverseCDI *>(pd)->set_probe_scaling(n, alpha);
+}
+
+void ref_pd_get_size(void *pd, int *nx, int *ny)
+{
+    Complex_2D *o = static_cast<PhaseDiverseCDI *>(pd)->get_transmission();
+    *nx = o ? o->get_size_x() : 0;
+    *ny = o ? o->get_size_y() : 0;
+}
+
+void ref_pd_get_transmission(void *pd, double *a)
+{
+    from_cplx(*static_cast<PhaseDiverseCDI *>(pd)->get_transmission(), a);
+}
+
+void ref_pd_set_transmission(void *pd, int nx, int ny, const double *a)
+{
+    Complex_2D t(nx, ny);
+    to_cplx(t, a);
+    static_cast<PhaseDiverseCDI *>(pd)->set_transmission(t);
+}
+
+void ref_pd_adjust_positions(void *pd, int type, int forward, int min_x, int max_x, int min_y,
+                             int max_y, double step_size)
+{
+    static_cast<PhaseDiverseCDI *>(pd)->adjust_positions(type, forward != 0, min_x, max_x, min_y,
+                                                         max_y, step_size);
+}
+
+double ref_pd_get_x(void *pd, int n)
+{
+    return static_cast<PhaseDiverseCDI *>(pd)->get_final_x_position(n);
+}
+
+double ref_pd_get_y(void *pd, int n)
+{
+    return static_cast<PhaseDiverseCDI *>(pd)->get_final_y_position(n);
+}
 
 } // extern "C"

@@ -1,7 +1,8 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-The reference's own hot-path sources (NADIA/src/{Complex_2D,BaseCDI,PlanarCDI,
-FresnelCDI,FresnelCDI_WF,PolyCDI}.c++), compiled unmodified in their double build against
+The reference's own sources (NADIA/src/{Complex_2D,BaseCDI,PlanarCDI,
+FresnelCDI,FresnelCDI_WF,PolyCDI,TransmissionConstraint,PhaseDiverseCDI}.c++,
+utils.c), compiled unmodified in their double build against
 the FFTW shim by oracle/build_oracle.py, run the scenarios of tests/scenarios.py
 on the synthetic inputs of pynadia.synth.  Each fixture stores the outputs
 and a digest of the inputs it was made from.
@@ -30,6 +31,12 @@ CASES = {
     "fresnel_mixed_32": (sc.fresnel_mixed, dict(n=32)),
     "poly_mixed_32": (sc.poly_mixed, dict(n=32, padding=2)),
     "fresnel_wf_mixed_32": (sc.fresnel_wf_mixed, dict(n=32)),
+    "phase_diverse_series_32": (sc.phase_diverse_mixed, dict(n=32)),
+    "phase_diverse_parallel_g2_32": (sc.phase_diverse_mixed,
+                                     dict(n=32, parallel=True, granularity=2, beta=0.8,
+                                          gamma=1.5, alphas=[1.0, 0.6, 1.4])),
+    "phase_diverse_align_32": (sc.phase_diverse_mixed, dict(n=32, adjust="cc")),
+    "phase_diverse_minerr_32": (sc.phase_diverse_mixed, dict(n=32, adjust="me", forward=False)),
 }
 
 
@@ -37,7 +44,10 @@ def input_digest(name):
     kw = CASES[name][1]
     n = kw.get("n", 32)
     h = hashlib.sha256()
-    if name.startswith("planar"):
+    if name.startswith("phase_diverse"):
+        c = sc.phase_diverse_inputs(n)
+        arrs = c.intensities + c.white_fields + [c.support, np.array(c.positions)]
+    elif name.startswith("planar"):
         c = sc.planar_inputs(n, ny=kw.get("ny"), beam_stop=0 if "custom" in name else 4)
         arrs = [c.intensity, c.support]
     elif name.startswith("fresnel_wf"):

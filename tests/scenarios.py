@@ -244,3 +244,57 @@ def fresnel_constrained(make, n=32, seed=2, iterations=12, hio_from=4):
         errs.append(s.get_error())
     return {"errors": np.array(errs), "esw": s.get_exit_surface_wave(),
             "transmission": s.get_transmission()}
+
+
+def phase_diverse_inputs(n, positions=((0, 0), (5, -3), (-4, 6)), seed=11):
+    return synth.PhaseDiverseCase(n, positions=positions, seed=seed)
+
+
+def phase_diverse_frames(make, c, offsets=None, constraint=False):
+    """FresnelCDI frames of a PhaseDiverseCase, each initialised with its own
+    seed; `offsets` perturbs the positions handed to add_new_position."""
+    frames = []
+    for k in range(len(c.positions)):
+        s = make("fresnel", c.n, c.n, white_field=c.white_fields[k], wavelength=c.wavelength,
+                 focal_detector_length=c.zfd, focal_sample_length=c.zfs[k], pixel_size=c.pixel,
+                 normalisation=1.0)
+        s.set_support(c.support)
+        s.set_intensity(c.intensities[k])
+        s.initialise_estimate(k + 1)
+        if constraint:
+            s.set_transmission_constraint(True, True)
+        frames.append(s)
+    return frames
+
+
+def phase_diverse_mixed(make, make_pd=None, n=32, parallel=False, granularity=1, cycles=3,
+                        per_cycle=2, beta=1.0, gamma=1.0, alphas=None, adjust=None,
+                        offsets=((0, 0), (1, -2), (2, 1)), constraint=False, forward=True):
+    """PhaseDiverseCDI over three Fresnel frames: optional position search
+    (adjust = 'cc' CROSS_CORRELATION or 'me' MINIMUM_ERROR, from positions
+    off by `offsets`), then `cycles` iterations in series or parallel mode."""
+    c = phase_diverse_inputs(n)
+    frames = phase_diverse_frames(make, c, constraint=constraint)
+    if make_pd is None:  # the CPU libraries: PhaseDiverseCDI of the frames' own library
+        import pyoracle
+        make_pd = lambda **k: pyoracle._PhaseDiverse(frames[0].L, **k)  # noqa: E731
+    pd = make_pd(beta=beta, gamma=gamma, parallel=parallel, granularity=granularity)
+    for k, f in enumerate(frames):
+        x, y = c.positions[k]
+        dx, dy = offsets[k] if adjust else (0, 0)
+        pd.add_new_position(f, x + dx, y + dy, alphas[k] if alphas else 1.0)
+    pd.set_iterations_per_cycle(per_cycle)
+    pd.initialise_estimate()
+    out = {"init": pd.get_transmission()}
+    if adjust == "cc":
+        pd.adjust_positions(0, forward, -6, 6, -6, 6)
+    elif adjust == "me":
+        pd.adjust_positions(1, forward, -6, 6, -6, 6, 2.0)
+    for _ in range(cycles):
+        pd.iterate()
+    out["object"] = pd.get_transmission()
+    out["positions"] = np.array([[pd.get_final_x_position(k), pd.get_final_y_position(k)]
+                                 for k in range(len(frames))])
+    out["frames"] = np.array([f.get_exit_surface_wave() for f in frames])
+    out["errors"] = np.array([f.get_error() for f in frames])
+    return out

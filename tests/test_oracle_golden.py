@@ -28,7 +28,9 @@ def oracle_factory(kind, nx, ny, **kw):
 
 
 @pytest.mark.parametrize("name", ["planar_mixed_32", "planar_mixed_32x48", "planar_custom_32",
-                                  "fresnel_mixed_32", "poly_mixed_32", "fresnel_wf_mixed_32"])
+                                  "fresnel_mixed_32", "poly_mixed_32", "fresnel_wf_mixed_32",
+                                  "phase_diverse_series_32", "phase_diverse_parallel_g2_32",
+                                  "phase_diverse_align_32", "phase_diverse_minerr_32"])
 def test_oracle_matches_golden(name):
     g, fn, kw = load_golden(name)
     res = fn(oracle_factory, **kw)

@@ -58,6 +58,41 @@ def test_fresnel_wf(n):
     same(sc.fresnel_wf_mixed(orc, n=n), sc.fresnel_wf_mixed(ref, n=n))
 
 
+@pytest.mark.parametrize("kw", [dict(), dict(parallel=True), dict(granularity=2),
+                                dict(parallel=True, granularity=3),
+                                dict(parallel=True, beta=0.7, gamma=2.0, alphas=[1.0, 0.5, 2.0]),
+                                dict(constraint=True), dict(adjust="cc"), dict(adjust="me"),
+                                dict(adjust="cc", forward=False), dict(adjust="me", granularity=2),
+                                dict(n=40, adjust="cc", granularity=2, parallel=True)],
+                         ids=lambda kw: "-".join("%s=%s" % i for i in kw.items()) or "series")
+def test_phase_diverse(kw):
+    kw = dict(kw)
+    n = kw.pop("n", 32)
+    same(sc.phase_diverse_mixed(orc, n=n, **kw), sc.phase_diverse_mixed(ref, n=n, **kw))
+
+
+def test_phase_diverse_remove_positions():
+    """remove_positions forgets the frames only: frames added afterwards
+    reuse the earlier positions, scalings and results by index."""
+    out = []
+    for make in (orc, ref):
+        c = sc.phase_diverse_inputs(32)
+        frames = sc.phase_diverse_frames(make, c)
+        import pyoracle
+        pd = pyoracle._PhaseDiverse(frames[0].L, beta=0.9)
+        for k, f in enumerate(frames[:2]):
+            pd.add_new_position(f, *c.positions[k])
+        pd.initialise_estimate()
+        pd.iterate()
+        pd.remove_positions()
+        pd.add_new_position(frames[2], *c.positions[2])
+        pd.iterate()
+        out.append((pd.get_transmission(), pd.get_final_x_position(2), frames[2].get_exit_surface_wave()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
+
+
 @pytest.mark.parametrize("n,padding", [(48, 3), (64, 4)])
 def test_poly(n, padding):
     same(sc.poly_mixed(orc, n=n, padding=padding), sc.poly_mixed(ref, n=n, padding=padding))
