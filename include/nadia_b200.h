@@ -410,6 +410,66 @@ int nadia_tuned_tiles(int nx, int ny, int fresnel, int batched, char *buf, int l
 int nadia_shrinkwrap_noalloc_f32(const float *esw_dev, float *support_dev, int nx, int ny,
                                  double gauss_width, double threshold, void *stream);
 
+/* ---- PhaseDiverseCDI (phase-diverse / ptychographic reconstruction) -------- */
+
+/* PhaseDiverseCDI (NADIA/include/PhaseDiverseCDI.h, NADIA/src/PhaseDiverseCDI.c++):
+ * reconstructions ("frames", FP64 handles: Fresnel frames exchange their
+ * transmission function, others their exit-surface wave) placed at (x, y) on
+ * one global object.  Series mode updates the object after each frame;
+ * parallel mode iterates every frame (concurrently on the GPU) and then
+ * blends them all.  granularity > 1 places frames with sub-pixel resolution
+ * (bilinear).  A frame handle can not be destroyed while it belongs to one of
+ * these objects.  Arrays are as elsewhere: element (x, y) at x*ny + y,
+ * complex interleaved. */
+typedef struct nadia_phase_diverse nadia_phase_diverse;
+
+/* PhaseDiverseCDI(beta, gamma, parallel, granularity) -- PhaseDiverseCDI.c++:17-33 */
+int nadia_pd_create(double beta, double gamma, int parallel, int granularity,
+                    nadia_phase_diverse **out);
+int nadia_pd_destroy(nadia_phase_diverse *pd);
+
+/* add_new_position(local, x, y, alpha) -- PhaseDiverseCDI.c++:104-160; grows
+ * the object to cover the frame */
+int nadia_pd_add_position(nadia_phase_diverse *pd, nadia_solver *frame, double x, double y,
+                          double alpha);
+
+/* remove_positions -- PhaseDiverseCDI.c++:60-66: forgets the frames only;
+ * frames added afterwards take over the earlier positions by index */
+int nadia_pd_remove_positions(nadia_phase_diverse *pd);
+
+/* initialise_estimate -- PhaseDiverseCDI.c++:163-177: object = 1, then every
+ * frame's current result blended in */
+int nadia_pd_initialise_estimate(nadia_phase_diverse *pd);
+
+/* `cycles` calls of iterate -- PhaseDiverseCDI.c++:180-230 */
+int nadia_pd_iterate(nadia_phase_diverse *pd, int cycles);
+
+/* set_iterations_per_cycle / set_feedback_parameter / set_amplification_factor
+ * / set_probe_scaling -- PhaseDiverseCDI.h:190-226 (NADIA_ERR_RANGE when the
+ * probe number is not that of an added position) */
+int nadia_pd_set_iterations_per_cycle(nadia_phase_diverse *pd, int iterations);
+int nadia_pd_set_feedback_parameter(nadia_phase_diverse *pd, double beta);
+int nadia_pd_set_amplification_factor(nadia_phase_diverse *pd, double gamma);
+int nadia_pd_set_probe_scaling(nadia_phase_diverse *pd, int n_probe, double alpha);
+
+/* the object's size (0 x 0 before the first position) */
+int nadia_pd_get_size(const nadia_phase_diverse *pd, int *nx, int *ny);
+
+/* get_transmission / set_transmission -- PhaseDiverseCDI.c++:77-101
+ * (set: NADIA_ERR_INVALID when the size differs from the current object's) */
+int nadia_pd_get_transmission(nadia_phase_diverse *pd, double *out);
+int nadia_pd_set_transmission(nadia_phase_diverse *pd, int nx, int ny, const double *t);
+
+/* adjust_positions(type, forwards, x_min, x_max, y_min, y_max, step_size) --
+ * PhaseDiverseCDI.c++:232-392: type 0 = CROSS_CORRELATION (image alignment,
+ * NADIA/src/utils.c:1151-1300), 1 = MINIMUM_ERROR (search of the frame error,
+ * PhaseDiverseCDI.c++:395-447) */
+int nadia_pd_adjust_positions(nadia_phase_diverse *pd, int type, int forward, int min_x,
+                              int max_x, int min_y, int max_y, double step_size);
+
+/* get_final_x_position / get_final_y_position -- PhaseDiverseCDI.h:255-262 */
+int nadia_pd_get_position(const nadia_phase_diverse *pd, int n_probe, double *x, double *y);
+
 #ifdef __cplusplus
 }
 #endif

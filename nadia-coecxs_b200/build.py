@@ -24,6 +24,7 @@ COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "
                  "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 PER_FILE = {
     "plain64.cu": ["--fmad=false"],
+    "phase_diverse.cu": ["--fmad=false"],
 }
 
 

@@ -9,6 +9,7 @@
 #include "batch.h"
 #include "fused32.h"
 #include "fused32_impl.h"
+#include "phase_diverse.h"
 #include "server.h"
 #include "solver.h"
 
@@ -17,6 +18,10 @@ using nadia::Solver;
 
 struct nadia_solver {
     Solver *s;
+};
+
+struct nadia_phase_diverse {
+    nadia::PhaseDiverse *p;
 };
 
 namespace {
@@ -163,6 +168,9 @@ int nadia_destroy(nadia_solver *h)
     return guard([&] {
         if (!h) return;
         if (h->s) {
+            NADIA_REQUIRE(h->s->pd_refs == 0, NADIA_ERR_STATE,
+                          "the reconstruction is a frame of a phase-diverse reconstruction; "
+                          "destroy that (or remove its positions) first");
             cudaSetDevice(h->s->device);
             delete h->s;
         }
@@ -436,6 +444,151 @@ int nadia_fft2d(double *a, int nx, int ny, int forward)
 int nadia_synchronize(nadia_solver *h)
 {
     return guard([&] { S(h).sync(); });
+}
+
+/* ---- PhaseDiverseCDI ------------------------------------------------------- */
+
+namespace {
+nadia::PhaseDiverse &P(nadia_phase_diverse *h)
+{
+    if (!h || !h->p) throw Error(NADIA_ERR_INVALID, "null phase-diverse handle");
+    NADIA_CUDA(cudaSetDevice(h->p->device));
+    nadia::t_alloc_stream = h->p->st;
+    return *h->p;
+}
+} // namespace
+
+int nadia_pd_create(double beta, double gamma, int parallel, int granularity,
+                    nadia_phase_diverse **out)
+{
+    return guard([&] {
+        need(out, "out");
+        *out = nullptr;
+        nadia_phase_diverse *h = new nadia_phase_diverse{nullptr};
+        try {
+            h->p = new nadia::PhaseDiverse(beta, gamma, parallel != 0, granularity);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int nadia_pd_destroy(nadia_phase_diverse *h)
+{
+    return guard([&] {
+        if (!h) return;
+        if (h->p) {
+            cudaSetDevice(h->p->device);
+            delete h->p;
+        }
+        delete h;
+    });
+}
+
+int nadia_pd_add_position(nadia_phase_diverse *h, nadia_solver *frame, double x, double y,
+                          double alpha)
+{
+    return guard([&] {
+        nadia::PhaseDiverse &p = P(h);
+        if (!frame || !frame->s) throw Error(NADIA_ERR_INVALID, "null frame handle");
+        p.add_position(frame->s, x, y, alpha);
+    });
+}
+
+int nadia_pd_remove_positions(nadia_phase_diverse *h)
+{
+    return guard([&] { P(h).remove_positions(); });
+}
+
+int nadia_pd_initialise_estimate(nadia_phase_diverse *h)
+{
+    return guard([&] { P(h).initialise_estimate(); });
+}
+
+int nadia_pd_iterate(nadia_phase_diverse *h, int cycles)
+{
+    return guard([&] {
+        NADIA_REQUIRE(cycles >= 0, NADIA_ERR_INVALID, "negative cycle count");
+        nadia::PhaseDiverse &p = P(h);
+        for (int c = 0; c < cycles; ++c) p.iterate();
+    });
+}
+
+int nadia_pd_set_iterations_per_cycle(nadia_phase_diverse *h, int iterations)
+{
+    return guard([&] {
+        NADIA_REQUIRE(iterations >= 0, NADIA_ERR_INVALID, "negative iteration count");
+        P(h).iterations_per_cycle = iterations;
+    });
+}
+
+int nadia_pd_set_feedback_parameter(nadia_phase_diverse *h, double beta)
+{
+    return guard([&] { P(h).set_feedback_parameter(beta); });
+}
+
+int nadia_pd_set_amplification_factor(nadia_phase_diverse *h, double gamma)
+{
+    return guard([&] { P(h).set_amplification_factor(gamma); });
+}
+
+int nadia_pd_set_probe_scaling(nadia_phase_diverse *h, int n_probe, double alpha)
+{
+    return guard([&] {
+        NADIA_REQUIRE(P(h).set_probe_scaling(n_probe, alpha), NADIA_ERR_RANGE,
+                      "the probe number given is too large (set the scaling after "
+                      "add_new_position)");
+    });
+}
+
+int nadia_pd_get_size(const nadia_phase_diverse *h, int *nx, int *ny)
+{
+    return guard([&] {
+        if (!h || !h->p) throw Error(NADIA_ERR_INVALID, "null phase-diverse handle");
+        need(nx, "nx");
+        need(ny, "ny");
+        *nx = h->p->obj ? h->p->nx : 0;
+        *ny = h->p->obj ? h->p->ny : 0;
+    });
+}
+
+int nadia_pd_get_transmission(nadia_phase_diverse *h, double *out)
+{
+    return guard([&] {
+        need(out, "out");
+        P(h).get_transmission(out);
+    });
+}
+
+int nadia_pd_set_transmission(nadia_phase_diverse *h, int nx, int ny, const double *t)
+{
+    return guard([&] {
+        need(t, "t");
+        P(h).set_transmission(nx, ny, t);
+    });
+}
+
+int nadia_pd_adjust_positions(nadia_phase_diverse *h, int type, int forward, int min_x,
+                              int max_x, int min_y, int max_y, double step_size)
+{
+    return guard([&] {
+        P(h).adjust_positions(type, forward != 0, min_x, max_x, min_y, max_y, step_size);
+    });
+}
+
+int nadia_pd_get_position(const nadia_phase_diverse *h, int n_probe, double *x, double *y)
+{
+    return guard([&] {
+        if (!h || !h->p) throw Error(NADIA_ERR_INVALID, "null phase-diverse handle");
+        need(x, "x");
+        need(y, "y");
+        NADIA_REQUIRE(n_probe >= 0 && n_probe < (int)h->p->xpos.size(), NADIA_ERR_RANGE,
+                      "no such position");
+        *x = h->p->xpos[n_probe];
+        *y = h->p->ypos[n_probe];
+    });
 }
 
 } // extern "C"

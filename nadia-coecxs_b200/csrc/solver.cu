@@ -684,6 +684,30 @@ void Solver::get_transmission(double *h)
     }
 }
 
+void Solver::transmission_to_device(double2 *dst)
+{
+    AllocScope scope(st);
+    NADIA_REQUIRE(prec == NADIA_FP64, NADIA_ERR_UNSUPPORTED,
+                  "phase-diverse frames run in the FP64 form");
+    if (kind == NADIA_FRESNEL) {
+        plain::fresnel_get_transmission(x.p, illum_sample.p, dst, n, st);
+        if (tc.active) apply_transmission_constraint(dst); // FresnelCDI.c++:352-353
+    } else {
+        NADIA_CUDA(cudaMemcpyAsync(dst, x.p, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    }
+}
+
+void Solver::transmission_from_device(const double2 *src)
+{
+    AllocScope scope(st);
+    NADIA_REQUIRE(prec == NADIA_FP64, NADIA_ERR_UNSUPPORTED,
+                  "phase-diverse frames run in the FP64 form");
+    if (kind == NADIA_FRESNEL)
+        plain::fresnel_set_transmission(src, illum_sample.p, x.p, nx, ny, st);
+    else
+        NADIA_CUDA(cudaMemcpyAsync(x.p, src, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+}
+
 void Solver::get_illumination_at_sample(double *h)
 {
     AllocScope scope(st);

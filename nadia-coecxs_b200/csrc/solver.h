@@ -22,6 +22,7 @@ struct Solver {
     size_t n = 0;
     int device = 0;
     unsigned long long uid = 0; // unique per handle (batch plans key on it)
+    int pd_refs = 0;            // phase-diverse reconstructions holding this one as a frame
     OwnedStream own_st;         // outlives every buffer below
     cudaStream_t st = nullptr;
 
@@ -144,6 +145,14 @@ struct Solver {
     void plain_convolve(double *arr, double gauss_width, int cut);
     void plain_apply_support(double2 *c);
     void apply_transmission_constraint(double2 *t);
+
+    // The result a PhaseDiverseCDI exchanges with this reconstruction
+    // (PhaseDiverseCDI.c++:330-345), device to device and ordered on st:
+    // FresnelCDI's transmission function (get_transmission_function with its
+    // constraint, set_transmission_function), else the exit-surface wave.
+    // FP64 form only.
+    void transmission_to_device(double2 *dst);
+    void transmission_from_device(const double2 *src);
     void ensure_temps();
     void update_n_best();
     void record_error();

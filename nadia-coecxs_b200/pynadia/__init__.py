@@ -131,6 +131,21 @@ _PROTOS = {
                                          ctypes.POINTER(ctypes.c_ulonglong)]),
     "nadia_device_bytes": (_LL, []),
     "nadia_tuned_tiles": (_I, [_I, _I, _I, _I, ctypes.c_char_p, _I]),
+    "nadia_pd_create": (_I, [ctypes.c_double, ctypes.c_double, _I, _I, ctypes.POINTER(_H)]),
+    "nadia_pd_destroy": (_I, [_H]),
+    "nadia_pd_add_position": (_I, [_H, _H, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+    "nadia_pd_remove_positions": (_I, [_H]),
+    "nadia_pd_initialise_estimate": (_I, [_H]),
+    "nadia_pd_iterate": (_I, [_H, _I]),
+    "nadia_pd_set_iterations_per_cycle": (_I, [_H, _I]),
+    "nadia_pd_set_feedback_parameter": (_I, [_H, ctypes.c_double]),
+    "nadia_pd_set_amplification_factor": (_I, [_H, ctypes.c_double]),
+    "nadia_pd_set_probe_scaling": (_I, [_H, _I, ctypes.c_double]),
+    "nadia_pd_get_size": (_I, [_H, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "nadia_pd_get_transmission": (_I, [_H, _D]),
+    "nadia_pd_set_transmission": (_I, [_H, _I, _I, _D]),
+    "nadia_pd_adjust_positions": (_I, [_H, _I, _I, _I, _I, _I, _I, ctypes.c_double]),
+    "nadia_pd_get_position": (_I, [_H, _I, _D, _D]),
 }
 
 _LIB = None
@@ -419,6 +434,84 @@ class Solver:
         p = ctypes.c_void_p()
         _check(self.lib.nadia_get_stream(self.h, ctypes.byref(p)))
         return p.value or 0
+
+
+class PhaseDiverse:
+    """PhaseDiverseCDI (NADIA/include/PhaseDiverseCDI.h) on the GPU over FP64
+    Solver frames: the reference's method names and defaults."""
+
+    CROSS_CORRELATION, MINIMUM_ERROR = 0, 1
+
+    def __init__(self, beta=1.0, gamma=1.0, parallel=False, granularity=1):
+        self.lib = load()
+        h = _H()
+        _check(self.lib.nadia_pd_create(beta, gamma, int(bool(parallel)), granularity,
+                                        ctypes.byref(h)))
+        self.h = h
+        self.frames = []  # the frames must outlive this object
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nadia_pd_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def add_new_position(self, frame, x=0.0, y=0.0, alpha=1.0):
+        _check(self.lib.nadia_pd_add_position(self.h, frame.h, x, y, alpha))
+        self.frames.append(frame)
+
+    def remove_positions(self):
+        _check(self.lib.nadia_pd_remove_positions(self.h))
+
+    def initialise_estimate(self):
+        _check(self.lib.nadia_pd_initialise_estimate(self.h))
+
+    def iterate(self, cycles=1):
+        _check(self.lib.nadia_pd_iterate(self.h, cycles))
+
+    def set_iterations_per_cycle(self, n):
+        _check(self.lib.nadia_pd_set_iterations_per_cycle(self.h, n))
+
+    def set_feedback_parameter(self, beta):
+        _check(self.lib.nadia_pd_set_feedback_parameter(self.h, beta))
+
+    def set_amplification_factor(self, gamma):
+        _check(self.lib.nadia_pd_set_amplification_factor(self.h, gamma))
+
+    def set_probe_scaling(self, n, alpha):
+        _check(self.lib.nadia_pd_set_probe_scaling(self.h, n, alpha))
+
+    def size(self):
+        nx, ny = _I(), _I()
+        _check(self.lib.nadia_pd_get_size(self.h, ctypes.byref(nx), ctypes.byref(ny)))
+        return nx.value, ny.value
+
+    def get_transmission(self):
+        nx, ny = self.size()
+        out = np.empty((nx, ny), dtype=np.complex128)
+        _check(self.lib.nadia_pd_get_transmission(self.h, _ptr(out)))
+        return out
+
+    def set_transmission(self, t):
+        t = np.ascontiguousarray(t, dtype=np.complex128)
+        _check(self.lib.nadia_pd_set_transmission(self.h, t.shape[0], t.shape[1], _ptr(t)))
+
+    def adjust_positions(self, type=0, forward=True, x_min=-50, x_max=50, y_min=-50, y_max=50,
+                         step_size=4.0):
+        _check(self.lib.nadia_pd_adjust_positions(self.h, type, int(bool(forward)), x_min, x_max,
+                                                  y_min, y_max, step_size))
+
+    def _position(self, n):
+        x, y = ctypes.c_double(), ctypes.c_double()
+        _check(self.lib.nadia_pd_get_position(self.h, n, ctypes.byref(x), ctypes.byref(y)))
+        return x.value, y.value
+
+    def get_final_x_position(self, n):
+        return self._position(n)[0]
+
+    def get_final_y_position(self, n):
+        return self._position(n)[1]
 
 
 def iterate_many(solvers, iterations):

@@ -1286,7 +1286,12 @@ static void pd_add_to_object(orc_pd *p, int n)
                         const double vi = f00[1] * (x1) * (y1) + f10[1] * x * (y1) + f01[1] * (x1) * y + f11[1] * x * y;
                         const int ni = (int)((i_ + 0.5 - xo - p->x_min) * sc + di);
                         const int nj = (int)((j_ + 0.5 - yo - p->y_min) * sc + dj);
-                        double *t = o + 2 * ((size_t)ni * p->ny + nj);
+                        /* the reference's flat index ni*ny + nj: a column past
+                         * either edge lands in the neighbouring row; outside
+                         * the whole array it writes out of bounds (skipped) */
+                        const long long f = (long long)ni * p->ny + nj;
+                        if (f < 0 || f >= (long long)p->nx * p->ny) continue;
+                        double *t = o + 2 * f;
                         double nr = wt * vr + t[0];
                         double nim = wt * vi + t[1];
                         if (!p->parallel) {
@@ -1330,8 +1335,11 @@ static void pd_update_from_object(orc_pd *p, int n)
                 double re = 0, im = 0;
                 for (int di = 0; di < sc; ++di)
                     for (int dj = 0; dj < sc; ++dj) {
-                        re += o[2 * ((size_t)(i + di) * p->ny + j + dj)];
-                        im += o[2 * ((size_t)(i + di) * p->ny + j + dj) + 1];
+                        /* flat index, as the reference reads (past the array: skipped) */
+                        const long long f = (long long)(i + di) * p->ny + j + dj;
+                        if (f >= (long long)p->nx * p->ny) continue;
+                        re += o[2 * f];
+                        im += o[2 * f + 1];
                     }
                 const double norm = 1 / ((double)(sc * sc));
                 s[0] = re * norm;
