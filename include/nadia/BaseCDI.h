@@ -15,8 +15,10 @@
 //     print_algorithm are virtual, so FresnelCDI_WF's versions (a warning:
 //     its algorithm is fixed) answer calls through a BaseCDI pointer too;
 //   - a TransmissionConstraint given to set_complex_constraint runs in the
-//     FP64 form only, and is read when iterate() or apply_support() next runs
-//     (changes to it after that are picked up at the following call).
+//     FP64 form (the reconstruction moves to it there), and is read when
+//     iterate() or apply_support() next runs (changes to it after that are
+//     picked up at the following call); the same holds for a reconstruction
+//     added to a PhaseDiverseCDI.
 #ifndef NADIA_DROPIN_BASECDI_H
 #define NADIA_DROPIN_BASECDI_H
 
@@ -49,9 +51,11 @@ public:
         }
     }
 
-    // BaseCDI::set_complex_constraint (BaseCDI.h:471-473)
+    // BaseCDI::set_complex_constraint (BaseCDI.h:471-473); constraints run in
+    // the FP64 form, to which an FP32 reconstruction moves here
     virtual void set_complex_constraint(TransmissionConstraint &trans_constraint)
     {
+        nadia_cxx::check(nadia_convert_to_fp64(h));
         transmission_constraint = &trans_constraint;
         trans_constraint.push_to(h, nx, ny, true);
     }
@@ -200,6 +204,15 @@ public:
     nadia_solver *handle() { return h; }
 
 protected:
+    friend class PhaseDiverseCDI;
+
+    // hand pending host-side changes (edited estimate, constraint) to the GPU
+    void prepare_device()
+    {
+        if (transmission_constraint) transmission_constraint->push_to(h, nx, ny);
+        complex.push();
+    }
+
     BaseCDI(Complex_2D &c, int n_best_)
         : complex(c), nx(c.get_size_x()), ny(c.get_size_y()), n_best(n_best_), support(nx, ny)
     {

@@ -136,6 +136,16 @@ int nadia_poly_set_spectrum_file(nadia_solver *s, const char *path);
  * the number in the file.  Needs no GPU. */
 int nadia_read_spec(const char *path, double *rows, int capacity, int *nrows);
 
+/* Moves an FP32 reconstruction to the FP64 form in place (no-op on FP64):
+ * estimate, support, intensity, beam stop, Fresnel illumination and geometry,
+ * spectrum, algorithm, error history and n-best results carry over, FP32
+ * values widened.  Needed before a transmission constraint or a
+ * phase-diverse position (both FP64 only) on an FP32 handle. */
+int nadia_convert_to_fp64(nadia_solver *s);
+
+/* NADIA_FP32 or NADIA_FP64. */
+int nadia_get_precision(const nadia_solver *s, int *precision);
+
 /* The padding PolyCDI derived from its spectrum (PolyCDI.c++:86-87). */
 int nadia_poly_get_padding(const nadia_solver *s, int *px, int *py);
 

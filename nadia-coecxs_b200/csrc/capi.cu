@@ -233,6 +233,20 @@ int nadia_read_spec(const char *path, double *rows, int capacity, int *nrows)
     });
 }
 
+int nadia_convert_to_fp64(nadia_solver *h)
+{
+    return guard([&] { S(h).convert_to_fp64(); });
+}
+
+int nadia_get_precision(const nadia_solver *h, int *precision)
+{
+    return guard([&] {
+        if (!h || !h->s) throw Error(NADIA_ERR_INVALID, "null handle");
+        need(precision, "precision");
+        *precision = h->s->prec;
+    });
+}
+
 int nadia_poly_get_padding(const nadia_solver *h, int *px, int *py)
 {
     return guard([&] {

@@ -228,6 +228,7 @@ void Solver::set_beam_stop(const double *mask)
 {
     AllocScope scope(st);
     has_beam_stop = true;
+    h_beam_stop.assign(mask, mask + n);
     if (prec == NADIA_FP64) {
         if (!beam_stop) beam_stop.alloc(n);
         h2d(beam_stop.p, mask, n * sizeof(double), st);
@@ -706,6 +707,64 @@ void Solver::transmission_from_device(const double2 *src)
         plain::fresnel_set_transmission(src, illum_sample.p, x.p, nx, ny, st);
     else
         NADIA_CUDA(cudaMemcpyAsync(x.p, src, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+}
+
+void Solver::convert_to_fp64()
+{
+    AllocScope scope(st);
+    if (prec == NADIA_FP64) return;
+    // read the FP32 state back
+    std::vector<double> xh(2 * n), sup(n);
+    f32->get_x(xh.data());
+    get_support(sup.data());
+    std::vector<std::vector<double>> best(n_best);
+    for (int i = 0; i < n_best; ++i) {
+        std::vector<float> f(2 * n);
+        d2h(f.data(), best32[i].p, n * sizeof(float2), st);
+        best[i].assign(f.begin(), f.end());
+    }
+    forget_batches_with(uid); // batch plans hold FP32 handles only
+    NADIA_CUDA(cudaStreamSynchronize(st));
+    f32.reset();
+    best32.clear();
+    prec = NADIA_FP64;
+    // the FP64 buffers, as the constructor makes them
+    x.alloc(n);
+    support.alloc(n);
+    isqrt.alloc(n);
+    recon.alloc(n);
+    tmp.alloc(n);
+    fft.init(nx, ny);
+    gauss_width_ = -1;
+    gauss_cut_ = -1;
+    h2d(x.p, xh.data(), n * sizeof(double2), st);
+    h_support = sup;
+    h_support_valid = true;
+    h2d(support.p, h_support.data(), n * sizeof(double), st);
+    h2d(isqrt.p, h_isqrt.data(), n * sizeof(double), st);
+    if (has_beam_stop) {
+        beam_stop.alloc(n);
+        h2d(beam_stop.p, h_beam_stop.data(), n * sizeof(double), st);
+    }
+    for (int i = 0; i < n_best; ++i) {
+        best64.emplace_back(n);
+        h2d(best64.back().p, best[i].data(), n * sizeof(double2), st);
+    }
+    if (kind == NADIA_FRESNEL) {
+        illum.alloc(n);
+        illum_sample.alloc(n);
+        coef.alloc((size_t)(nx / 2) * (ny / 2));
+        h2d(illum.p, h_illum.data(), illum.bytes(), st);
+        fresnel_set_experimental_parameters(wavelength, zfd, zfs, pixel);
+    }
+    if (kind == NADIA_POLY && has_spectrum) {
+        d_spec.alloc(2 * (size_t)nlambda);
+        h2d(d_spec.p, spectrum.data(), d_spec.bytes(), st);
+        padded.alloc((size_t)(nx + 2 * px) * (ny + 2 * py));
+        isc.alloc(n);
+        fft_pad.init(nx + 2 * px, ny + 2 * py);
+    }
+    NADIA_CUDA(cudaStreamSynchronize(st));
 }
 
 void Solver::get_illumination_at_sample(double *h)

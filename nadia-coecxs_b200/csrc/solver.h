@@ -36,6 +36,7 @@ struct Solver {
     std::vector<double> h_support;
     bool h_support_valid = true;
     bool has_beam_stop = false;
+    std::vector<double> h_beam_stop; // the mask as given (kept for convert_to_fp64)
 
     // error history: one slot per iteration on the device
     static constexpr int kRing = 65536;
@@ -153,6 +154,12 @@ struct Solver {
     // FP64 form only.
     void transmission_to_device(double2 *dst);
     void transmission_from_device(const double2 *src);
+
+    // Moves an FP32 reconstruction to the FP64 form in place: the estimate,
+    // support, intensity, beam stop, illumination and geometry, spectrum,
+    // algorithm, error history and n-best results carry over (FP32 values
+    // widened); later iterations run the plain FP64 path.  No-op on FP64.
+    void convert_to_fp64();
     void ensure_temps();
     void update_n_best();
     void record_error();

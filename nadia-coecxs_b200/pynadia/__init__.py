@@ -131,6 +131,8 @@ _PROTOS = {
                                          ctypes.POINTER(ctypes.c_ulonglong)]),
     "nadia_device_bytes": (_LL, []),
     "nadia_tuned_tiles": (_I, [_I, _I, _I, _I, ctypes.c_char_p, _I]),
+    "nadia_convert_to_fp64": (_I, [_H]),
+    "nadia_get_precision": (_I, [_H, ctypes.POINTER(_I)]),
     "nadia_pd_create": (_I, [ctypes.c_double, ctypes.c_double, _I, _I, ctypes.POINTER(_H)]),
     "nadia_pd_destroy": (_I, [_H]),
     "nadia_pd_add_position": (_I, [_H, _H, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
@@ -235,6 +237,16 @@ class Solver:
         if getattr(self, "h", None):
             self.lib.nadia_destroy(self.h)
             self.h = None
+
+    def convert_to_fp64(self):
+        """Move an FP32 reconstruction to the FP64 form in place."""
+        _check(self.lib.nadia_convert_to_fp64(self.h))
+        self.precision = FP64
+
+    def get_precision(self):
+        p = _I()
+        _check(self.lib.nadia_get_precision(self.h, ctypes.byref(p)))
+        return p.value
 
     __del__ = close
 

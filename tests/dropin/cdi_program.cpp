@@ -6,7 +6,7 @@
 // estimate read back every 10 iterations), reading inputs from and writing
 // results to raw little-endian float64 files in a directory.
 //
-//   cdi_program <planar|fresnel|poly|example|wf> <nx> <ny> <dir> [padding]
+//   cdi_program <planar|fresnel|poly|example|wf|tc|pd> <nx> <ny> <dir> [padding]
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -18,6 +18,7 @@
 #include <Double_2D.h>
 #include <FresnelCDI.h>
 #include <FresnelCDI_WF.h>
+#include <PhaseDiverseCDI.h>
 #include <PlanarCDI.h>
 #include <PolyCDI.h>
 
@@ -247,6 +248,46 @@ static int white_field(int nx, int ny)
     return 0;
 }
 
+// PhaseDiverseCDI over three FresnelCDI frames (tests/scenarios.py
+// phase_diverse_mixed with adjust="cc"): params.bin holds wavelength,
+// focus-to-detector, pixel, then per frame focus-to-sample, x, y, dx, dy
+static int phase_diverse(int nx, int ny)
+{
+    const int frames = 3;
+    std::vector<double> p = load("params.bin", 3 + 5 * frames);
+    Double_2D support = real_2d("support.bin", nx, ny);
+    std::vector<Complex_2D *> esw;
+    std::vector<FresnelCDI *> proj;
+    PhaseDiverseCDI pd(1.0, 1.0, false, 1);
+    for (int k = 0; k < frames; ++k) {
+        esw.push_back(new Complex_2D(nx, ny));
+        Complex_2D wf(nx, ny);
+        complex_2d("white_field" + std::to_string(k) + ".bin", wf);
+        const double *f = &p[3 + 5 * k];
+        proj.push_back(new FresnelCDI(*esw.back(), wf, p[0], p[1], f[0], p[2], 1.0));
+        proj.back()->set_support(support);
+        proj.back()->set_intensity(real_2d("intensity" + std::to_string(k) + ".bin", nx, ny));
+        proj.back()->initialise_estimate(k + 1);
+    }
+    for (int k = 0; k < frames; ++k) {
+        const double *f = &p[3 + 5 * k];
+        pd.add_new_position(proj[k], f[1] + f[3], f[2] + f[4]);
+    }
+    pd.set_iterations_per_cycle(2);
+    pd.initialise_estimate();
+    pd.adjust_positions(PhaseDiverseCDI::CROSS_CORRELATION, true, -6, 6, -6, 6);
+    for (int c = 0; c < 3; ++c) pd.iterate();
+    save_complex("object.bin", *pd.get_transmission());
+    std::vector<double> pos;
+    for (int k = 0; k < frames; ++k) {
+        pos.push_back(pd.get_final_x_position(k));
+        pos.push_back(pd.get_final_y_position(k));
+        save_complex("frame" + std::to_string(k) + ".bin", *esw[k]);
+    }
+    save("positions.bin", pos);
+    return 0;
+}
+
 // the flow of the reference's PlanarCDI example, two short cycles
 static int example(int nx, int ny)
 {
@@ -312,6 +353,7 @@ int main(int argc, char **argv)
         if (mode == "example") return example(nx, ny);
         if (mode == "wf") return white_field(nx, ny);
         if (mode == "tc") return constrained(nx, ny);
+        if (mode == "pd") return phase_diverse(nx, ny);
     } catch (const nadia_cxx::Failure &e) {
         std::cerr << "failure " << e.code << ": " << e.what() << std::endl;
         return 4;

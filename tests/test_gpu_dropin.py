@@ -265,3 +265,44 @@ def test_planar_fp32_form(programs, tmp_path):
     sup = get(tmp_path, "support_out.bin", (n, n))
     assert np.array_equal(sup, f32(same["support"]))
     assert sup.min() >= 0 and sup.max() <= 1.0
+
+
+def _phase_diverse_inputs(d, n):
+    c = sc.phase_diverse_inputs(n)
+    offsets = ((0, 0), (1, -2), (2, 1))
+    put(d, "support.bin", c.support)
+    params = [c.wavelength, c.zfd, c.pixel]
+    for k in range(3):
+        put(d, "white_field%d.bin" % k, c.white_fields[k])
+        put(d, "intensity%d.bin" % k, c.intensities[k])
+        params += [c.zfs[k], c.positions[k][0], c.positions[k][1], offsets[k][0], offsets[k][1]]
+    put(d, "params.bin", params)
+
+
+def test_phase_diverse_double_build(programs, tmp_path):
+    """PhaseDiverseCDI (three FresnelCDI frames, cross-correlation position
+    search, series iterations) from a caller of the reference's classes:
+    double build bit-identical to the oracle."""
+    n = 32
+    _phase_diverse_inputs(tmp_path, n)
+    run(programs[True], "pd", n, n, tmp_path)
+    ref = sc.phase_diverse_mixed(po.Oracle, n=n, adjust="cc")
+    obj = ref["object"]
+    assert np.array_equal(get(tmp_path, "object.bin", obj.shape, cplx=True), obj)
+    assert np.array_equal(get(tmp_path, "positions.bin", (3, 2)), ref["positions"])
+    for k in range(3):
+        assert np.array_equal(get(tmp_path, "frame%d.bin" % k, (n, n), cplx=True), ref["frames"][k])
+
+
+def test_phase_diverse_float_build_moves_frames_to_fp64(programs, tmp_path):
+    """Float build at 256^2: the frames start in the FP32 form (their
+    initial estimates are made there) and move to the FP64 form when added;
+    the run completes and its position search lands within a pixel of the
+    double build's."""
+    n = 256
+    _phase_diverse_inputs(tmp_path, n)
+    run(programs[False], "pd", n, n, tmp_path)
+    ref = sc.phase_diverse_mixed(oracle_factory(False), n=n, adjust="cc")
+    got = get(tmp_path, "object.bin", ref["object"].shape, cplx=True)
+    assert np.isfinite(got).all()
+    assert np.max(np.abs(get(tmp_path, "positions.bin", (3, 2)) - ref["positions"])) <= 1
