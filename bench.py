@@ -60,6 +60,8 @@ def parse():
     p.add_argument("--fresnel-only", action="store_true",
                    help="print the FresnelCDI batch report only")
     p.add_argument("--no-wf", action="store_true", help="skip the FresnelCDI_WF report")
+    p.add_argument("--no-pd", action="store_true", help="skip the PhaseDiverseCDI report")
+    p.add_argument("--pd-only", action="store_true", help="print the PhaseDiverseCDI report only")
     p.add_argument("--wf-only", action="store_true", help="print the FresnelCDI_WF report only")
     p.add_argument("--quick-poly", action="store_true",
                    help="device-resident FP32 PolyCDI steps only (1024^2 padded to 1080^2; "
@@ -431,6 +433,87 @@ def white_field_report(pynadia, synth, n=2048, iters=26):
     return out
 
 
+def phase_diverse_report(pynadia, synth, n=1024, cycles=15):
+    """PhaseDiverseCDI modelled on the reference's example
+    (NADIA/examples/PhaseDiverse_example.c): seven FresnelCDI frames of
+    1024^2 at the example's positions, wavelength, pixel size and distances,
+    each with the default transmission constraint (unit magnitude, charge
+    flipping), series mode, cross-correlation position search before cycle 0
+    and minimum-error search before cycle 10, 15 cycles.  Frames run in the
+    FP64 form (PhaseDiverseCDI's form).  The calls are synchronous, so the
+    times are host wall times around them.  The reference's float build is
+    timed for one cycle on one host core."""
+    import numpy as np
+    fz = 16.353e-3
+    fd = [0.909513, 0.909388, 0.909263, 0.909213, 0.909088, 0.909088, 0.909088]
+    fs = [18.513e-3, 18.388e-3, 18.263e-3, 18.213e-3, 18.088e-3, 18.088e-3, 18.088e-3]
+    pos = list(zip([0, 23, 3, 35, 30, 37, 60], [-150, -145, -134, -123, -150, -93, 210]))
+    c = synth.PhaseDiverseCase(n, positions=pos, seed=31, wavelength=4.892e-10,
+                               zfd=[d - fz for d in fd], zfs=[z - fz for z in fs], pixel=13.5e-6)
+
+    def frames_on(make):
+        out = []
+        for k in range(len(pos)):
+            f = make("fresnel", n, n, white_field=c.white_fields[k], wavelength=c.wavelength,
+                     focal_detector_length=c.zfds[k], focal_sample_length=c.zfs[k],
+                     pixel_size=c.pixel, normalisation=1.0)
+            f.set_support(c.support)
+            f.set_intensity(c.intensities[k])
+            f.initialise_estimate(0)
+            f.set_transmission_constraint(True, True)
+            out.append(f)
+        return out
+
+    def gpu_make(kind, nx, ny, **kw):
+        return pynadia.Solver(kind, nx, ny, precision=pynadia.FP64, **kw)
+
+    def run(frames, pd, search=True, n_cycles=cycles):
+        for k, f in enumerate(frames):
+            pd.add_new_position(f, *pos[k])
+        pd.initialise_estimate()
+        for i in range(n_cycles):
+            if search and i == 0:
+                pd.adjust_positions(0)
+            if search and i == 10:
+                pd.adjust_positions(1)
+            pd.iterate()
+
+    # warm-up: one short run (kernels, plans, pools)
+    frames = frames_on(gpu_make)
+    run(frames, pynadia.PhaseDiverse(), search=False, n_cycles=1)
+    frames = frames_on(gpu_make)
+    pd = pynadia.PhaseDiverse()
+    t = time.perf_counter()
+    run(frames, pd)
+    whole = time.perf_counter() - t
+    found = [(pd.get_final_x_position(k), pd.get_final_y_position(k)) for k in range(len(pos))]
+    t = time.perf_counter()
+    pd.iterate(5)
+    per_cycle = (time.perf_counter() - t) / 5
+    obj = pd.get_transmission()
+    out = {"frames": len(pos), "grid": [n, n], "object": list(obj.shape), "cycles": cycles,
+           "gpu_fp64_s_per_reconstruction": whole, "gpu_fp64_ms_per_cycle": 1000.0 * per_cycle,
+           "positions_found": found, "object_finite": bool(np.isfinite(obj).all())}
+    pd.close()
+    for f in frames:
+        f.close()
+    sys.path.insert(0, ORACLE)
+    import pyoracle as po
+    if po.reference_available("32_fast"):
+        rmake = lambda kind, nx, ny, **kw: po.Reference(kind, nx, ny, variant="32_fast", **kw)  # noqa: E731
+        rframes = frames_on(rmake)
+        rpd = po.ReferencePD("32_fast")
+        for k, f in enumerate(rframes):
+            rpd.add_new_position(f, *pos[k])
+        rpd.initialise_estimate()
+        t = time.perf_counter()
+        rpd.iterate()
+        cpu = time.perf_counter() - t
+        out["cpu_reference_float_s_per_cycle_one_core"] = cpu
+        out["gpu_over_cpu_per_cycle"] = cpu / per_cycle
+    return out
+
+
 def quick_poly(pynadia, synth, args):
     """`args.batch` FP32 PolyCDI reconstructions of 1024^2 padded to 1080^2
     (10-line spectrum, 5% FWHM), HIO, stepped together; per-pass device times."""
@@ -480,6 +563,8 @@ def ours(args, rank, world, local_rank):
         return quick_poly(pynadia, synth, args)
     if args.wf_only:
         return {"white_field": white_field_report(pynadia, synth)}
+    if args.pd_only:
+        return {"phase_diverse": phase_diverse_report(pynadia, synth)}
     if args.fresnel_only:
         return {"fresnel_batch": fresnel_batch_report(pynadia, synth, n_items=args.fresnel_batch)}
     dist = None
@@ -656,6 +741,7 @@ def ours(args, rank, world, local_rank):
             fresnel_batch = fresnel_batch_report(pynadia, synth, n_items=args.fresnel_batch)
 
         white_field = white_field_report(pynadia, synth) if not args.no_wf else None
+        phase_diverse = phase_diverse_report(pynadia, synth) if not args.no_pd else None
 
         serving = None
         if args.serve_requests > 0:
@@ -684,6 +770,7 @@ def ours(args, rank, world, local_rank):
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": launches, "fp64_plain": fp64, "accuracy": accuracy,
             "serving": serving, "fresnel_batch": fresnel_batch, "white_field": white_field,
+            "phase_diverse": phase_diverse,
         }
     if dist:
         dist.barrier()

@@ -445,6 +445,7 @@ void PhaseDiverse::add_position(Solver *f, double x, double y, double a)
     NADIA_CUDA(cudaMemsetAsync(result.back().p, 0, result.back().bytes(), st));
     weight.emplace_back((size_t)lnx * lny);
     NADIA_CUDA(cudaMemsetAsync(weight.back().p, 0, weight.back().bytes(), st));
+    base.emplace_back();
     if (!obj) {
         x_min = (int)(-x);
         y_min = (int)(-y);
@@ -474,14 +475,24 @@ void PhaseDiverse::remove_positions()
     frames.clear();
 }
 
-// set_up_weights, PhaseDiverseCDI.c++:450-530, on the host in the
-// reference's order, then uploaded
+// set_up_weights, PhaseDiverseCDI.c++:450-530: each weight's
+// alpha * pow(|illumination| / max, gamma) (0 outside the support) on the
+// host in the reference's order, recomputed only when its inputs change;
+// series mode multiplies it by beta on the device, parallel mode
+// normalises over the frames on the host
+__global__ void k_times(const double *a, double f, double *out, size_t n)
+{
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x)
+        out[k] = a[k] * f;
+}
+
 void PhaseDiverse::set_up_weights()
 {
     if (weights_set) return;
     weights_set = true;
+    AllocScope scope(st);
     const int frames_n = (int)frames.size();
-    std::vector<std::vector<double>> w(frames_n);
     for (int n = 0; n < frames_n; ++n) {
         Solver *f = frames[n];
         const int lnx = rnx[n], lny = rny[n];
@@ -490,6 +501,10 @@ void PhaseDiverse::set_up_weights()
         NADIA_REQUIRE(f->nx == lnx && f->ny == lny, NADIA_ERR_UNSUPPORTED,
                       "a frame added after remove_positions differs in size from the "
                       "position it takes over");
+        Base &b = base[n];
+        if (b.frame == f && b.version == f->weights_version && b.gamma == gamma &&
+            b.alpha == alpha[n])
+            continue;
         std::vector<double> support(f->n), mag;
         f->get_support(support.data());
         double max = 0;
@@ -503,39 +518,52 @@ void PhaseDiverse::set_up_weights()
             for (double v : mag)
                 if (v > max) max = v;
         }
-        w[n].resize((size_t)lnx * lny);
+        b.h.resize((size_t)lnx * lny);
         for (int i = 0; i < lnx; ++i)
             for (int j = 0; j < lny; ++j) {
                 double value = f->kind == NADIA_FRESNEL ? mag[(size_t)i * lny + j] / max : 1;
                 value = alpha[n] * std::pow(value, gamma);
                 if (support[(size_t)i * f->ny + j] <= 0.0) value = 0;
-                if (!parallel) value *= beta;
-                w[n][(size_t)i * lny + j] = value;
+                b.h[(size_t)i * lny + j] = value;
             }
+        if (b.d.n != b.h.size()) b.d.alloc(b.h.size());
+        h2d_sync(b.d.p, b.h.data(), b.h.size() * sizeof(double), st);
+        b.frame = f;
+        b.version = f->weights_version;
+        b.gamma = gamma;
+        b.alpha = alpha[n];
     }
-    if (parallel) {
-        std::vector<double> norm((size_t)nx * ny, 0.0);
-        for (int n = 0; n < frames_n; ++n)
-            for (int i_ = 0; i_ < rnx[n]; ++i_)
-                for (int j_ = 0; j_ < rny[n]; ++j_) {
-                    const int i = (int)(i_ - xpos[n] - x_min), j = (int)(j_ - ypos[n] - y_min);
-                    if (i >= 0 && j >= 0 && i < nx && j < ny) {
-                        const double v = w[n][(size_t)i_ * rny[n] + j_];
-                        double &t = norm[(size_t)i * ny + j];
-                        t = n == 0 ? v : v + t;
-                    }
-                }
-        for (int n = 0; n < frames_n; ++n)
-            for (int i_ = 0; i_ < rnx[n]; ++i_)
-                for (int j_ = 0; j_ < rny[n]; ++j_) {
-                    const int i = (int)(i_ - xpos[n] - x_min), j = (int)(j_ - ypos[n] - y_min);
-                    if (i >= 0 && j >= 0 && i < nx && j < ny) {
-                        double &v = w[n][(size_t)i_ * rny[n] + j_];
-                        const double nn = norm[(size_t)i * ny + j];
-                        v = nn <= 0 ? 0 : beta * v / nn;
-                    }
-                }
+    if (!parallel) {
+        for (int n = 0; n < frames_n; ++n) {
+            const size_t m = (size_t)rnx[n] * rny[n];
+            k_times<<<grid_for(m), kThreads, 0, st>>>(base[n].d.p, beta, weight[n].p, m);
+        }
+        NADIA_CUDA(cudaGetLastError());
+        return;
     }
+    std::vector<std::vector<double>> w(frames_n);
+    for (int n = 0; n < frames_n; ++n) w[n] = base[n].h;
+    std::vector<double> norm((size_t)nx * ny, 0.0);
+    for (int n = 0; n < frames_n; ++n)
+        for (int i_ = 0; i_ < rnx[n]; ++i_)
+            for (int j_ = 0; j_ < rny[n]; ++j_) {
+                const int i = (int)(i_ - xpos[n] - x_min), j = (int)(j_ - ypos[n] - y_min);
+                if (i >= 0 && j >= 0 && i < nx && j < ny) {
+                    const double v = w[n][(size_t)i_ * rny[n] + j_];
+                    double &t = norm[(size_t)i * ny + j];
+                    t = n == 0 ? v : v + t;
+                }
+            }
+    for (int n = 0; n < frames_n; ++n)
+        for (int i_ = 0; i_ < rnx[n]; ++i_)
+            for (int j_ = 0; j_ < rny[n]; ++j_) {
+                const int i = (int)(i_ - xpos[n] - x_min), j = (int)(j_ - ypos[n] - y_min);
+                if (i >= 0 && j >= 0 && i < nx && j < ny) {
+                    double &v = w[n][(size_t)i_ * rny[n] + j_];
+                    const double nn = norm[(size_t)i * ny + j];
+                    v = nn <= 0 ? 0 : beta * v / nn;
+                }
+            }
     for (int n = 0; n < frames_n; ++n)
         h2d_sync(weight[n].p, w[n].data(), w[n].size() * sizeof(double), st);
 }

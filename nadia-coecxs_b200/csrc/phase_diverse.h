@@ -42,6 +42,16 @@ struct PhaseDiverse {
     std::vector<int> rnx, rny;
     std::vector<DevBuf<double2>> result; // single_result
     std::vector<DevBuf<double>> weight;  // weights
+    // alpha * (|illumination| / max)^gamma, 0 outside the support: the part
+    // of each weight that needs the host's pow, kept until its inputs change
+    struct Base {
+        const Solver *frame = nullptr;
+        unsigned long long version = ~0ull;
+        double gamma = 0, alpha = 0;
+        std::vector<double> h;
+        DevBuf<double> d;
+    };
+    std::vector<Base> base;
 
     // the current object: the owned global one, or a temporary during the
     // position search (adjust_positions swaps it as the reference does)

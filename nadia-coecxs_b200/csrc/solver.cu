@@ -198,6 +198,7 @@ void Solver::upload_support()
 void Solver::set_support(const double *obj, bool soften)
 {
     AllocScope scope(st);
+    ++weights_version;
     double max = host_max(obj, n);
     for (size_t k = 0; k < n; ++k) h_support[k] = obj[k] / max;
     h_support_valid = true;
@@ -309,6 +310,7 @@ void Solver::fresnel_set_experimental_parameters(double wl, double zfd_, double 
                                                  double pixel_)
 {
     AllocScope scope(st);
+    ++weights_version;
     wavelength = wl;
     pixel = pixel_;
     zfd = zfd_;
@@ -460,6 +462,7 @@ void Solver::fresnel_wf_init(double wl, double zone_focal, double focal_detector
 // both axes) set to 1 over the current support, then convolve(support, 3, 5)
 void Solver::fresnel_wf_set_support(double z_diameter, double size)
 {
+    ++weights_version;
     AllocScope scope(st);
     NADIA_REQUIRE(kind == NADIA_FRESNEL_WF, NADIA_ERR_INVALID, "needs a FresnelCDI_WF handle");
     if (!h_support_valid) get_support(h_support.data());
@@ -482,6 +485,7 @@ void Solver::fresnel_set_norm(double nn)
 {
     AllocScope scope(st);
     NADIA_REQUIRE(kind == NADIA_FRESNEL, NADIA_ERR_INVALID, "set_norm needs a FresnelCDI handle");
+    ++weights_version;
     double old = norm;
     norm = nn;
     double f = nn / old;
@@ -713,6 +717,7 @@ void Solver::convert_to_fp64()
 {
     AllocScope scope(st);
     if (prec == NADIA_FP64) return;
+    ++weights_version;
     // read the FP32 state back
     std::vector<double> xh(2 * n), sup(n);
     f32->get_x(xh.data());
@@ -995,6 +1000,7 @@ void Solver::get_error_history(double *out, int count)
 void Solver::apply_shrinkwrap(double gauss_width, double thresh)
 {
     AllocScope scope(st);
+    ++weights_version;
     if (prec == NADIA_FP32) {
         f32->shrinkwrap(gauss_width, thresh);
         h_support_valid = false;

@@ -23,6 +23,9 @@ struct Solver {
     int device = 0;
     unsigned long long uid = 0; // unique per handle (batch plans key on it)
     int pd_refs = 0;            // phase-diverse reconstructions holding this one as a frame
+    // bumped whenever the support or the Fresnel illumination changes (the
+    // inputs of a phase-diverse object's weights)
+    unsigned long long weights_version = 0;
     OwnedStream own_st;         // outlives every buffer below
     cudaStream_t st = nullptr;
 

@@ -184,11 +184,16 @@ class PhaseDiverseCase:
     different focus-to-sample distance per frame (the phase diversity)."""
 
     def __init__(self, n, positions=((0, 0), (5, -3), (-4, 6)), seed=11, energy_kev=8.0,
-                 zfd=1.0, zfs=(1.0e-3, 0.97e-3, 1.04e-3), pixel=13.5e-6, photons=None):
+                 zfd=1.0, zfs=(1.0e-3, 0.97e-3, 1.04e-3), pixel=13.5e-6, photons=None,
+                 wavelength=None):
         self.n = n
         self.positions = [tuple(float(v) for v in p) for p in positions]
-        self.wavelength = FresnelCase.HC_KEV_M / energy_kev
-        self.zfd, self.pixel = zfd, pixel
+        self.wavelength = wavelength or FresnelCase.HC_KEV_M / energy_kev
+        self.pixel = pixel
+        # one focus-to-detector distance for all frames (zfd), or one per frame
+        zl = list(zfd) if hasattr(zfd, "__len__") else [zfd]
+        self.zfd = zl[0]
+        self.zfds = [zl[k % len(zl)] for k in range(len(positions))]
         self.zfs = [zfs[k % len(zfs)] for k in range(len(positions))]
         xmin = int(-self.positions[0][0])
         ymin = int(-self.positions[0][1])
@@ -210,7 +215,7 @@ class PhaseDiverseCase:
         self.white_fields, self.intensities, self.windows = [], [], []
         for k, (sx, sy) in enumerate(starts):
             wf = wamp * np.exp(1j * alpha * r2 * (1 + 0.1 * k)) * 100.0
-            coef = fresnel_factor(n, n, self.wavelength, zfd, self.zfs[k], pixel)
+            coef = fresnel_factor(n, n, self.wavelength, self.zfds[k], self.zfs[k], pixel)
             illum = fresnel_from_detector(wf, coef)
             T = self.object[sx - lo_x:sx - lo_x + n, sy - lo_y:sy - lo_y + n]
             esw = (T - 1) * illum

@@ -49,9 +49,9 @@ def ppm_writer(tmp_path_factory):
     return write
 
 
-def run_tool(exe, case, seed, timeout=600):
+def run_tool(exe, case, seed, timeout=600, env=None):
     r = subprocess.run([exe, os.path.basename(case.config), case.kind, str(seed)], cwd=case.dir,
-                       capture_output=True, text=True, timeout=timeout)
+                       capture_output=True, text=True, timeout=timeout, env=env)
     assert r.returncode == 0, r.stdout + r.stderr
     return r.stdout
 

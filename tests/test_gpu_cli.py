@@ -49,15 +49,19 @@ def test_double_build_iteration_by_iteration(tmp_path, tools, ppm_writer):
 
 @pytest.mark.parametrize("build,n", [("double", 64), ("float", 256)])
 def test_restart_from_checkpoint(tmp_path, tools, build, n):
+    """The three runs are separate processes: the FP32 form's tile choice is
+    pinned (NADIA_TUNE=0) so that all three run the same kernels -- a timed
+    choice may differ between processes, and with it the rounding."""
+    env = dict(os.environ, NADIA_TUNE="0")
     whole = cc.CliCase("planar", n, tmp_path, stages=[("HIO", 40)], shrinkwrap_iterations=0,
                        prefix="whole", output_iterations=100)
-    run_tool(tools[build], whole, seed=2)
+    run_tool(tools[build], whole, seed=2, env=env)
     first = cc.CliCase("planar", n, tmp_path, stages=[("HIO", 20)], shrinkwrap_iterations=0,
                        prefix="first", output_iterations=100)
-    run_tool(tools[build], first, seed=2)
+    run_tool(tools[build], first, seed=2, env=env)
     rest = cc.CliCase("planar", n, tmp_path, stages=[("HIO", 20)], shrinkwrap_iterations=0,
                       prefix="rest", output_iterations=100, starting_point="first.cplx")
-    run_tool(tools[build], rest, seed=99)  # the seed is unused after a restart
+    run_tool(tools[build], rest, seed=99, env=env)  # the seed is unused after a restart
     a = cc.read_cplx(whole.path("whole.cplx"), n, n)
     b = cc.read_cplx(rest.path("rest.cplx"), n, n)
     assert np.array_equal(a, b)
