@@ -686,62 +686,30 @@ bool Fused32::Impl::push_slot_async(cudaStream_t st)
 }
 
 // Host arrays are in the reference's order (element (x, y) at x*ny + y); the
-// device arrays in the panel layout.  The conversion runs on the GPU through
-// a staging buffer, so the host only converts doubles to floats in order.
-namespace {
-template <int ST>
-__global__ void k_natural_to_panel(const float *__restrict__ src, float *__restrict__ dst, int nx,
-                                   int ny, int fold)
+// device arrays in the panel layout.  The host converts, so uploads and
+// readbacks are plain copies: they run on the copy engines and never wait
+// for SMs held by other reconstructions' passes.
+void Fused32::Impl::put_panel_f(const float *h, int stride, void *dst, bool fold)
 {
-    const size_t n = (size_t)nx * ny;
-    for (size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x; a < n;
-         a += (size_t)gridDim.x * blockDim.x) {
-        const size_t t = a / kPanel;
-        const int kx = (int)(t % nx), ky = (int)(t / nx) * kPanel + (int)(a % kPanel);
-        int dx = kx, dy = ky;
+    std::vector<float> p(n * stride);
+    for (int ky = 0; ky < ny; ++ky) {
+        int dy = ky;
         if (fold) {
-            dx = kx + nx / 2;
-            dx = dx >= nx ? dx - nx : dx;
             dy = ky + ny / 2;
             dy = dy >= ny ? dy - ny : dy;
         }
-        const size_t d = (size_t)dx * ny + dy;
-#pragma unroll
-        for (int c = 0; c < ST; ++c) dst[a * ST + c] = src[d * ST + c];
+        for (int kx = 0; kx < nx; ++kx) {
+            int dx = kx;
+            if (fold) {
+                dx = kx + nx / 2;
+                dx = dx >= nx ? dx - nx : dx;
+            }
+            const size_t a = panel_index_dev(kx, ky, nx), d = (size_t)dx * ny + dy;
+            for (int c = 0; c < stride; ++c) p[a * stride + c] = h[d * stride + c];
+        }
     }
-}
-
-template <int ST>
-__global__ void k_panel_to_natural(const float *__restrict__ src, float *__restrict__ dst, int nx,
-                                   int ny)
-{
-    const size_t n = (size_t)nx * ny;
-    for (size_t d = blockIdx.x * (size_t)blockDim.x + threadIdx.x; d < n;
-         d += (size_t)gridDim.x * blockDim.x) {
-        const int xx = (int)(d / ny), yy = (int)(d % ny);
-        const size_t a = panel_index_dev(xx, yy, nx);
-#pragma unroll
-        for (int c = 0; c < ST; ++c) dst[d * ST + c] = src[a * ST + c];
-    }
-}
-} // namespace
-
-void Fused32::Impl::ensure_stage()
-{
-    if (!stage) stage.alloc(n);
-}
-
-void Fused32::Impl::put_panel_f(const float *h, int stride, void *dst, bool fold)
-{
-    ensure_stage();
-    NADIA_CUDA(cudaMemcpyAsync(stage.p, h, n * stride * sizeof(float), cudaMemcpyHostToDevice,
+    NADIA_CUDA(cudaMemcpyAsync(dst, p.data(), n * stride * sizeof(float), cudaMemcpyHostToDevice,
                                S.st));
-    const float *src = reinterpret_cast<const float *>(stage.p);
-    if (stride == 1)
-        k_natural_to_panel<1><<<grid1(n), 256, 0, S.st>>>(src, (float *)dst, nx, ny, fold);
-    else
-        k_natural_to_panel<2><<<grid1(n), 256, 0, S.st>>>(src, (float *)dst, nx, ny, fold);
-    g_launches += 1;
     NADIA_CUDA(cudaStreamSynchronize(S.st));
 }
 
@@ -754,15 +722,15 @@ void Fused32::Impl::put_panel(const double *h, int stride, void *dst, bool fold)
 
 void Fused32::Impl::get_panel_f(const void *src, int stride, float *h)
 {
-    ensure_stage();
-    float *d = reinterpret_cast<float *>(stage.p);
-    if (stride == 1)
-        k_panel_to_natural<1><<<grid1(n), 256, 0, S.st>>>((const float *)src, d, nx, ny);
-    else
-        k_panel_to_natural<2><<<grid1(n), 256, 0, S.st>>>((const float *)src, d, nx, ny);
-    g_launches += 1;
-    NADIA_CUDA(cudaMemcpyAsync(h, d, n * stride * sizeof(float), cudaMemcpyDeviceToHost, S.st));
+    std::vector<float> p(n * stride);
+    NADIA_CUDA(cudaMemcpyAsync(p.data(), src, n * stride * sizeof(float), cudaMemcpyDeviceToHost,
+                               S.st));
     NADIA_CUDA(cudaStreamSynchronize(S.st));
+    for (int xx = 0; xx < nx; ++xx)
+        for (int yy = 0; yy < ny; ++yy) {
+            const size_t a = panel_index_dev(xx, yy, nx), d = (size_t)xx * ny + yy;
+            for (int c = 0; c < stride; ++c) h[d * stride + c] = p[a * stride + c];
+        }
 }
 
 void Fused32::Impl::get_panel(const void *src, int stride, double *h)

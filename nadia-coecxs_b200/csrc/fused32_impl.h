@@ -132,7 +132,7 @@ struct Fused32::Impl {
     Solver &S;
     int nx = 0, ny = 0, ncol = 0;
     size_t n = 0;
-    DevBuf<float2> P, x, W, ill, tx, ty, stage;
+    DevBuf<float2> P, x, W, ill, tx, ty;
     DevBuf<float> sup, mI, tmp1, tmp2, maxpart;
     DevBuf<double> partials;
     DevBuf<long long> iter;
@@ -162,8 +162,7 @@ struct Fused32::Impl {
     void use_choice(const f32::Choice *c);
     // host arrays in the reference's order <-> device arrays in the panel
     // layout (stride 1: real, 2: complex; fold: PlanarCDI's centred detector
-    // to transform order), converted on the device through `stage`
-    void ensure_stage();
+    // to transform order), converted on the host: plain copies on the device
     void put_panel(const double *h, int stride, void *dst, bool fold);
     void put_panel_f(const float *h, int stride, void *dst, bool fold);
     void get_panel(const void *src, int stride, double *h);
