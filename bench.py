@@ -433,6 +433,29 @@ def white_field_report(pynadia, synth, n=2048, iters=26):
     return out
 
 
+class quiet_stdout:
+    """Sends file descriptor 1 to /dev/null for the duration: the reference's
+    classes print progress there, and the bench prints one JSON line."""
+
+    def __enter__(self):
+        import ctypes
+        self.libc = ctypes.CDLL(None)
+        sys.stdout.flush()
+        self.libc.fflush(None)
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        self.libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+        return False
+
+
 def phase_diverse_report(pynadia, synth, n=1024, cycles=15):
     """PhaseDiverseCDI modelled on the reference's example
     (NADIA/examples/PhaseDiverse_example.c): seven FresnelCDI frames of
@@ -501,14 +524,15 @@ def phase_diverse_report(pynadia, synth, n=1024, cycles=15):
     import pyoracle as po
     if po.reference_available("32_fast"):
         rmake = lambda kind, nx, ny, **kw: po.Reference(kind, nx, ny, variant="32_fast", **kw)  # noqa: E731
-        rframes = frames_on(rmake)
-        rpd = po.ReferencePD("32_fast")
-        for k, f in enumerate(rframes):
-            rpd.add_new_position(f, *pos[k])
-        rpd.initialise_estimate()
-        t = time.perf_counter()
-        rpd.iterate()
-        cpu = time.perf_counter() - t
+        with quiet_stdout():
+            rframes = frames_on(rmake)
+            rpd = po.ReferencePD("32_fast")
+            for k, f in enumerate(rframes):
+                rpd.add_new_position(f, *pos[k])
+            rpd.initialise_estimate()
+            t = time.perf_counter()
+            rpd.iterate()
+            cpu = time.perf_counter() - t
         out["cpu_reference_float_s_per_cycle_one_core"] = cpu
         out["gpu_over_cpu_per_cycle"] = cpu / per_cycle
     return out
