@@ -62,6 +62,11 @@ def parse():
     p.add_argument("--no-wf", action="store_true", help="skip the FresnelCDI_WF report")
     p.add_argument("--no-pd", action="store_true", help="skip the PhaseDiverseCDI report")
     p.add_argument("--pd-only", action="store_true", help="print the PhaseDiverseCDI report only")
+    p.add_argument("--no-tc", action="store_true", help="skip the TransmissionConstraint report")
+    p.add_argument("--tc-only", action="store_true",
+                   help="print the TransmissionConstraint report only")
+    p.add_argument("--tc-profile", action="store_true",
+                   help="three iterations with the region constraint only (for ncu)")
     p.add_argument("--wf-only", action="store_true", help="print the FresnelCDI_WF report only")
     p.add_argument("--quick-poly", action="store_true",
                    help="device-resident FP32 PolyCDI steps only (1024^2 padded to 1080^2; "
@@ -433,6 +438,75 @@ def white_field_report(pynadia, synth, n=2048, iters=26):
     return out
 
 
+def constraint_report(pynadia, synth, n=2048, iters=50, modes=("none", "pixel", "regions"),
+                      cpu=True):
+    """TransmissionConstraint (charge flipping, unit magnitude, and three
+    complex-constraint regions) on a PlanarCDI HIO reconstruction of 2048^2 in
+    the FP64 form: device time per iteration without the constraint, with the
+    per-pixel part, and with regions (CUDA events on the handle's stream).
+    The constraint runs once per support projection, i.e. twice per HIO
+    iteration.  Algorithmic bytes per pixel and application: per-pixel part
+    read + write of the field (32); with regions also the region map on both
+    kernels and the field once more for the region sums (16 + 4 + 4 = 24 more).
+    The reference's float build is timed for one iteration of each on one
+    host core."""
+    import torch
+    c = synth.PlanarCase(n, n // 6, 2, 1e9, seed=41, support_side=int(0.42 * n), beam_stop=0)
+    regions, alphas, fixed = synth.constraint_regions(n)
+
+    def setup(s, mode):
+        s.set_support(c.support)
+        s.set_intensity(c.intensity)
+        s.initialise_estimate(1)
+        s.set_algorithm(3)  # HIO
+        if mode == "pixel":
+            s.set_transmission_constraint(True, True, -1)
+        elif mode == "regions":
+            s.set_transmission_constraint(True, True, -1, regions, alphas, fixed)
+
+    out = {"grid": [n, n], "iterations": iters}
+    ms = {}
+    for mode in modes:
+        s = pynadia.Solver("planar", n, n, precision=pynadia.FP64)
+        setup(s, mode)
+        s.iterate(3)
+        s.synchronize()
+        st = torch.cuda.ExternalStream(s.stream())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s.iterate(iters)
+        b.record(st)
+        b.synchronize()
+        ms[mode] = a.elapsed_time(b) / iters
+        s.close()
+    peak, _ = measured_peak()
+    px = n * n
+    out["gpu_fp64_ms_per_iteration"] = ms
+    for mode, bpp in (("pixel", 32.0), ("regions", 56.0)):
+        if mode not in ms or "none" not in ms:
+            continue
+        extra = (ms[mode] - ms["none"]) / 2 / 1000.0  # seconds per application
+        if extra > 0:
+            gbs = bpp * px / extra / 1e9
+            out[mode + "_constraint"] = {"us_per_application": extra * 1e6,
+                                         "algorithmic_bytes_per_pixel": bpp,
+                                         "hbm_gbs_algorithmic": gbs, "roofline_frac": gbs / peak}
+    sys.path.insert(0, ORACLE)
+    import pyoracle as po
+    if cpu and po.reference_available("32_fast"):
+        cpu = {}
+        with quiet_stdout():
+            for mode in ("none", "pixel", "regions"):
+                r = po.Reference("planar", n, n, variant="32_fast")
+                setup(r, mode)
+                t = time.perf_counter()
+                r.iterate()
+                cpu[mode] = time.perf_counter() - t
+        out["cpu_reference_float_s_per_iteration_one_core"] = cpu
+        out["gpu_over_cpu_regions"] = cpu["regions"] / (ms["regions"] / 1000.0)
+    return out
+
+
 class quiet_stdout:
     """Sends file descriptor 1 to /dev/null for the duration: the reference's
     classes print progress there, and the bench prints one JSON line."""
@@ -513,9 +587,18 @@ def phase_diverse_report(pynadia, synth, n=1024, cycles=15):
     t = time.perf_counter()
     pd.iterate(5)
     per_cycle = (time.perf_counter() - t) / 5
+    # the frames' own iterations of a cycle, without the blending around them
+    t = time.perf_counter()
+    for _ in range(5):
+        for f in frames:
+            f.iterate(1)
+            f.synchronize()
+    frames_only = (time.perf_counter() - t) / 5
     obj = pd.get_transmission()
     out = {"frames": len(pos), "grid": [n, n], "object": list(obj.shape), "cycles": cycles,
            "gpu_fp64_s_per_reconstruction": whole, "gpu_fp64_ms_per_cycle": 1000.0 * per_cycle,
+           "gpu_frames_ms_per_cycle": 1000.0 * frames_only,
+           "gpu_blending_ms_per_cycle": 1000.0 * (per_cycle - frames_only),
            "positions_found": found, "object_finite": bool(np.isfinite(obj).all())}
     pd.close()
     for f in frames:
@@ -589,6 +672,11 @@ def ours(args, rank, world, local_rank):
         return {"white_field": white_field_report(pynadia, synth)}
     if args.pd_only:
         return {"phase_diverse": phase_diverse_report(pynadia, synth)}
+    if args.tc_only:
+        return {"transmission_constraint": constraint_report(pynadia, synth)}
+    if args.tc_profile:  # a short run of the region constraint alone, for ncu
+        return {"transmission_constraint": constraint_report(pynadia, synth, iters=3,
+                                                             modes=("regions",), cpu=False)}
     if args.fresnel_only:
         return {"fresnel_batch": fresnel_batch_report(pynadia, synth, n_items=args.fresnel_batch)}
     dist = None
@@ -781,6 +869,7 @@ def ours(args, rank, world, local_rank):
 
         white_field = white_field_report(pynadia, synth) if not args.no_wf else None
         phase_diverse = phase_diverse_report(pynadia, synth) if not args.no_pd else None
+        constraint = constraint_report(pynadia, synth) if not args.no_tc else None
 
         serving = None
         if args.serve_requests > 0:
@@ -809,7 +898,7 @@ def ours(args, rank, world, local_rank):
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": launches, "fp64_plain": fp64, "accuracy": accuracy,
             "serving": serving, "fresnel_batch": fresnel_batch, "white_field": white_field,
-            "phase_diverse": phase_diverse,
+            "phase_diverse": phase_diverse, "transmission_constraint": constraint,
         }
     if dist:
         dist.barrier()

@@ -715,18 +715,28 @@ void fresnel_get_transmission(const double2 *esw, const double2 *ill, double2 *o
 }
 
 // TransmissionConstraint::apply_constraint, TransmissionConstraint.c++:76-172
+// region sums of |ln|t|| and |arg t| per block, in a fixed order: each
+// thread walks its pixels four at a time (one int4 of the region map, so the
+// map streams at full width) and accumulates region pixels in order
 __global__ void k_tc_sums(const double2 *__restrict__ t, const int *__restrict__ region, size_t n,
                           int R, double *partials)
 {
     double lnA[kMaxRegions], ph[kMaxRegions];
     for (int r = 0; r < R; ++r) lnA[r] = ph[r] = 0;
-    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
-         k += (size_t)gridDim.x * blockDim.x) {
-        const int r = region[k];
-        if (r > 0) {
-            const double2 v = t[k];
-            ph[r - 1] += fabs(atan2(v.y, v.x));
-            lnA[r - 1] += fabs(log(mag_of(v)));
+    const int4 *reg4 = reinterpret_cast<const int4 *>(region);
+    const size_t n4 = n / 4; // n = nx*ny with even nx and ny
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n4;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int4 rr = __ldg(&reg4[q]);
+        const int rv[4] = {rr.x, rr.y, rr.z, rr.w};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int r = rv[c];
+            if (r > 0) {
+                const double2 v = t[4 * q + c];
+                ph[r - 1] += fabs(atan2(v.y, v.x));
+                lnA[r - 1] += fabs(log(mag_of(v)));
+            }
         }
     }
     for (int r = 0; r < R; ++r) {
@@ -740,17 +750,18 @@ __global__ void k_tc_sums(const double2 *__restrict__ t, const int *__restrict__
     }
 }
 
+// one block per region: the block partials summed by a fixed tree
 __global__ void k_tc_cmean(const double *partials, int nblocks, int R, const double *params,
                            double *cmean)
 {
-    const int r = threadIdx.x;
-    if (r >= R) return;
+    const int r = blockIdx.x;
     double a = 0, b = 0;
-    for (int blk = 0; blk < nblocks; ++blk) {
+    for (int blk = threadIdx.x; blk < nblocks; blk += blockDim.x) {
         a += partials[2 * ((size_t)blk * R + r)];
         b += partials[2 * ((size_t)blk * R + r) + 1];
     }
-    cmean[r] = params[4 * r + 2] != 0 ? params[4 * r + 3] : a / b;
+    block_sum2(a, b);
+    if (threadIdx.x == 0) cmean[r] = params[4 * r + 2] != 0 ? params[4 * r + 3] : a / b;
 }
 
 __global__ void k_tc_apply(double2 *t, const int *__restrict__ region, size_t n, int R,
@@ -760,10 +771,10 @@ __global__ void k_tc_apply(double2 *t, const int *__restrict__ region, size_t n,
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
          k += (size_t)gridDim.x * blockDim.x) {
         double2 v = t[k];
-        const double phase_old = atan2(v.y, v.x);
         double mag_old = mag_of(v);
         const int r = R > 0 ? region[k] : 0;
         if (r > 0) {
+            const double phase_old = atan2(v.y, v.x);
             const double a1 = params[4 * (r - 1)], a2 = params[4 * (r - 1) + 1];
             const double cm = cmean[r - 1];
             const double mag_new = exp((1 - a1) * log(mag_old) + a1 * cm * phase_old);
@@ -790,7 +801,7 @@ void transmission_constraint(double2 *t, const int *region, size_t n, int nregio
 {
     if (nregions > 0) {
         k_tc_sums<<<kRedBlocks, kThreads, 0, s>>>(t, region, n, nregions, partials);
-        k_tc_cmean<<<1, 32, 0, s>>>(partials, kRedBlocks, nregions, params, cmean);
+        k_tc_cmean<<<nregions, kThreads, 0, s>>>(partials, kRedBlocks, nregions, params, cmean);
     }
     if (nregions > 0 || charge_flip || enforce_unity)
         k_tc_apply<<<grid_of(n), kThreads, 0, s>>>(t, region, n, nregions, params, cmean,

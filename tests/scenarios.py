@@ -189,19 +189,8 @@ def fresnel_wf_mixed(make, n=32, seed=6, iterations=12):
 
 
 def constraint_regions(n, ny=None):
-    """Three ComplexConstraint regions inside the central support: two
-    disjoint blocks and a third that overlaps the first (the earlier region
-    keeps the shared pixels)."""
-    ny = ny or n
-    c0, c1 = n // 2, ny // 2
-    q = max(2, n // 10)
-    a = np.zeros((n, ny))
-    b = np.zeros((n, ny))
-    c = np.zeros((n, ny))
-    a[c0 - q:c0, c1 - q:c1] = 1
-    b[c0:c0 + q, c1:c1 + q] = 1
-    c[c0 - q // 2:c0 + q // 2, c1 - q:c1] = 1
-    return [a, b, c], [(0.5, 0.4), (0.3, 0.6), (0.8, 0.1)], np.array([np.nan, 0.7, np.nan])
+    """Three ComplexConstraint regions (pynadia.synth.constraint_regions)."""
+    return synth.constraint_regions(n, ny)
 
 
 def planar_constrained(make, n=32, seed=3, iterations=12, hio_from=3):
