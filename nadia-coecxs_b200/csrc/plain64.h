@@ -23,6 +23,8 @@ struct Fft2d {
     DevBuf<double2> wx, wy;
     int rows_per_block = 1, cols_per_block = 1;
     size_t row_smem = 0, col_smem = 0;
+    bool row_one = false, col_one = false; // radix-2/4/8 plans: the one-buffer kernels
+    bool col_wide = false;                 // columns of 2048 points and more: 512 threads
     void init(int nx, int ny);
     void exec(double2 *a, bool forward, cudaStream_t s) const;
 };
