@@ -65,6 +65,8 @@ def parse():
     p.add_argument("--no-tc", action="store_true", help="skip the TransmissionConstraint report")
     p.add_argument("--tc-only", action="store_true",
                    help="print the TransmissionConstraint report only")
+    p.add_argument("--pd-profile", action="store_true",
+                   help="two phase-diverse cycles without position searches (for ncu)")
     p.add_argument("--tc-profile", action="store_true",
                    help="three iterations with the region constraint only (for ncu)")
     p.add_argument("--wf-only", action="store_true", help="print the FresnelCDI_WF report only")
@@ -530,7 +532,7 @@ class quiet_stdout:
         return False
 
 
-def phase_diverse_report(pynadia, synth, n=1024, cycles=15):
+def phase_diverse_report(pynadia, synth, n=1024, cycles=15, cpu=True, search=True):
     """PhaseDiverseCDI modelled on the reference's example
     (NADIA/examples/PhaseDiverse_example.c): seven FresnelCDI frames of
     1024^2 at the example's positions, wavelength, pixel size and distances,
@@ -581,7 +583,7 @@ def phase_diverse_report(pynadia, synth, n=1024, cycles=15):
     frames = frames_on(gpu_make)
     pd = pynadia.PhaseDiverse()
     t = time.perf_counter()
-    run(frames, pd)
+    run(frames, pd, search=search)
     whole = time.perf_counter() - t
     found = [(pd.get_final_x_position(k), pd.get_final_y_position(k)) for k in range(len(pos))]
     t = time.perf_counter()
@@ -605,7 +607,7 @@ def phase_diverse_report(pynadia, synth, n=1024, cycles=15):
         f.close()
     sys.path.insert(0, ORACLE)
     import pyoracle as po
-    if po.reference_available("32_fast"):
+    if cpu and po.reference_available("32_fast"):
         rmake = lambda kind, nx, ny, **kw: po.Reference(kind, nx, ny, variant="32_fast", **kw)  # noqa: E731
         with quiet_stdout():
             rframes = frames_on(rmake)
@@ -674,6 +676,9 @@ def ours(args, rank, world, local_rank):
         return {"phase_diverse": phase_diverse_report(pynadia, synth)}
     if args.tc_only:
         return {"transmission_constraint": constraint_report(pynadia, synth)}
+    if args.pd_profile:  # a short phase-diverse run without the searches, for ncu
+        return {"phase_diverse": phase_diverse_report(pynadia, synth, cycles=2, cpu=False,
+                                                      search=False)}
     if args.tc_profile:  # a short run of the region constraint alone, for ncu
         return {"transmission_constraint": constraint_report(pynadia, synth, iters=3,
                                                              modes=("regions",), cpu=False)}
