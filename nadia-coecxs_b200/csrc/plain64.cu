@@ -306,6 +306,124 @@ __global__ void k_combine(double2 *x, const double2 *__restrict__ pfs,
     }
 }
 
+// k_support's operation on one value
+__device__ __forceinline__ double2 supported(double2 v, double sv)
+{
+    if (sv == 0) return make_double2(0.0, 0.0);
+    if (sv < 1) return make_double2(v.x * sv, v.y * sv);
+    return v;
+}
+
+// The combine loop with the support projections formed on the fly (no
+// transmission constraint, no PfPs term): Ps x = support(x), PsPf x =
+// support(Pf x); the same sums in the same order as copying, projecting and
+// combining separately.
+__global__ void k_combine_support(double2 *x, const double2 *__restrict__ pf,
+                                  const double *__restrict__ sup, int use_ps, int use_psf,
+                                  Weights W, size_t n)
+{
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const double2 v = x[k];
+        const double sv = sup[k];
+        double vr = W.id * v.x, vi = W.id * v.y;
+        double2 f = make_double2(0.0, 0.0);
+        if (pf) {
+            f = pf[k];
+            vr += W.w[3] * f.x;
+            vi += W.w[3] * f.y;
+        }
+        if (use_ps) {
+            const double2 t = supported(v, sv);
+            vr += W.w[2] * t.x;
+            vi += W.w[2] * t.y;
+        }
+        if (use_psf) {
+            const double2 t = supported(f, sv);
+            vr += W.w[0] * t.x;
+            vi += W.w[0] * t.y;
+        }
+        x[k] = make_double2(vr, vi);
+    }
+}
+
+// PlanarCDI's detector side of project_intensity (PlanarCDI.c++:65-73 around
+// BaseCDI::scale_intensity, BaseCDI.c++:163-189) between the two transforms:
+// invert(scale) -> scale_intensity -> invert(scale).  The quadrant swap pairs
+// q with p(q), so per element out[q] = s * set_mag(s * a[q], sqrt(I)[p(q)])
+// (measured pixels; s * (s * a[q]) otherwise) -- the same operations.
+__global__ void k_detector_planar(double2 *c, const double *__restrict__ isqrt,
+                                  const double *__restrict__ bs, int nx, int ny, double s,
+                                  double *partials)
+{
+    double diff = 0, mag = 0;
+    const int mx = nx / 2, my = ny / 2;
+    const size_t n = (size_t)nx * ny;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q / ny), j = (int)(q - (size_t)i * ny);
+        const int ip = i < mx ? i + mx : i - mx, jp = j < my ? j + my : j - my;
+        const size_t d = (size_t)ip * ny + jp;
+        const double2 u = c[q];
+        double2 v = make_double2(u.x * s, u.y * s);
+        if (bs == nullptr || bs[d] > 0) {
+            const double cis = isqrt[d];
+            const double cm = mag_of(v);
+            v = set_mag(v, cis);
+            mag += cis * cis;
+            diff += (cm - cis) * (cm - cis);
+        }
+        c[q] = make_double2(v.x * s, v.y * s);
+    }
+    block_sum2(diff, mag);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = diff;
+        partials[2 * blockIdx.x + 1] = mag;
+    }
+}
+
+// FresnelCDI's detector side between the two transforms (FresnelCDI.c++:217-250):
+// multiply_factors(-1) -> add(illumination) -> scale_intensity ->
+// add(-illumination) -> multiply_factors(+1), all at the same element.
+__global__ void k_detector_fresnel(double2 *c, const double2 *__restrict__ coef,
+                                   const double2 *__restrict__ ill,
+                                   const double *__restrict__ isqrt,
+                                   const double *__restrict__ bs, int nx, int ny,
+                                   double *partials)
+{
+    double diff = 0, mag = 0;
+    const double x_mid = (nx - 1) / 2.0, y_mid = (ny - 1) / 2.0;
+    const int qy = ny / 2;
+    const size_t n = (size_t)nx * ny;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / ny), j = (int)(e - (size_t)i * ny);
+        const int i_ = (int)(x_mid - fabs(x_mid - i));
+        const int j_ = (int)(y_mid - fabs(y_mid - j));
+        const double2 cf = coef[(size_t)i_ * qy + j_];
+        const double2 t = ill[e];
+        double2 o = c[e];
+        double cr = cf.x, ci = -1 * cf.y;
+        double2 v = make_double2(o.x * cr - o.y * ci, o.y * cr + o.x * ci);
+        v = make_double2(v.x + 1.0 * t.x, v.y + 1.0 * t.y);
+        if (bs == nullptr || bs[e] > 0) {
+            const double cis = isqrt[e];
+            const double cm = mag_of(v);
+            v = set_mag(v, cis);
+            mag += cis * cis;
+            diff += (cm - cis) * (cm - cis);
+        }
+        v = make_double2(v.x + -1.0 * t.x, v.y + -1.0 * t.y);
+        ci = 1 * cf.y;
+        c[e] = make_double2(v.x * cr - v.y * ci, v.y * cr + v.x * ci);
+    }
+    block_sum2(diff, mag);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = diff;
+        partials[2 * blockIdx.x + 1] = mag;
+    }
+}
+
 __global__ void k_multiply_factors(double2 *c, const double2 *__restrict__ coef, int nx, int ny,
                                    int direction)
 {
@@ -781,6 +899,32 @@ void combine(double2 *x, const double2 *pfs, const double2 *pf, const double2 *p
     for (int i = 0; i < 5; ++i) W.w[i] = w[i];
     W.id = 1 + w[4];
     k_combine<<<grid_of(n), kThreads, 0, s>>>(x, pfs, pf, ps, psf, W, n);
+}
+
+void combine_support(double2 *x, const double2 *pf, const double *support, bool use_ps,
+                     bool use_psf, const double w[5], size_t n, cudaStream_t s)
+{
+    Weights W;
+    for (int i = 0; i < 5; ++i) W.w[i] = w[i];
+    W.id = 1 + w[4];
+    k_combine_support<<<grid_of(n), kThreads, 0, s>>>(x, pf, support, use_ps ? 1 : 0,
+                                                     use_psf ? 1 : 0, W, n);
+}
+
+void detector_planar(double2 *c, const double *isqrt, const double *bs, int nx, int ny,
+                     double *partials, double *err, cudaStream_t s)
+{
+    const double f = 1.0 / (sqrt((double)(nx * ny))); // invert(scale), Complex_2D.c++:318-353
+    k_detector_planar<<<kRedBlocks, kThreads, 0, s>>>(c, isqrt, bs, nx, ny, f, partials);
+    k_finish_error<<<1, kThreads, 0, s>>>(partials, kRedBlocks, err);
+}
+
+void detector_fresnel(double2 *c, const double2 *coef, const double2 *ill, const double *isqrt,
+                      const double *bs, int nx, int ny, double *partials, double *err,
+                      cudaStream_t s)
+{
+    k_detector_fresnel<<<kRedBlocks, kThreads, 0, s>>>(c, coef, ill, isqrt, bs, nx, ny, partials);
+    k_finish_error<<<1, kThreads, 0, s>>>(partials, kRedBlocks, err);
 }
 
 void multiply_factors(double2 *c, const double2 *coef, int nx, int ny, int direction,

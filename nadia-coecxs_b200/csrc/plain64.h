@@ -45,6 +45,22 @@ void support_constraint(double2 *c, const double *support, size_t n, cudaStream_
 void combine(double2 *x, const double2 *pfs, const double2 *pf, const double2 *ps,
              const double2 *psf, const double w[5], size_t n, cudaStream_t s);
 
+// The combine with Ps and PsPf formed on the fly from the support (valid
+// without a transmission constraint and without the PfPs term); pf may be
+// null (no Pf term, and then no PsPf term).
+void combine_support(double2 *x, const double2 *pf, const double *support, bool use_ps,
+                     bool use_psf, const double w[5], size_t n, cudaStream_t s);
+
+// The detector side of project_intensity between its two transforms, one
+// kernel each: PlanarCDI invert -> scale_intensity -> invert (PlanarCDI.c++:
+// 65-73); FresnelCDI multiply_factors -> add(W) -> scale_intensity ->
+// add(-W) -> multiply_factors (FresnelCDI.c++:217-250).  Error to *err.
+void detector_planar(double2 *c, const double *isqrt, const double *bs, int nx, int ny,
+                     double *partials, double *err, cudaStream_t s);
+void detector_fresnel(double2 *c, const double2 *coef, const double2 *ill, const double *isqrt,
+                      const double *bs, int nx, int ny, double *partials, double *err,
+                      cudaStream_t s);
+
 // FresnelCDI::multiply_factors, FresnelCDI.c++:98-126 (quarter table coef).
 void multiply_factors(double2 *c, const double2 *coef, int nx, int ny, int direction,
                       cudaStream_t s);

@@ -861,6 +861,19 @@ void Solver::plain_project(double2 *c)
         plain_scale(padded.p);
         plain_propagate_from(padded.p, true);
         plain::unpad(padded.p, nx, ny, px, py, c, st);
+    } else if (kind == NADIA_PLANAR) {
+        // propagate_to, scale_intensity, propagate_from with the element-wise
+        // steps between the transforms in one kernel
+        fft.exec(c, true, st);
+        plain::detector_planar(c, isqrt.p, bs_ptr(), nx, ny, partials.p, d_err.p, st);
+        fft.exec(c, false, st);
+    } else if (kind == NADIA_FRESNEL) {
+        plain::invert(c, nx, ny, true, st);
+        fft.exec(c, true, st);
+        plain::detector_fresnel(c, coef.p, illum.p, isqrt.p, bs_ptr(), nx, ny, partials.p,
+                                d_err.p, st);
+        fft.exec(c, false, st);
+        plain::invert(c, nx, ny, true, st);
     } else {
         plain_propagate_to(c, false);
         plain_scale(c);
@@ -894,6 +907,18 @@ void Solver::plain_iterate_once()
     if (algorithm == NADIA_ER) {
         plain_project(x.p);
         plain_apply_support(x.p);
+        return;
+    }
+    if (!tc.active && w[PFS] == 0 && (w[PSF] == 0 || w[PF] != 0)) {
+        // the support projections formed inside the combine (same arithmetic)
+        const bool pf = w[PF] != 0;
+        if (pf) {
+            if (!tPF) tPF.alloc(n);
+            NADIA_CUDA(cudaMemcpyAsync(tPF.p, x.p, nb, cudaMemcpyDeviceToDevice, st));
+            plain_project(tPF.p);
+        }
+        plain::combine_support(x.p, pf ? tPF.p : nullptr, support.p, w[PS] != 0, w[PSF] != 0,
+                               w, n, st);
         return;
     }
     ensure_temps();
