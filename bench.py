@@ -397,9 +397,8 @@ def white_field_report(pynadia, synth, n=2048, iters=26):
     512 on each side), 26 iterations: the FP64 form on the GPU (CUDA events)
     against the reference's float build on one host core (one timed
     iteration).  Algorithmic bytes of the FP64 form per pixel and iteration:
-    four 2-D transforms of two passes (4 x 2 x 32), two quadrant swaps (2 x
-    32), two factor multiplies (2 x 32), the support (40) and the modulus (40)
-    = 464."""
+    four 2-D transforms of two passes (4 x 2 x 32), two swap-and-factor passes
+    (2 x 32), the support (40) and the modulus (40) = 400."""
     import torch
     f = synth.FresnelWFCase(n, seed=21)
     kw = dict(wavelength=f.wavelength, zone_focal_length=f.z12, focal_detector_length=f.z23,
@@ -420,7 +419,7 @@ def white_field_report(pynadia, synth, n=2048, iters=26):
     err = s.get_error()
     s.close()
     peak, _ = measured_peak()
-    gbs = 464.0 * n * n * iters / sec / 1e9
+    gbs = 400.0 * n * n * iters / sec / 1e9
     out = {"grid": [n, n], "iterations": iters, "gpu_fp64_ms_per_iteration": 1000.0 * sec / iters,
            "gpu_fp64_recon_per_s": 1.0 / sec, "final_error": err,
            "hbm_gbs_algorithmic": gbs, "roofline_frac": gbs / peak}

@@ -424,6 +424,48 @@ __global__ void k_detector_fresnel(double2 *c, const double2 *__restrict__ coef,
     }
 }
 
+// multiply_factors' operation on element (i, j)
+__device__ __forceinline__ double2 factor_at(double2 o, const double2 *__restrict__ coef, int i,
+                                             int j, int nx, int ny, int direction)
+{
+    const double x_mid = (nx - 1) / 2.0, y_mid = (ny - 1) / 2.0;
+    const int i_ = (int)(x_mid - fabs(x_mid - i));
+    const int j_ = (int)(y_mid - fabs(y_mid - j));
+    const double2 cf = coef[(size_t)i_ * (ny / 2) + j_];
+    const double cr = cf.x, ci = direction * cf.y;
+    return make_double2(o.x * cr - o.y * ci, o.y * cr + o.x * ci);
+}
+
+// invert(scale) and multiply_factors in one pass (FresnelCDI_WF.c++:165-182):
+// each thread takes a swap pair (q, p(q)); factors_first multiplies before
+// the swap (propagate_to_detector), otherwise after it (propagate_from)
+__global__ void k_invert_factors(double2 *a, const double2 *__restrict__ coef, int nx, int ny,
+                                 double s, int direction, int factors_first)
+{
+    const int mx = nx / 2, my = ny / 2;
+    const size_t total = (size_t)nx * my;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / my), j = (int)(e - (size_t)i * my);
+        const int jn = j + my;
+        int in = i + mx;
+        if (i >= mx) in = in - 2 * mx;
+        double2 *pp = a + (size_t)in * ny + jn, *qq = a + (size_t)i * ny + j;
+        double2 t = *pp, u = *qq;
+        if (factors_first) {
+            t = factor_at(t, coef, in, jn, nx, ny, direction);
+            u = factor_at(u, coef, i, j, nx, ny, direction);
+        }
+        double2 np = make_double2(u.x * s, u.y * s), nq = make_double2(t.x * s, t.y * s);
+        if (!factors_first) {
+            np = factor_at(np, coef, in, jn, nx, ny, direction);
+            nq = factor_at(nq, coef, i, j, nx, ny, direction);
+        }
+        *pp = np;
+        *qq = nq;
+    }
+}
+
 __global__ void k_multiply_factors(double2 *c, const double2 *__restrict__ coef, int nx, int ny,
                                    int direction)
 {
@@ -899,6 +941,14 @@ void combine(double2 *x, const double2 *pfs, const double2 *pf, const double2 *p
     for (int i = 0; i < 5; ++i) W.w[i] = w[i];
     W.id = 1 + w[4];
     k_combine<<<grid_of(n), kThreads, 0, s>>>(x, pfs, pf, ps, psf, W, n);
+}
+
+void invert_factors(double2 *c, const double2 *coef, int nx, int ny, int direction,
+                    bool factors_first, cudaStream_t s)
+{
+    const double f = 1.0 / (sqrt((double)(nx * ny)));
+    k_invert_factors<<<grid_of((size_t)nx * (ny / 2)), kThreads, 0, s>>>(
+        c, coef, nx, ny, f, direction, factors_first ? 1 : 0);
 }
 
 void combine_support(double2 *x, const double2 *pf, const double *support, bool use_ps,

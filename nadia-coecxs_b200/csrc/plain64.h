@@ -61,6 +61,11 @@ void detector_fresnel(double2 *c, const double2 *coef, const double2 *ill, const
                       const double *bs, int nx, int ny, double *partials, double *err,
                       cudaStream_t s);
 
+// invert(scale) and multiply_factors in one pass, the factors applied before
+// the swap (factors_first) or after it -- FresnelCDI_WF's propagations.
+void invert_factors(double2 *c, const double2 *coef, int nx, int ny, int direction,
+                    bool factors_first, cudaStream_t s);
+
 // FresnelCDI::multiply_factors, FresnelCDI.c++:98-126 (quarter table coef).
 void multiply_factors(double2 *c, const double2 *coef, int nx, int ny, int direction,
                       cudaStream_t s);

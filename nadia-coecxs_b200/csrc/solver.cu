@@ -790,8 +790,7 @@ void Solver::plain_propagate_to(double2 *c, bool pg)
     if (kind == NADIA_FRESNEL_WF) {
         // FresnelCDI_WF::propagate_to_detector, FresnelCDI_WF.c++:176-182
         fft.exec(c, true, st);
-        plain::multiply_factors(c, coef.p, nx, ny, -1, st);
-        plain::invert(c, nx, ny, true, st);
+        plain::invert_factors(c, coef.p, nx, ny, -1, true, st); // factors, then the swap
         fft.exec(c, true, st);
     } else if (kind == NADIA_FRESNEL) {
         // FresnelCDI::propagate_to_detector, FresnelCDI.c++:245-250
@@ -815,8 +814,7 @@ void Solver::plain_propagate_from(double2 *c, bool pg)
     if (kind == NADIA_FRESNEL_WF) {
         // FresnelCDI_WF::propagate_from_detector, FresnelCDI_WF.c++:165-173
         fft.exec(c, false, st);
-        plain::invert(c, nx, ny, true, st);
-        plain::multiply_factors(c, coef.p, nx, ny, +1, st);
+        plain::invert_factors(c, coef.p, nx, ny, +1, false, st); // the swap, then factors
         fft.exec(c, false, st);
     } else if (kind == NADIA_FRESNEL) {
         // FresnelCDI::propagate_from_detector, FresnelCDI.c++:238-243
