@@ -14,11 +14,13 @@
 //   - set_algorithm, set_custom_algorithm, set_relaxation_parameter and
 //     print_algorithm are virtual, so FresnelCDI_WF's versions (a warning:
 //     its algorithm is fixed) answer calls through a BaseCDI pointer too;
-//   - a TransmissionConstraint given to set_complex_constraint runs in the
-//     FP64 form (the reconstruction moves to it there), and is read when
-//     iterate() or apply_support() next runs (changes to it after that are
-//     picked up at the following call); the same holds for a reconstruction
-//     added to a PhaseDiverseCDI.
+//   - a TransmissionConstraint's per-pixel part (charge flipping, unit
+//     magnitude) runs inside the FP32 form's fused passes; complex-constraint
+//     regions and custom functions run in the FP64 form, to which an FP32
+//     reconstruction moves when it gets them (as does an FP32 PolyCDI given
+//     any constraint).  The constraint is read when iterate() or
+//     apply_support() next runs (changes to it after that are picked up at
+//     the following call).
 #ifndef NADIA_DROPIN_BASECDI_H
 #define NADIA_DROPIN_BASECDI_H
 
@@ -51,11 +53,9 @@ public:
         }
     }
 
-    // BaseCDI::set_complex_constraint (BaseCDI.h:471-473); constraints run in
-    // the FP64 form, to which an FP32 reconstruction moves here
+    // BaseCDI::set_complex_constraint (BaseCDI.h:471-473)
     virtual void set_complex_constraint(TransmissionConstraint &trans_constraint)
     {
-        nadia_cxx::check(nadia_convert_to_fp64(h));
         transmission_constraint = &trans_constraint;
         trans_constraint.push_to(h, nx, ny, true);
     }

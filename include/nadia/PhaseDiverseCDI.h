@@ -4,8 +4,8 @@
 // other BaseCDI) frames, run on the GPU through nadia_pd_* (include/nadia_b200.h).
 //
 // Differences a caller can observe:
-//   - frames run in the FP64 form; a frame of the float build moves to it
-//     when it is added (nadia_convert_to_fp64);
+//   - frames keep their form (the float build's FP32 frames stay FP32, the
+//     object is FP64); an FP32 PolyCDI frame moves to the FP64 form when added;
 //   - get_transmission returns a copy of the object, refreshed by each call;
 //     edits to it reach the reconstruction through set_transmission;
 //   - frames must outlive this object (as in the reference), and the library
@@ -41,9 +41,13 @@ public:
     // add_new_position -- PhaseDiverseCDI.c++:104-160
     void add_new_position(BaseCDI *local, double x = 0, double y = 0, double alpha = 1)
     {
-        nadia_cxx::check(nadia_convert_to_fp64(local->handle()));
         local->prepare_device();
-        nadia_cxx::check(nadia_pd_add_position(h, local->handle(), x, y, alpha));
+        int rc = nadia_pd_add_position(h, local->handle(), x, y, alpha);
+        if (rc == NADIA_ERR_UNSUPPORTED) { // an FP32 PolyCDI frame
+            nadia_cxx::check(nadia_convert_to_fp64(local->handle()));
+            rc = nadia_pd_add_position(h, local->handle(), x, y, alpha);
+        }
+        nadia_cxx::check(rc);
         frames.push_back(local);
         std::cout << "Added position " << frames.size() - 1 << std::endl;
     }

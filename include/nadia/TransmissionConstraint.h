@@ -152,9 +152,19 @@ public:
             alpha[2 * r + 1] = c->get_alpha2();
             fixed[r] = c->is_c_fixed() ? c->get_c_mean() : NAN;
         }
-        nadia_cxx::check(nadia_set_transmission_constraint(
+        // regions and custom functions run in the FP64 form (the per-pixel
+        // part also runs inside the FP32 form's fused passes)
+        if (R > 0 || custom_constraint) nadia_cxx::check(nadia_convert_to_fp64(h));
+        int rc = nadia_set_transmission_constraint(
             h, do_enforce_unity, do_charge_flip, flip_sign, R, R ? regions.data() : nullptr,
-            R ? alpha.data() : nullptr, R ? fixed.data() : nullptr));
+            R ? alpha.data() : nullptr, R ? fixed.data() : nullptr);
+        if (rc == NADIA_ERR_UNSUPPORTED) { // e.g. an FP32 PolyCDI
+            nadia_cxx::check(nadia_convert_to_fp64(h));
+            rc = nadia_set_transmission_constraint(
+                h, do_enforce_unity, do_charge_flip, flip_sign, R, R ? regions.data() : nullptr,
+                R ? alpha.data() : nullptr, R ? fixed.data() : nullptr);
+        }
+        nadia_cxx::check(rc);
         nadia_cxx::check(nadia_set_transmission_custom(h, custom_constraint ? &trampoline : nullptr,
                                                        this));
     }

@@ -139,8 +139,9 @@ int nadia_read_spec(const char *path, double *rows, int capacity, int *nrows);
 /* Moves an FP32 reconstruction to the FP64 form in place (no-op on FP64):
  * estimate, support, intensity, beam stop, Fresnel illumination and geometry,
  * spectrum, algorithm, error history and n-best results carry over, FP32
- * values widened.  Needed before a transmission constraint or a
- * phase-diverse position (both FP64 only) on an FP32 handle. */
+ * values widened.  Needed before complex-constraint regions or a custom
+ * constraint function (FP64 only), or any constraint or phase-diverse
+ * position on an FP32 PolyCDI. */
 int nadia_convert_to_fp64(nadia_solver *s);
 
 /* NADIA_FP32 or NADIA_FP64. */
@@ -161,7 +162,10 @@ int nadia_poly_get_padding(const nadia_solver *s, int *px, int *py);
  * most 16) ComplexConstraint regions, given as nregions masks of nx*ny
  * (a pixel belongs to the first region whose mask is > 0 there), alpha as
  * nregions pairs (alpha1, alpha2), fixed_c as nregions values (NaN = c_mean
- * measured each time; NULL = all measured).  FP64 form only. */
+ * measured each time; NULL = all measured).  The FP32 form runs the
+ * per-pixel part (unit magnitude, charge flipping) inside its fused row pass
+ * and returns NADIA_ERR_UNSUPPORTED for regions and for PolyCDI: convert the
+ * handle first (nadia_convert_to_fp64). */
 int nadia_set_transmission_constraint(nadia_solver *s, int enforce_unity, int charge_flip,
                                       int flip_sign, int nregions, const double *regions,
                                       const double *alpha, const double *fixed_c);
@@ -169,7 +173,8 @@ int nadia_set_transmission_constraint(nadia_solver *s, int enforce_unity, int ch
 /* TransmissionConstraint::set_custom_constraint (TransmissionConstraint.h:
  * 357-359): fn is called on the host with the constrained transmission
  * (interleaved complex, x*ny+y) after the built-in steps and may change it;
- * NULL removes it.  Needs a constraint set first. */
+ * NULL removes it.  Needs a constraint set first; FP64 form only
+ * (NADIA_ERR_UNSUPPORTED on FP32 unless fn is NULL). */
 int nadia_set_transmission_custom(nadia_solver *s,
                                   void (*fn)(double *transmission, int nx, int ny, void *user),
                                   void *user);
@@ -423,7 +428,8 @@ int nadia_shrinkwrap_noalloc_f32(const float *esw_dev, float *support_dev, int n
 /* ---- PhaseDiverseCDI (phase-diverse / ptychographic reconstruction) -------- */
 
 /* PhaseDiverseCDI (NADIA/include/PhaseDiverseCDI.h, NADIA/src/PhaseDiverseCDI.c++):
- * reconstructions ("frames", FP64 handles: Fresnel frames exchange their
+ * reconstructions ("frames": FP64 handles, or FP32 ones other than PolyCDI;
+ * Fresnel frames exchange their
  * transmission function, others their exit-surface wave) placed at (x, y) on
  * one global object.  Series mode updates the object after each frame;
  * parallel mode iterates every frame (concurrently on the GPU) and then

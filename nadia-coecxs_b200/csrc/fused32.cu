@@ -257,6 +257,39 @@ __global__ void k_fresnel_set_t(const float2 *t, const float2 *ill, float2 *esw,
     }
 }
 
+// the constraint's per-pixel part over a whole panel-layout array (the
+// transmission function FresnelCDI::get_transmission_function returns)
+__global__ void k_tc_pixels(float2 *t, size_t n, const Slot *slot)
+{
+    const Slot &S = *slot;
+    for (size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x; a < n;
+         a += (size_t)gridDim.x * blockDim.x)
+        t[a] = tc_pixel(t[a], S);
+}
+
+// panel layout (float) <-> the reference's order (double), on the device
+__global__ void k_panel_widen(const float2 *src, double2 *dst, int nx, int ny)
+{
+    const size_t n = (size_t)nx * ny;
+    for (size_t d = blockIdx.x * (size_t)blockDim.x + threadIdx.x; d < n;
+         d += (size_t)gridDim.x * blockDim.x) {
+        const int xx = (int)(d / ny), yy = (int)(d % ny);
+        const float2 v = src[panel_index_dev(xx, yy, nx)];
+        dst[d] = make_double2(v.x, v.y);
+    }
+}
+
+__global__ void k_panel_narrow(const double2 *src, float2 *dst, int nx, int ny)
+{
+    const size_t n = (size_t)nx * ny;
+    for (size_t d = blockIdx.x * (size_t)blockDim.x + threadIdx.x; d < n;
+         d += (size_t)gridDim.x * blockDim.x) {
+        const int xx = (int)(d / ny), yy = (int)(d % ny);
+        const double2 v = src[d];
+        dst[panel_index_dev(xx, yy, nx)] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
 // T = (ESW + L) / L, 1 where L = 0 (FresnelCDI.c++:298-355)
 __global__ void k_fresnel_get_t(const float2 *esw, const float2 *ill, float2 *out, size_t n)
 {
@@ -419,10 +452,11 @@ bool supported(int n) { return !variants(n).empty(); }
 namespace {
 
 struct TuneKey {
-    int dev, nx, ny, fresnel, batch;
+    int dev, nx, ny, fresnel, batch, plain_rows;
     bool operator<(const TuneKey &o) const
     {
-        return std::tie(dev, nx, ny, fresnel, batch) < std::tie(o.dev, o.nx, o.ny, o.fresnel, o.batch);
+        return std::tie(dev, nx, ny, fresnel, batch, plain_rows) <
+               std::tie(o.dev, o.nx, o.ny, o.fresnel, o.batch, o.plain_rows);
     }
 };
 
@@ -452,14 +486,14 @@ float time_launches(const std::function<void(cudaStream_t)> &f, cudaStream_t st,
 
 } // namespace
 
-const Choice &choose(int nx, int ny, bool fresnel, int nslots)
+const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
 {
     static std::mutex mu;
     static std::map<TuneKey, Choice> cache;
     int dev = 0;
     NADIA_CUDA(cudaGetDevice(&dev));
     const int batch = nslots > 1 ? 4 : 1;
-    TuneKey key{dev, nx, ny, fresnel ? 1 : 0, batch};
+    TuneKey key{dev, nx, ny, fresnel ? 1 : 0, batch, plain_rows ? 1 : 0};
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
@@ -478,12 +512,12 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots)
     for (const auto &v : cv)
         if (ny % v.L == 0) cols.push_back(&v);
     for (const auto &v : rv)
-        if (nx % v.L == 0) rows.push_back(&v);
+        if (nx % v.L == 0 && !(plain_rows && v.persistent)) rows.push_back(&v);
     NADIA_REQUIRE(!cols.empty() && !rows.empty(), NADIA_ERR_UNSUPPORTED,
                   "grid shape does not divide into the FP32 tiles");
     ch.col = cols[0];
     ch.row = rows[0];
-    const char *tfile = getenv("NADIA_TUNE_FILE");
+    const char *tfile = plain_rows ? nullptr : getenv("NADIA_TUNE_FILE");
     if (tfile) {
         if (FILE *f = fopen(tfile, "r")) {
             int a, b, c, d, ci, ri;
@@ -865,11 +899,65 @@ void Fused32::fresnel_set_transmission(const double *t)
     I.S.sync();
 }
 
+void Fused32::set_constraint(bool on, bool unity, bool flip, int flip_sign)
+{
+    Impl &I = *impl;
+    NADIA_REQUIRE(!on || I.S.kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
+                  "a transmission constraint on PolyCDI runs in the FP64 form");
+    I.h_slot.tc_on = on ? 1 : 0;
+    I.h_slot.tc_unity = on && unity ? 1 : 0;
+    I.h_slot.tc_flip = on && flip ? 1 : 0;
+    I.h_slot.tc_sign = flip_sign > 0 ? 1.f : -1.f;
+    I.h_slot.tc_ill = on && I.S.kind == NADIA_FRESNEL ? I.ill.p : nullptr;
+    if (I.S.kind != NADIA_POLY) {
+        NADIA_CUDA(cudaStreamSynchronize(I.S.st));
+        I.choice = &choose(I.nx, I.ny, I.S.kind == NADIA_FRESNEL, 1, on);
+        if (I.graph_exec) { // captured with the other variants
+            cudaGraphExecDestroy(I.graph_exec);
+            I.graph_exec = nullptr;
+        }
+        I.use_choice(I.choice);
+    }
+    I.push_slot();
+}
+
+bool Fused32::constrained() const { return impl->h_slot.tc_on != 0; }
+
+void Fused32::transmission_to_device(double2 *dst)
+{
+    Impl &I = *impl;
+    const float2 *src = I.x.p;
+    if (I.S.kind == NADIA_FRESNEL) {
+        I.p_valid = false; // T is formed in the work array
+        I.push_slot();
+        k_fresnel_get_t<<<grid1(I.n), 256, 0, I.S.st>>>(I.x.p, I.ill.p, I.P.p, I.n);
+        if (I.h_slot.tc_on) k_tc_pixels<<<grid1(I.n), 256, 0, I.S.st>>>(I.P.p, I.n, I.slot.p);
+        src = I.P.p;
+    }
+    k_panel_widen<<<grid1(I.n), 256, 0, I.S.st>>>(src, dst, I.nx, I.ny);
+    NADIA_CUDA(cudaGetLastError());
+}
+
+void Fused32::transmission_from_device(const double2 *src)
+{
+    Impl &I = *impl;
+    I.p_valid = false;
+    if (I.S.kind == NADIA_FRESNEL) {
+        k_panel_narrow<<<grid1(I.n), 256, 0, I.S.st>>>(src, I.P.p, I.nx, I.ny);
+        k_fresnel_set_t<<<grid1(I.n), 256, 0, I.S.st>>>(I.P.p, I.ill.p, I.x.p, I.nx, I.ny);
+    } else {
+        k_panel_narrow<<<grid1(I.n), 256, 0, I.S.st>>>(src, I.x.p, I.nx, I.ny);
+    }
+    NADIA_CUDA(cudaGetLastError());
+}
+
 void Fused32::fresnel_get_transmission(double *t)
 {
     Impl &I = *impl;
     I.p_valid = false; // T is formed in the work array
+    I.push_slot();
     k_fresnel_get_t<<<grid1(I.n), 256, 0, I.S.st>>>(I.x.p, I.ill.p, I.P.p, I.n);
+    if (I.h_slot.tc_on) k_tc_pixels<<<grid1(I.n), 256, 0, I.S.st>>>(I.P.p, I.n, I.slot.p);
     I.get_panel(I.P.p, 2, t);
 }
 

@@ -23,6 +23,14 @@ public:
     void fresnel_initialise(const double *t);
     void fresnel_set_transmission(const double *t);
     void fresnel_get_transmission(double *t);
+    // TransmissionConstraint's per-pixel part (charge flipping, unit
+    // magnitude) inside the row pass's support projections
+    void set_constraint(bool on, bool unity, bool flip, int flip_sign);
+    bool constrained() const;
+    // the result a PhaseDiverseCDI exchanges (Fresnel: the transmission
+    // function; else the estimate), natural order, double, on the device
+    void transmission_to_device(double2 *dst);
+    void transmission_from_device(const double2 *src);
     void get_illumination_at_sample(double *h);
     void set_x(const double *h);
     void get_x(double *h);

@@ -39,6 +39,13 @@ struct alignas(64) Slot {
     float s0;               // 1/sqrt(nx*ny)
     double inv_norm2;       // 1 / sum of sqrt(I)^2 over measured pixels
     int *flag;              // raised when a device-side wait gives up
+    // TransmissionConstraint's per-pixel part (charge flipping, unit
+    // magnitude) applied in each support projection of the row pass (the
+    // non-persistent variants); for FresnelCDI on the transmission function,
+    // with tc_ill the illumination at the sample (else null)
+    int tc_on, tc_unity, tc_flip;
+    float tc_sign;
+    const float2 *tc_ill;
     // PolyCDI: P is the padded mx x my grid (the estimate sits at rows
     // px..px+nx-1, columns py..py+ny-1); q holds |Psi|^2 of the padded
     // detector field in centred coordinates (panel layout over mx rows);
@@ -50,6 +57,27 @@ struct alignas(64) Slot {
     const float *wl;
     int nl, px, py, mx, my;
 };
+
+#ifdef __CUDACC__
+// TransmissionConstraint::apply_constraint's per-pixel part
+// (TransmissionConstraint.c++:136-160): charge flipping, then unit magnitude
+// judged on the magnitude before the flip
+__device__ __forceinline__ float2 tc_pixel(float2 v, const Slot &S)
+{
+    const float mag_old = sqrtf(v.x * v.x + v.y * v.y);
+    if (S.tc_flip && S.tc_sign * v.y > 0.f) v.y = -1.f * v.y;
+    if (S.tc_unity && mag_old > 1.f) {
+        const float m = sqrtf(v.x * v.x + v.y * v.y);
+        if (m == 0.f) {
+            v = make_float2(1.f, 0.f);
+        } else {
+            const float q = 1.f / m;
+            v = make_float2(v.x * q, v.y * q);
+        }
+    }
+    return v;
+}
+#endif
 
 struct Gauss {
     float w[6];
@@ -116,7 +144,9 @@ struct Choice {
     const TileVariant *col = nullptr, *row = nullptr;
     float col_us = 0, row_us = 0;
 };
-const Choice &choose(int nx, int ny, bool fresnel, int nslots);
+// plain_rows: only row variants that are not persistent (the ones that
+// carry the transmission constraint)
+const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows = false);
 
 const float2 *twiddle_table(int n);
 int sm_count();

@@ -104,6 +104,27 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_col(const Slot *const *slots
 
 // ----------------------------------------------------------------- row pass
 
+// the constraint on a support-projected value z at panel address a, column
+// yy: on z itself, or for FresnelCDI on its transmission function
+// T = (z + L) / L (FresnelCDI::apply_support, FresnelCDI.c++:203-215), written
+// back as L T - L for columns below nx (set_transmission_function's bound)
+__device__ __forceinline__ float2 tc_apply(float2 z, const Slot &S, size_t a, int yy, int nx,
+                                           int ny)
+{
+    if (!S.tc_ill) return tc_pixel(z, S);
+    if (ny >= nx && yy >= nx) return z;
+    const float2 l = S.tc_ill[a];
+    const float denom = l.x * l.x + l.y * l.y;
+    float2 t = make_float2(1.f, 0.f);
+    if (denom != 0.f) {
+        const float rn = l.x * (z.x + l.x) + l.y * (z.y + l.y);
+        const float in = l.x * (z.y + l.y) - l.y * (z.x + l.x);
+        t = make_float2(rn / denom, in / denom);
+    }
+    t = tc_pixel(t, S);
+    return make_float2(l.x * t.x - l.y * t.y - l.x, l.x * t.y + l.y * t.x - l.y);
+}
+
 
 template <class C, int MODE>
 __global__ void __launch_bounds__(C::NT, C::MINB) k_row(const Slot *const *slots, int nx, int ny,
@@ -141,6 +162,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_row(const Slot *const *slots
         const float *__restrict__ sup = S.sup;
         const float wid = S.w_id, wpf = S.w_pf, wps = S.w_ps, wpsf = S.w_psf;
         const bool er = S.er;
+        const bool tc = S.tc_on != 0;
         for_each_slot<C, false, false>([&](int e, int s, int pos) {
             const size_t a = paddr(i0 + s, pos, nx);
             const float f = support_factor(__ldg(&sup[a]));
@@ -148,10 +170,16 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_row(const Slot *const *slots
             float2 xn;
             if (er) {
                 xn = cscale(y, f);
+                if (tc) xn = tc_apply(xn, S, a, pos, nx, ny);
             } else {
                 const float2 xk = x[a];
-                xn = make_float2(wid * xk.x + wpf * y.x + wps * (f * xk.x) + wpsf * (f * y.x),
-                                 wid * xk.y + wpf * y.y + wps * (f * xk.y) + wpsf * (f * y.y));
+                float2 ps = make_float2(f * xk.x, f * xk.y), psf = make_float2(f * y.x, f * y.y);
+                if (tc) {
+                    ps = tc_apply(ps, S, a, pos, nx, ny);
+                    psf = tc_apply(psf, S, a, pos, nx, ny);
+                }
+                xn = make_float2(wid * xk.x + wpf * y.x + wps * ps.x + wpsf * psf.x,
+                                 wid * xk.y + wpf * y.y + wps * ps.y + wpsf * psf.y);
             }
             x[a] = xn;
             v[e] = xn;

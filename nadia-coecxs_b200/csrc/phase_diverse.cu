@@ -428,8 +428,8 @@ void PhaseDiverse::add_position(Solver *f, double x, double y, double a)
 {
     AllocScope scope(st);
     NADIA_REQUIRE(f, NADIA_ERR_INVALID, "null frame");
-    NADIA_REQUIRE(f->prec == NADIA_FP64, NADIA_ERR_UNSUPPORTED,
-                  "phase-diverse frames run in the FP64 form");
+    NADIA_REQUIRE(f->prec == NADIA_FP64 || f->kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
+                  "PolyCDI phase-diverse frames run in the FP64 form");
     NADIA_REQUIRE(f->device == device, NADIA_ERR_INVALID,
                   "the frame lives on another device than the phase-diverse object");
     weights_set = false;
@@ -846,8 +846,17 @@ void PhaseDiverse::adjust_positions(int type, bool forward, int min_x, int max_x
             Solver *f = frames[n];
             to_object(n); // the frame's support
             const double *single_img = single.p;
+            DevBuf<double> fsup;
+            const double *fsupport = f->support.p;
+            if (f->prec != NADIA_FP64) { // the FP32 form keeps its support in its own layout
+                std::vector<double> h(f->n);
+                f->get_support(h.data());
+                fsup.alloc(f->n);
+                h2d_sync(fsup.p, h.data(), f->n * sizeof(double), st);
+                fsupport = fsup.p;
+            }
             if (sc == 1) {
-                NADIA_CUDA(cudaMemcpyAsync(weight_int.p, f->support.p,
+                NADIA_CUDA(cudaMemcpyAsync(weight_int.p, fsupport,
                                            std::min(weight_int.bytes(), f->n * sizeof(double)),
                                            cudaMemcpyDeviceToDevice, st));
             } else {
@@ -858,7 +867,7 @@ void PhaseDiverse::adjust_positions(int type, bool forward, int min_x, int max_x
                         single.p, lnx, lny, single_int.p, sc);
                 if (f->nx > 2 && f->ny > 2 && f->nx * sc == bnx && f->ny * sc == bny)
                     k_interpolate<<<grid_for((size_t)(f->nx - 2) * (f->ny - 2)), kThreads, 0, st>>>(
-                        f->support.p, f->nx, f->ny, weight_int.p, sc);
+                        fsupport, f->nx, f->ny, weight_int.p, sc);
                 NADIA_CUDA(cudaGetLastError());
                 single_img = single_int.p;
             }

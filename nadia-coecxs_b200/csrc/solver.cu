@@ -378,10 +378,24 @@ void Solver::set_transmission_constraint(int unity, int flip, int flip_sign, int
                                          const double *fixed_c)
 {
     AllocScope scope(st);
-    NADIA_REQUIRE(prec == NADIA_FP64, NADIA_ERR_UNSUPPORTED,
-                  "transmission constraints run in the FP64 form");
     NADIA_REQUIRE(nregions >= 0 && nregions <= plain::kMaxRegions, NADIA_ERR_INVALID,
                   "between 0 and 16 complex-constraint regions");
+    if (prec == NADIA_FP32) {
+        // the per-pixel part runs inside the fused row pass; regions need
+        // whole-image sums between the projection and its update
+        NADIA_REQUIRE(nregions == 0 && kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
+                      "complex-constraint regions (and PolyCDI constraints) run in the FP64 "
+                      "form: convert the reconstruction first");
+        f32->set_constraint(true, unity != 0, flip != 0, flip_sign);
+        tc.active = true;
+        tc.unity = unity ? 1 : 0;
+        tc.flip = flip ? 1 : 0;
+        tc.flip_sign = flip_sign > 0 ? 1 : -1;
+        tc.nregions = 0;
+        tc.custom = nullptr;
+        tc.user = nullptr;
+        return;
+    }
     NADIA_REQUIRE(nregions == 0 || (regions && alpha), NADIA_ERR_INVALID,
                   "complex-constraint regions need their masks and alphas");
     NADIA_CUDA(cudaStreamSynchronize(st)); // buffers of an earlier constraint may be replaced
@@ -413,6 +427,9 @@ void Solver::set_transmission_constraint(int unity, int flip, int flip_sign, int
 void Solver::set_transmission_custom(void (*fn)(double *, int, int, void *), void *user)
 {
     NADIA_REQUIRE(tc.active, NADIA_ERR_STATE, "set a transmission constraint first");
+    NADIA_REQUIRE(!fn || prec == NADIA_FP64, NADIA_ERR_UNSUPPORTED,
+                  "a custom constraint function runs in the FP64 form: convert the "
+                  "reconstruction first");
     tc.custom = fn;
     tc.user = user;
 }
@@ -420,6 +437,7 @@ void Solver::set_transmission_custom(void (*fn)(double *, int, int, void *), voi
 void Solver::clear_transmission_constraint()
 {
     NADIA_CUDA(cudaStreamSynchronize(st));
+    if (prec == NADIA_FP32 && tc.active) f32->set_constraint(false, false, false, 1);
     tc.active = false;
     tc.custom = nullptr;
     tc.user = nullptr;
@@ -692,8 +710,12 @@ void Solver::get_transmission(double *h)
 void Solver::transmission_to_device(double2 *dst)
 {
     AllocScope scope(st);
-    NADIA_REQUIRE(prec == NADIA_FP64, NADIA_ERR_UNSUPPORTED,
-                  "phase-diverse frames run in the FP64 form");
+    if (prec == NADIA_FP32) {
+        NADIA_REQUIRE(kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
+                      "PolyCDI phase-diverse frames run in the FP64 form");
+        f32->transmission_to_device(dst);
+        return;
+    }
     if (kind == NADIA_FRESNEL) {
         plain::fresnel_get_transmission(x.p, illum_sample.p, dst, n, st);
         if (tc.active) apply_transmission_constraint(dst); // FresnelCDI.c++:352-353
@@ -705,8 +727,12 @@ void Solver::transmission_to_device(double2 *dst)
 void Solver::transmission_from_device(const double2 *src)
 {
     AllocScope scope(st);
-    NADIA_REQUIRE(prec == NADIA_FP64, NADIA_ERR_UNSUPPORTED,
-                  "phase-diverse frames run in the FP64 form");
+    if (prec == NADIA_FP32) {
+        NADIA_REQUIRE(kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
+                      "PolyCDI phase-diverse frames run in the FP64 form");
+        f32->transmission_from_device(src);
+        return;
+    }
     if (kind == NADIA_FRESNEL)
         plain::fresnel_set_transmission(src, illum_sample.p, x.p, nx, ny, st);
     else
@@ -730,6 +756,9 @@ void Solver::convert_to_fp64()
     }
     forget_batches_with(uid); // batch plans hold FP32 handles only
     NADIA_CUDA(cudaStreamSynchronize(st));
+    const bool had_tc = tc.active;
+    const int tcu = tc.unity, tcf = tc.flip, tcs = tc.flip_sign;
+    tc.active = false;
     f32.reset();
     best32.clear();
     prec = NADIA_FP64;
@@ -769,6 +798,7 @@ void Solver::convert_to_fp64()
         isc.alloc(n);
         fft_pad.init(nx + 2 * px, ny + 2 * py);
     }
+    if (had_tc) set_transmission_constraint(tcu, tcf, tcs, 0, nullptr, nullptr, nullptr);
     NADIA_CUDA(cudaStreamSynchronize(st));
 }
 

@@ -126,9 +126,11 @@ def test_transmission_custom_function():
 
 
 def test_transmission_constraint_refusals():
+    # the FP32 form takes the per-pixel part only: regions need the FP64 form
     s = pynadia.Solver("planar", 256, 256, precision=pynadia.FP32)
+    regions, alphas, fixed = sc.constraint_regions(256)
     with pytest.raises(pynadia.NadiaError) as e:
-        s.set_transmission_constraint(True, True)
+        s.set_transmission_constraint(True, True, 1, regions, alphas, fixed)
     assert e.value.code == 3
     s = gpu("planar", 32, 32)
     with pytest.raises(pynadia.NadiaError) as e:   # a custom function needs a constraint
