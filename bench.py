@@ -443,12 +443,10 @@ def constraint_report(pynadia, synth, n=2048, iters=50, modes=("none", "pixel", 
                       cpu=True):
     """TransmissionConstraint (charge flipping, unit magnitude, and three
     complex-constraint regions) on a PlanarCDI HIO reconstruction of 2048^2 in
-    the FP64 form: device time per iteration without the constraint, with the
-    per-pixel part, and with regions (CUDA events on the handle's stream).
-    The constraint runs once per support projection, i.e. twice per HIO
-    iteration.  Algorithmic bytes per pixel and application: per-pixel part
-    read + write of the field (32); with regions also the region map on both
-    kernels and the field once more for the region sums (16 + 4 + 4 = 24 more).
+    the FP64 form (without, with the per-pixel part, with regions) and the
+    FP32 form (without, with the per-pixel part inside its fused row pass):
+    device time per iteration, CUDA events on the handle's stream.  The
+    constraint runs in each support projection, twice per HIO iteration.
     The reference's float build is timed for one iteration of each on one
     host core."""
     import torch
@@ -480,9 +478,32 @@ def constraint_report(pynadia, synth, n=2048, iters=50, modes=("none", "pixel", 
         b.synchronize()
         ms[mode] = a.elapsed_time(b) / iters
         s.close()
-    peak, _ = measured_peak()
-    px = n * n
     out["gpu_fp64_ms_per_iteration"] = ms
+    # the per-pixel part inside the FP32 fused row pass
+    ms32 = {}
+    for mode in ("none", "pixel"):
+        if mode not in modes:
+            continue
+        s = pynadia.Solver("planar", n, n, precision=pynadia.FP32)
+        setup(s, mode)
+        s.iterate(3)
+        s.synchronize()
+        st = torch.cuda.ExternalStream(s.stream())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s.iterate(iters)
+        b.record(st)
+        b.synchronize()
+        ms32[mode] = a.elapsed_time(b) / iters
+        s.close()
+    if ms32:
+        out["gpu_fp32_ms_per_iteration"] = ms32
+    # without a constraint the FP64 form forms the support projections inside
+    # its combine; with one it projects, constrains and combines separately,
+    # so the differences below are the whole cost of the constraint
+    if "none" in ms:
+        out["fp64_constraint_cost_ms_per_iteration"] = {
+            m: ms[m] - ms["none"] for m in ms if m != "none"}
     for mode, bpp in (("pixel", 32.0), ("regions", 56.0)):
         if mode not in ms or "none" not in ms:
             continue
@@ -537,8 +558,8 @@ def phase_diverse_report(pynadia, synth, n=1024, cycles=15, cpu=True, search=Tru
     1024^2 at the example's positions, wavelength, pixel size and distances,
     each with the default transmission constraint (unit magnitude, charge
     flipping), series mode, cross-correlation position search before cycle 0
-    and minimum-error search before cycle 10, 15 cycles.  Frames run in the
-    FP64 form (PhaseDiverseCDI's form).  The calls are synchronous, so the
+    and minimum-error search before cycle 10, 15 cycles, with FP64 frames and
+    again with FP32 frames (the object is FP64 in both).  The calls are synchronous, so the
     times are host wall times around them.  The reference's float build is
     timed for one cycle on one host core."""
     import numpy as np
@@ -562,8 +583,10 @@ def phase_diverse_report(pynadia, synth, n=1024, cycles=15, cpu=True, search=Tru
             out.append(f)
         return out
 
+    prec = [pynadia.FP64]
+
     def gpu_make(kind, nx, ny, **kw):
-        return pynadia.Solver(kind, nx, ny, precision=pynadia.FP64, **kw)
+        return pynadia.Solver(kind, nx, ny, precision=prec[0], **kw)
 
     def run(frames, pd, search=True, n_cycles=cycles):
         for k, f in enumerate(frames):
@@ -604,6 +627,21 @@ def phase_diverse_report(pynadia, synth, n=1024, cycles=15, cpu=True, search=Tru
     pd.close()
     for f in frames:
         f.close()
+    # the same with FP32 frames (the float build's form; the object stays FP64)
+    prec[0] = pynadia.FP32
+    frames = frames_on(gpu_make)
+    run(frames, pynadia.PhaseDiverse(), search=False, n_cycles=1)
+    frames = frames_on(gpu_make)
+    pd = pynadia.PhaseDiverse()
+    t = time.perf_counter()
+    run(frames, pd, search=search)
+    out["gpu_fp32_frames_s_per_reconstruction"] = time.perf_counter() - t
+    t = time.perf_counter()
+    pd.iterate(5)
+    out["gpu_fp32_frames_ms_per_cycle"] = 1000.0 * (time.perf_counter() - t) / 5
+    pd.close()
+    for f in frames:
+        f.close()
     sys.path.insert(0, ORACLE)
     import pyoracle as po
     if cpu and po.reference_available("32_fast"):
@@ -619,6 +657,7 @@ def phase_diverse_report(pynadia, synth, n=1024, cycles=15, cpu=True, search=Tru
             cpu = time.perf_counter() - t
         out["cpu_reference_float_s_per_cycle_one_core"] = cpu
         out["gpu_over_cpu_per_cycle"] = cpu / per_cycle
+        out["gpu_fp32_frames_over_cpu_per_cycle"] = cpu / (out["gpu_fp32_frames_ms_per_cycle"] / 1000.0)
     return out
 
 
