@@ -726,20 +726,23 @@ bool Fused32::Impl::push_slot_async(cudaStream_t st)
 void Fused32::Impl::put_panel_f(const float *h, int stride, void *dst, bool fold)
 {
     std::vector<float> p(n * stride);
-    for (int ky = 0; ky < ny; ++ky) {
-        int dy = ky;
+    // x outer, y inner: the source is read in order, and the panel rows a
+    // column writes (16 bytes each) are the next column's neighbours
+    for (int kx = 0; kx < nx; ++kx) {
+        int dx = kx;
         if (fold) {
-            dy = ky + ny / 2;
-            dy = dy >= ny ? dy - ny : dy;
+            dx = kx + nx / 2;
+            dx = dx >= nx ? dx - nx : dx;
         }
-        for (int kx = 0; kx < nx; ++kx) {
-            int dx = kx;
+        const float *src = h + (size_t)dx * ny * stride;
+        for (int ky = 0; ky < ny; ++ky) {
+            int dy = ky;
             if (fold) {
-                dx = kx + nx / 2;
-                dx = dx >= nx ? dx - nx : dx;
+                dy = ky + ny / 2;
+                dy = dy >= ny ? dy - ny : dy;
             }
-            const size_t a = panel_index_dev(kx, ky, nx), d = (size_t)dx * ny + dy;
-            for (int c = 0; c < stride; ++c) p[a * stride + c] = h[d * stride + c];
+            const size_t a = panel_index_dev(kx, ky, nx);
+            for (int c = 0; c < stride; ++c) p[a * stride + c] = src[(size_t)dy * stride + c];
         }
     }
     NADIA_CUDA(cudaMemcpyAsync(dst, p.data(), n * stride * sizeof(float), cudaMemcpyHostToDevice,
