@@ -504,15 +504,6 @@ def constraint_report(pynadia, synth, n=2048, iters=50, modes=("none", "pixel", 
     if "none" in ms:
         out["fp64_constraint_cost_ms_per_iteration"] = {
             m: ms[m] - ms["none"] for m in ms if m != "none"}
-    for mode, bpp in (("pixel", 32.0), ("regions", 56.0)):
-        if mode not in ms or "none" not in ms:
-            continue
-        extra = (ms[mode] - ms["none"]) / 2 / 1000.0  # seconds per application
-        if extra > 0:
-            gbs = bpp * px / extra / 1e9
-            out[mode + "_constraint"] = {"us_per_application": extra * 1e6,
-                                         "algorithmic_bytes_per_pixel": bpp,
-                                         "hbm_gbs_algorithmic": gbs, "roofline_frac": gbs / peak}
     sys.path.insert(0, ORACLE)
     import pyoracle as po
     if cpu and po.reference_available("32_fast"):
