@@ -41,13 +41,15 @@ class CliCase:
     """kind: planar, fresnel_wf, fresnel or poly; n: grid side."""
 
     def __init__(self, kind, n, directory, stages=None, output_iterations=10,
-                 shrinkwrap_iterations=12, info_level=0, prefix=None, starting_point=None):
+                 shrinkwrap_iterations=12, info_level=0, prefix=None, starting_point=None,
+                 diffraction=False):
         self.kind, self.n, self.dir = kind, n, str(directory)
         self.output_iterations = output_iterations
         self.shrinkwrap = shrinkwrap_iterations
         self.gauss_width, self.threshold = 1.5, 0.1
         self.prefix = prefix or (kind + "_out")
         self.starting_point = starting_point
+        self.diffraction = diffraction
         self.stages = stages or [("ER", 4), ("HIO", 20), ("RAAR", 8), ("ER", 3)]
         self.kw = {}
         os.makedirs(self.dir, exist_ok=True)
@@ -102,6 +104,9 @@ class CliCase:
                     shrinkwrap_threshold=self.threshold, info_level=info_level)
         if starting_point:
             keys["starting_point_file_name"] = starting_point
+        if diffraction:
+            keys["output_diffraction_estimate"] = 1
+            keys["use_log_scale_for_diffraction"] = 1
         self.config = self.path(self.prefix + ".config")
         with open(self.config, "w") as fh:
             fh.write("# %s reconstruction\n" % kind)
@@ -120,6 +125,11 @@ class CliCase:
         oi = self.output_iterations
         return {i: "%s_%d.ppm" % (self.prefix, i) for i in range(total) if oi and i % oi == 0}
 
+    def diffraction_names(self):
+        """The tool's names for the diffraction images (the reference's tool
+        appends them to the magnitude image's name instead)."""
+        return {i: "%s_diffraction_%d.ppm" % (self.prefix, i) for i in self.image_names()}
+
     def expected(self, seed, make=po.Oracle):
         n = self.n
         s = make(self.kind, n, n, **self.kw)
@@ -131,7 +141,7 @@ class CliCase:
             s.set_exit_surface_wave(read_cplx(self.path(self.starting_point), n, n))
         else:
             s.initialise_estimate(seed)
-        images, i = {}, 0
+        images, diffraction, i = {}, {}, 0
         oi, k = self.output_iterations, self.shrinkwrap
         for alg, count in self.stages:
             if self.kind != "fresnel_wf":
@@ -140,10 +150,13 @@ class CliCase:
                 s.iterate()
                 if oi and i % oi == 0:
                     images[i] = magnitude(s.get_exit_surface_wave())
+                    if self.diffraction:
+                        m = magnitude(s.propagate_to_detector(s.get_exit_surface_wave()))
+                        diffraction[i] = m * m
                 if k and i % k == k - 1:
                     s.apply_shrinkwrap(self.gauss_width, self.threshold)
                 i += 1
-        out = {"final": s.get_exit_surface_wave(), "images": images}
+        out = {"final": s.get_exit_surface_wave(), "images": images, "diffraction": diffraction}
         if self.kind == "fresnel":
             out["transmission"] = s.get_transmission()
         return out

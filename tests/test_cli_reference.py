@@ -34,14 +34,14 @@ def ppm_writer(tmp_path_factory):
     L.shim_write_ppm.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, D, ctypes.c_int,
                                  ctypes.c_double, ctypes.c_double]
 
-    def write(directory, name, img):
+    def write(directory, name, img, log_scale=False):
         os.makedirs(directory, exist_ok=True)
         a = np.ascontiguousarray(img, dtype=np.float64)
         cwd = os.getcwd()
         os.chdir(directory)
         try:
             assert L.shim_write_ppm(name.encode(), a.shape[0], a.shape[1], a.ctypes.data_as(D),
-                                    0, 0.0, 0.0) == 1
+                                    1 if log_scale else 0, 0.0, 0.0) == 1
         finally:
             os.chdir(cwd)
         with open(os.path.join(directory, name), "rb") as fh:
@@ -70,6 +70,11 @@ def check_outputs(case, seed, ppm_writer, exp=None):
     if case.kind == "fresnel":
         t = cc.read_cplx(case.path("transmission_function.cplx"), n, n)
         assert np.array_equal(t, exp["transmission"])
+    if case.diffraction:
+        for i, name in case.diffraction_names().items():
+            want = ppm_writer(case.path("expected"), name, exp["diffraction"][i], True)
+            with open(case.path(name), "rb") as fh:
+                assert fh.read() == want, name
 
 
 @pytest.mark.parametrize("kind,n", [("planar", 64), ("planar", 40), ("fresnel_wf", 32),

@@ -37,6 +37,15 @@ def test_double_build_matches_oracle(tmp_path, tools, ppm_writer, kind, n):
     check_outputs(case, 3, ppm_writer)
 
 
+@pytest.mark.parametrize("kind", ["planar", "fresnel"])
+def test_double_build_diffraction_images(tmp_path, tools, ppm_writer, kind):
+    """output_diffraction_estimate: |propagate_to_detector(estimate)|^2 on a
+    log scale every output_iterations, bit for bit."""
+    case = cc.CliCase(kind, 32, tmp_path / kind, diffraction=True, output_iterations=7)
+    run_tool(tools["double"], case, seed=4)
+    check_outputs(case, 4, ppm_writer)
+
+
 def test_double_build_iteration_by_iteration(tmp_path, tools, ppm_writer):
     """info_level 2 runs and prints every iteration on its own; the files are
     the same as those of the chunked run."""
