@@ -105,59 +105,85 @@ __global__ void k_blur_x(const float *in, float *out, int nx, int ny, Gauss g, f
 // |x| (or a real input) blurred by the truncated Gaussian over one 32x32 tile
 // of the grid, from a 40x40 halo tile in shared memory (rows then columns);
 // writes the blurred values and the tile maximum.  Panel layout in and out.
+// CUT > 0 fixes the cut-off at compile time (apply_shrinkwrap's 4): the taps
+// unroll and the weights stay in registers; CUT = 0 reads it from g.
+// Launched with kSwThreads threads (block 32 x 8); every loop has a fixed
+// trip count, so a thread issues all its halo loads before it uses one.
+// Row strides of 44 and 36 words put the 8 rows x 4 panel columns that a
+// warp touches in the halo and column phases on 32 different banks.
 constexpr int kSwTile = 32;
-template <bool CPLX>
-__global__ void k_blur_tiles(const void *in, float *out, int nx, int ny, Gauss g, float *maxpart)
+constexpr int kSwThreads = 256;
+template <bool CPLX, int CUT>
+__global__ void __launch_bounds__(kSwThreads) k_blur_tiles(const void *in, float *out, int nx,
+                                                           int ny, Gauss g, float *maxpart)
 {
+    static_assert(CUT >= 0 && CUT <= 4, "the halo holds a cut-off of at most 4");
     constexpr int H = kSwTile + 8; // cut-off up to 4 on each side
-    __shared__ float tile[H][H + 1];
-    __shared__ float rows[H][kSwTile + 1];
-    const int cut = g.cut;
+    constexpr int NT = kSwThreads;
+    __shared__ float tile[H][H + 4];
+    __shared__ float rows[H][kSwTile + 4];
+    const int cut = CUT > 0 ? CUT : g.cut;
     const int i0 = blockIdx.y * kSwTile - 4, j0 = blockIdx.x * kSwTile - 4;
-    const int t = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
     // halo: panel-major so that each panel's rows are one contiguous run
-    for (int e = t; e < H * H; e += nt) {
-        const int jj = e % kPanel, a = (e / kPanel) % H, pb = e / (kPanel * H);
-        const int i = i0 + a, j = j0 + pb * kPanel + jj;
-        float v = 0.f;
-        if (i >= 0 && i < nx && j >= 0 && j < ny) {
-            const size_t ad = paddr(i, j, nx);
-            if (CPLX) {
-                const float2 c = __ldg(&((const float2 *)in)[ad]);
-                v = sqrtf(c.x * c.x + c.y * c.y);
-            } else {
-                v = __ldg(&((const float *)in)[ad]);
+#pragma unroll
+    for (int k = 0; k < (H * H + NT - 1) / NT; ++k) {
+        const int e = t + k * NT;
+        if (e < H * H) {
+            const int jj = e % kPanel, a = (e / kPanel) % H, pb = e / (kPanel * H);
+            const int i = i0 + a, j = j0 + pb * kPanel + jj;
+            float v = 0.f;
+            if (i >= 0 && i < nx && j >= 0 && j < ny) {
+                const size_t ad = paddr(i, j, nx);
+                if (CPLX) {
+                    const float2 c = __ldg(&((const float2 *)in)[ad]);
+                    v = sqrtf(c.x * c.x + c.y * c.y);
+                } else {
+                    v = __ldg(&((const float *)in)[ad]);
+                }
             }
+            tile[a][pb * kPanel + jj] = v;
         }
-        tile[a][pb * kPanel + jj] = v;
     }
     __syncthreads();
-    for (int e = t; e < H * kSwTile; e += nt) {
+    static_assert(H * kSwTile % NT == 0 && kSwTile * kSwTile % NT == 0, "whole rounds");
+#pragma unroll
+    for (int k = 0; k < H * kSwTile / NT; ++k) {
+        const int e = t + k * NT;
         const int a = e / kSwTile, b = e % kSwTile;
         float acc = 0.f;
+#pragma unroll
         for (int d = -cut; d <= cut; ++d) acc += g.w[d < 0 ? -d : d] * tile[a][b + 4 + d];
         rows[a][b] = acc;
     }
     __syncthreads();
     float m = -INFINITY;
-    for (int e = t; e < kSwTile * kSwTile; e += nt) {
+#pragma unroll
+    for (int k = 0; k < kSwTile * kSwTile / NT; ++k) {
+        const int e = t + k * NT;
         const int jj = e % kPanel, a = (e / kPanel) % kSwTile, pb = e / (kPanel * kSwTile);
         const int b = pb * kPanel + jj;
         const int i = blockIdx.y * kSwTile + a, j = blockIdx.x * kSwTile + b;
-        if (i >= nx || j >= ny) continue;
-        float acc = 0.f;
-        for (int d = -cut; d <= cut; ++d) acc += g.w[d < 0 ? -d : d] * rows[a + 4 + d][b];
-        out[paddr(i, j, nx)] = acc;
-        m = fmaxf(m, acc);
+        if (i < nx && j < ny) {
+            float acc = 0.f;
+#pragma unroll
+            for (int d = -cut; d <= cut; ++d) acc += g.w[d < 0 ? -d : d] * rows[a + 4 + d][b];
+            out[paddr(i, j, nx)] = acc;
+            m = fmaxf(m, acc);
+        }
     }
-    __shared__ float red[256];
-    red[t] = m;
+    // block maximum: warps by shuffles, then the 8 warp maxima
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+    __shared__ float red[NT / 32];
+    if ((t & 31) == 0) red[t >> 5] = m;
     __syncthreads();
-    for (int off = 128; off > 0; off >>= 1) {
-        if (t < off) red[t] = fmaxf(red[t], red[t + off]);
-        __syncthreads();
+    if (t == 0) {
+        float r = red[0];
+#pragma unroll
+        for (int w = 1; w < NT / 32; ++w) r = fmaxf(r, red[w]);
+        maxpart[blockIdx.y * gridDim.x + blockIdx.x] = r;
     }
-    if (t == 0) maxpart[blockIdx.y * gridDim.x + blockIdx.x] = red[0];
 }
 
 // Square grids visit every element once in apply_threshold, so the values
@@ -1082,11 +1108,14 @@ void Fused32::Impl::blur(bool cplx, const void *in, double gauss_width, int cut)
         maxpart.alloc(std::max(nb, (int)kMaxBlocks) + 2);
     }
     if (cut <= 4) {
-        dim3 grid((ny + kSwTile - 1) / kSwTile, (nx + kSwTile - 1) / kSwTile), block(32, 8);
-        if (cplx)
-            k_blur_tiles<true><<<grid, block, 0, S.st>>>(in, tmp2.p, nx, ny, g, maxpart.p);
+        dim3 grid((ny + kSwTile - 1) / kSwTile, (nx + kSwTile - 1) / kSwTile),
+            block(32, kSwThreads / 32);
+        if (cplx && cut == 4)
+            k_blur_tiles<true, 4><<<grid, block, 0, S.st>>>(in, tmp2.p, nx, ny, g, maxpart.p);
+        else if (cplx)
+            k_blur_tiles<true, 0><<<grid, block, 0, S.st>>>(in, tmp2.p, nx, ny, g, maxpart.p);
         else
-            k_blur_tiles<false><<<grid, block, 0, S.st>>>(in, tmp2.p, nx, ny, g, maxpart.p);
+            k_blur_tiles<false, 0><<<grid, block, 0, S.st>>>(in, tmp2.p, nx, ny, g, maxpart.p);
         k_max_final<<<1, 256, 0, S.st>>>(maxpart.p, nb);
         g_launches += 2;
         return;
