@@ -578,7 +578,6 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
         NADIA_CUDA(cudaMemsetAsync(tx.p, 0, tx.bytes(), st));
         NADIA_CUDA(cudaMemsetAsync(ty.p, 0, ty.bytes(), st));
         NADIA_CUDA(cudaMemsetAsync(iter.p, 0, iter.bytes(), st));
-    NADIA_CUDA(cudaMemsetAsync(flag.p, 0, flag.bytes(), st));
         for (int i = 0; i < ns; ++i) {
             P[i].alloc(n); X[i].alloc(n); sup[i].alloc(n); mI[i].alloc(n);
             NADIA_CUDA(cudaMemsetAsync(P[i].p, 0, P[i].bytes(), st));
