@@ -84,14 +84,14 @@ def _cpu_worker(args):
     """One reference-code reconstruction stream on one core: time `iters`
     HIO iterations at 2048^2 (plus one shrinkwrap), return seconds/iteration
     and seconds/shrinkwrap."""
-    libkind, iters = args
+    libkind, iters, variant = args
     sys.path[:0] = [ORACLE, PKG]
     import numpy as np
     import pyoracle as po
     from pynadia import synth
     c = synth.planar_case("c3")
     if libkind == "reference":
-        s = po.Reference("planar", N, N, variant="32_fast")
+        s = po.Reference("planar", N, N, variant=variant)
     else:
         s = po.Oracle("planar", N, N)
     s.set_support(c.support)
@@ -117,8 +117,15 @@ def cpu_kind():
     return "port"
 
 
-def cpu_sample(procs, iters):
-    """Reconstructions/s of the reference CPU code on `procs` cores."""
+def reference_build_available(variant):
+    sys.path.insert(0, ORACLE)
+    import pyoracle as po
+    return po.reference_available(variant)
+
+
+def cpu_sample(procs, iters, variant="32_fast"):
+    """Reconstructions/s of the reference CPU code on `procs` cores
+    (variant "32_fast": the float build, "64_fast": the double build)."""
     kind = cpu_kind()
     if kind == "port":
         sys.path.insert(0, ORACLE)
@@ -127,15 +134,16 @@ def cpu_sample(procs, iters):
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
-        res = pool.map(_cpu_worker, [(kind, iters)] * procs)
+        res = pool.map(_cpu_worker, [(kind, iters, variant)] * procs)
     wall = time.perf_counter() - t0
     per_recon = [t_it * ITERS + t_sw * (ITERS // SW_EVERY) for t_it, t_sw in res]
     value = sum(1.0 / s for s in per_recon)
     desc = ("%d independent %dx%d HIO streams, %d timed iterations + 1 shrinkwrap each, "
             "extrapolated to %d iterations with shrinkwrap every %d; %s"
             % (procs, N, N, iters, ITERS, SW_EVERY,
-               "reference C++ float build (-O3 -ffast-math) + project FFTW-API shim "
-               "(FFTW unavailable)" if kind == "reference" else "oracle restatement (FP64)"))
+               "reference C++ %s build (-O3 -ffast-math) + project FFTW-API shim "
+               "(FFTW unavailable)" % ("double" if variant == "64_fast" else "float")
+               if kind == "reference" else "oracle restatement (FP64)"))
     return {"value": value, "unit": "recon/s", "cores": procs, "kind": kind, "sample": desc,
             "s_per_iteration": sum(r[0] for r in res) / len(res), "wall_s": wall}
 
@@ -913,6 +921,19 @@ def ours(args, rank, world, local_rank):
         if not args.no_cpu:
             procs = max(1, min(os.cpu_count() or 1, 8))
             cpu = cpu_sample(procs, iters=2)
+            if cpu["kind"] == "reference" and reference_build_available("64_fast"):
+                # the reference's double build (-DDOUBLE_PRECISION), the
+                # arithmetic of the FP64 form, on the same sample; an
+                # auxiliary figure, so a failure is reported, not raised
+                try:
+                    d = cpu_sample(procs, iters=1, variant="64_fast")
+                    cpu["double_build"] = {
+                        "value": d["value"], "unit": "recon/s", "cores": procs,
+                        "s_per_iteration": d["s_per_iteration"], "sample": d["sample"],
+                        "gpu_fp64_over_one_core":
+                            d["s_per_iteration"] / (fp64["ms_per_iteration"] / 1000.0)}
+                except Exception as e:  # noqa: BLE001
+                    cpu["double_build"] = {"error": repr(e)}
         step_ms_sorted = sorted(step_ms)
         line = {
             "metric": METRIC, "value": value, "unit": "recon/s", "n_gpus": world,
