@@ -84,7 +84,9 @@ def _cpu_worker(args):
     """One reference-code reconstruction stream on one core: time `iters`
     HIO iterations at 2048^2 (plus one shrinkwrap), return seconds/iteration
     and seconds/shrinkwrap."""
-    libkind, iters, variant = args
+    libkind, iters, variant, threads = args
+    # read by the threaded build when it plans its transforms
+    os.environ["NADIA_REF_FFT_THREADS"] = str(threads)
     sys.path[:0] = [ORACLE, PKG]
     import numpy as np
     import pyoracle as po
@@ -123,9 +125,10 @@ def reference_build_available(variant):
     return po.reference_available(variant)
 
 
-def cpu_sample(procs, iters, variant="32_fast"):
-    """Reconstructions/s of the reference CPU code on `procs` cores
-    (variant "32_fast": the float build, "64_fast": the double build)."""
+def cpu_sample(procs, iters, variant="32_fast", threads=1):
+    """Reconstructions/s of the reference CPU code in `procs` processes
+    (variant "32_fast": the float build, "64_fast": the double build,
+    "32_fast_mt": the float build with its FFTs on `threads` threads)."""
     kind = cpu_kind()
     if kind == "port":
         sys.path.insert(0, ORACLE)
@@ -134,15 +137,17 @@ def cpu_sample(procs, iters, variant="32_fast"):
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
-        res = pool.map(_cpu_worker, [(kind, iters, variant)] * procs)
+        res = pool.map(_cpu_worker, [(kind, iters, variant, threads)] * procs)
     wall = time.perf_counter() - t0
     per_recon = [t_it * ITERS + t_sw * (ITERS // SW_EVERY) for t_it, t_sw in res]
     value = sum(1.0 / s for s in per_recon)
     desc = ("%d independent %dx%d HIO streams, %d timed iterations + 1 shrinkwrap each, "
             "extrapolated to %d iterations with shrinkwrap every %d; %s"
             % (procs, N, N, iters, ITERS, SW_EVERY,
-               "reference C++ %s build (-O3 -ffast-math) + project FFTW-API shim "
-               "(FFTW unavailable)" % ("double" if variant == "64_fast" else "float")
+               "reference C++ %s build (-O3 -ffast-math%s) + project FFTW-API shim "
+               "(FFTW unavailable)" % ("double" if variant == "64_fast" else "float",
+                                       ", MULTI_THREADED, FFTs on %d threads" % threads
+                                       if variant.endswith("_mt") else "")
                if kind == "reference" else "oracle restatement (FP64)"))
     return {"value": value, "unit": "recon/s", "cores": procs, "kind": kind, "sample": desc,
             "s_per_iteration": sum(r[0] for r in res) / len(res), "wall_s": wall}
@@ -934,6 +939,17 @@ def ours(args, rank, world, local_rank):
                             d["s_per_iteration"] / (fp64["ms_per_iteration"] / 1000.0)}
                 except Exception as e:  # noqa: BLE001
                     cpu["double_build"] = {"error": repr(e)}
+            if cpu["kind"] == "reference" and reference_build_available("32_fast_mt"):
+                # one reconstruction with its FFTs on every host core (the
+                # reference's --enable-threads build); per-pixel loops stay serial
+                nth = os.cpu_count() or 1
+                try:
+                    d = cpu_sample(1, iters=2, variant="32_fast_mt", threads=nth)
+                    cpu["float_build_fft_threads"] = {
+                        "value": d["value"], "unit": "recon/s", "cores": nth,
+                        "s_per_iteration": d["s_per_iteration"], "sample": d["sample"]}
+                except Exception as e:  # noqa: BLE001
+                    cpu["float_build_fft_threads"] = {"error": repr(e)}
         step_ms_sorted = sorted(step_ms)
         line = {
             "metric": METRIC, "value": value, "unit": "recon/s", "n_gpus": world,

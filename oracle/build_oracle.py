@@ -113,6 +113,10 @@ def build_reference(force=False):
         "libnadia_ref64.so": ["-DDOUBLE_PRECISION", *PARITY_FLAGS],
         "libnadia_ref64_fast.so": ["-DDOUBLE_PRECISION", "-O3", "-ffast-math"],
         "libnadia_ref32_fast.so": ["-O3", "-ffast-math"],
+        # the reference's MULTI_THREADED float build (Complex_2D.c++:465-467):
+        # FFTs on NADIA_REF_FFT_THREADS threads, the rest of the loop serial
+        "libnadia_ref32_fast_mt.so": ["-O3", "-ffast-math", "-DMULTI_THREADED",
+                                      "-DNUM_THREADS=nadia_shim_env_threads()"],
     }
     srcs = [os.path.join(nadia, s) for s in REF_SOURCES]
     own = [os.path.join(HERE, f) for f in ("fftw_shim.c", "canon_fft.h", "ref_driver.cpp",
@@ -140,7 +144,7 @@ def build_reference(force=False):
         o = os.path.join(objdir, "fftw_shim.o")
         _run(["gcc", "-c", "-fPIC", "-w", *flags, os.path.join(HERE, "fftw_shim.c"), "-o", o])
         objs.append(o)
-        _run(["g++", "-shared", "-o", out, *objs, "-lm"])
+        _run(["g++", "-shared", "-o", out, *objs, "-lm", "-lpthread"])
     return outs
 
 
@@ -200,7 +204,7 @@ def build_reference_tools(force=False):
         _run(["ar", "rcs", lib, *objs])
     if force or _stale(cli, [os.path.join(nadia, s) for s in CLI_SOURCES] + own):
         objs = _objects(nadia, inc, CLI_SOURCES, os.path.join(REF_OUT, "obj_cli"), flags, own)
-        _run(["g++", "-o", cli, *objs, "-lm"])
+        _run(["g++", "-o", cli, *objs, "-lm", "-lpthread"])
     return {"io": lib, "cli": cli, "include": inc}
 
 

@@ -50,6 +50,10 @@ void fftwf_free(void *p);
 int fftwf_init_threads(void);
 void fftwf_plan_with_nthreads(int n);
 
+/* the FFT thread count for a build that passes it as NUM_THREADS:
+   NADIA_REF_FFT_THREADS from the environment, default 1 (not part of FFTW) */
+int nadia_shim_env_threads(void);
+
 #ifdef __cplusplus
 }
 #endif

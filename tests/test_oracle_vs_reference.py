@@ -122,3 +122,20 @@ def test_read_spec(tmp_path):
     assert got.shape == (3, 2)
     assert np.float32(got[0, 0]) == np.float32(1.0 / np.float32(1200))
     assert got[2, 1] == np.float32(2e15)
+
+
+@pytest.mark.skipif(not (po.reference_available("32_fast") and
+                         po.reference_available("32_fast_mt")),
+                    reason="timing builds of the reference not built")
+def test_threaded_fft_build_matches_serial_build(monkeypatch):
+    """The reference's MULTI_THREADED float build, whose FFTs the shim splits
+    over NADIA_REF_FFT_THREADS threads (the CPU baseline's --enable-threads
+    leg), gives the serial float build's results bit for bit: 40 rows over 5
+    threads, 56 columns in 4 blocks (the last one ragged) over 4 of them."""
+    monkeypatch.setenv("NADIA_REF_FFT_THREADS", "5")
+
+    def make(variant):
+        return lambda kind, nx, ny, **kw: po.Reference(kind, nx, ny, variant=variant, **kw)
+
+    same(sc.planar_mixed(make("32_fast"), n=40, ny=56, n_best=0),
+         sc.planar_mixed(make("32_fast_mt"), n=40, ny=56, n_best=0))
