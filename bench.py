@@ -119,6 +119,32 @@ def cpu_kind():
     return "port"
 
 
+def host_probe():
+    """The host the CPU legs ran on: core count, CPU model, and whether an
+    FFTW library is installed (the reference's FFT; when it is absent the
+    reference builds run their FFTs through the project's FFTW-API shim)."""
+    info = {"nproc": os.cpu_count()}
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    info["cpu_model"] = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        r = subprocess.run(["ldconfig", "-p"], capture_output=True, text=True, timeout=20)
+        # FFTW's own libraries (libfftw3, libfftw3f, ...), not cuFFTW
+        libs = sorted({ln.split()[0] for ln in r.stdout.splitlines()
+                       if ln.strip().startswith("libfftw3")})
+        info["fftw_libraries"] = libs
+        info["fftw"] = "installed (not linked: the timed builds use the shim)" if libs \
+            else "FFTW unavailable"
+    except (OSError, subprocess.SubprocessError) as e:
+        info["fftw"] = "probe failed: %r" % (e,)
+    return info
+
+
 def reference_build_available(variant):
     sys.path.insert(0, ORACLE)
     import pyoracle as po
@@ -926,6 +952,7 @@ def ours(args, rank, world, local_rank):
         if not args.no_cpu:
             procs = max(1, min(os.cpu_count() or 1, 8))
             cpu = cpu_sample(procs, iters=2)
+            cpu["host"] = host_probe()
             if cpu["kind"] == "reference" and reference_build_available("64_fast"):
                 # the reference's double build (-DDOUBLE_PRECISION), the
                 # arithmetic of the FP64 form, on the same sample; an
