@@ -1017,6 +1017,7 @@ def reference(args, rank, world):
         vals.append(info["value"])
     value = sum(vals) / len(vals)
     info["value"] = value
+    info["host"] = host_probe()
     return {"metric": METRIC, "value": value, "unit": "recon/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * info["wall_s"], "higher_is_better": True,
