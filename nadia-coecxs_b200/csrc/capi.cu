@@ -321,6 +321,7 @@ int nadia_get_exit_surface_wave_f32(nadia_solver *h, float *a)
 
 int nadia_iterate(nadia_solver *h, int iterations)
 {
+    nadia::Range range("nadia_iterate");
     return guard([&] { S(h).iterate(iterations); });
 }
 
@@ -336,6 +337,7 @@ int nadia_get_error_history(nadia_solver *h, double *e, int count)
 
 int nadia_apply_shrinkwrap(nadia_solver *h, double gauss_width, double threshold)
 {
+    nadia::Range range("nadia_apply_shrinkwrap");
     return guard([&] { S(h).apply_shrinkwrap(gauss_width, threshold); });
 }
 
@@ -609,6 +611,7 @@ int nadia_pd_get_position(const nadia_phase_diverse *h, int n_probe, double *x, 
 
 extern "C" int nadia_iterate_many(nadia_solver *const *solvers, int count, int iterations)
 {
+    nadia::Range range("nadia_iterate_many");
     return guard([&] {
         need(solvers, "solvers");
         std::vector<Solver *> v;

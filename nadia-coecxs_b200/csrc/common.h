@@ -12,9 +12,20 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "nadia_b200.h"
 
 namespace nadia {
+
+// A named range on the host timeline for profilers (Nsight tools show it;
+// with no tool attached the calls do nothing).
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
 
 // An error carried to the C ABI boundary, where it becomes a status code.
 struct Error : std::runtime_error {

@@ -401,6 +401,7 @@ void Server::run()
         std::vector<Record *> keep;
         const double t0 = now();
         try {
+            Range range("nadia_server_step");
             if (c > 0) iterate_many(handles.data(), (int)handles.size(), c);
             for (Record *r : active_) {
                 r->done_iters += c;
