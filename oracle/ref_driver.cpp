@@ -255,6 +255,19 @@ void ref_poly_set_spectrum_file(void *h, const char *path)
     static_cast<PolyCDI *>(S(h)->cdi)->set_spectrum(std::string(path));
 }
 
+// PolyCDI::expand_wl on a field of fx x fy (PolyCDI.c++:296-334), then
+// get_intensity (PolyCDI.h:244-246) into out (the solver's nx x ny)
+void ref_poly_expand_wl(void *h, const double *field, int fx, int fy, double *out)
+{
+    PolyCDI *p = static_cast<PolyCDI *>(S(h)->cdi);
+    Complex_2D c(fx, fy);
+    to_cplx(c, field);
+    p->expand_wl(c);
+    Double_2D r = p->get_intensity();
+    for (int i = 0; i < S(h)->nx; ++i)
+        for (int j = 0; j < S(h)->ny; ++j) out[(size_t)i * S(h)->ny + j] = r.get(i, j);
+}
+
 int ref_get_best_result(void *h, int index, double *err, double *a)
 {
     double e = 0;
