@@ -153,9 +153,14 @@ public:
     // PolyCDI::set_transmission -- PolyCDI.h:220
     void set_transmission(Complex_2D &new_transmission) { set_exit_surface_wave(new_transmission); }
 
+    // PolyCDI::set_iterations_per_cycle (PolyCDI.h:200-202): stored only;
+    // PolyCDI::iterate never reads it in the reference either
+    void set_iterations_per_cycle(int iterations) { iterations_per_cycle = iterations; }
+
 private:
     nadia_cxx::PolySpectrum spec;
     Double_2D intensity_sqrt_calc;
+    int iterations_per_cycle = 0;
 };
 
 #endif
