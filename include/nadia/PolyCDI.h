@@ -153,6 +153,23 @@ public:
     // PolyCDI::set_transmission -- PolyCDI.h:220
     void set_transmission(Complex_2D &new_transmission) { set_exit_surface_wave(new_transmission); }
 
+    // PolyCDI::sum_intensity (PolyCDI.c++:404-430): the sum over the fields
+    // c[m] of eigen[m] * |c[m]|^2.  The reference never fills its mode
+    // weights (eigen), so any non-empty list throws std::out_of_range there,
+    // and here; an empty one gives zeros.
+    Double_2D sum_intensity(std::vector<Complex_2D> &c)
+    {
+        Double_2D magnitude(nx, ny);
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j) {
+                double mag_total = 0;
+                for (size_t mode = 0; mode < c.size(); ++mode)
+                    mag_total += eigen.at(mode) * c.at(mode).get_mag(i, j) * c.at(mode).get_mag(i, j);
+                magnitude.set(i, j, mag_total);
+            }
+        return magnitude;
+    }
+
     // PolyCDI::set_iterations_per_cycle (PolyCDI.h:200-202): stored only;
     // PolyCDI::iterate never reads it in the reference either
     void set_iterations_per_cycle(int iterations) { iterations_per_cycle = iterations; }
@@ -161,6 +178,7 @@ private:
     nadia_cxx::PolySpectrum spec;
     Double_2D intensity_sqrt_calc;
     int iterations_per_cycle = 0;
+    std::vector<double> eigen; // never filled, as in the reference
 };
 
 #endif
