@@ -161,6 +161,15 @@ inline int write_ppm(std::string file_name, const Double_2D &data, bool log_scal
     return SUCCESS;
 }
 
+// io.h's line_tokeniser (NADIA/include/io.h:289-299): the tab-separated
+// fields of a line appended to *data (a line without tabs is one field)
+inline void line_tokeniser(std::string line, std::vector<std::string> *data)
+{
+    std::string field;
+    std::istringstream in(line);
+    while (std::getline(in, field, '\t')) data->push_back(field);
+}
+
 // a P2 image back into a Double_2D (grey levels as values)
 inline int read_ppm(std::string file_name, Double_2D &data)
 {

@@ -145,4 +145,14 @@ int shim_config(const char *path, const char *key, int kind, char *out, int cap)
     return c.getStatus();
 }
 
+// line_tokeniser's fields joined by '|', each followed by it
+int shim_tokenise(const char *line, char *out, int cap)
+{
+    std::vector<std::string> f;
+    line_tokeniser(line, &f);
+    std::string s;
+    for (const std::string &v : f) s += v + "|";
+    return put(s, out, cap) < 0 ? -1 : (int)f.size();
+}
+
 } // extern "C"

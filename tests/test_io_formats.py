@@ -28,6 +28,7 @@ def _bind(path):
         "shim_write_spec": [s, i, i, D],
         "shim_read_spec": [s, i, D, ctypes.POINTER(i), ctypes.POINTER(i)],
         "shim_config": [s, s, i, ctypes.c_char_p, i],
+        "shim_tokenise": [s, ctypes.c_char_p, i],
     }.items():
         getattr(L, name).argtypes = args
         getattr(L, name).restype = i
@@ -252,3 +253,15 @@ def test_config_values(libs, tmp_path):
     assert q("empty_list", "S")[0] == 0
     assert own.shim_config(str(tmp_path / "none").encode(), b"x", ord("s"),
                            ctypes.create_string_buffer(16), 16) == 0
+
+
+def test_line_tokeniser_matches_reference(libs):
+    # io.h's line_tokeniser splits on tabs only (NADIA/include/io.h:289-299)
+    own, ref = libs[0], _ref(libs)
+    for line in [b"1\t2\t3", b"a b\tc", b"", b"\t", b"x\t\ty\t", b"no tabs here", b"\t\tz"]:
+        got = []
+        for L in (own, ref):
+            buf = ctypes.create_string_buffer(256)
+            n = L.shim_tokenise(line, buf, 256)
+            got.append((n, buf.value))
+        assert got[0] == got[1], (line, got)
