@@ -3,10 +3,12 @@
 * The reference's own example programs (NADIA/examples: PlanarCDI,
   FresnelCDI, FresnelCDI_WF, PolyCDI, ComplexConstraints and the Planar and
   Poly simulations), unmodified, compile and link against include/nadia and
-  libnadia_b200.so in the float and the double build.  Not built: the
-  PhaseDiverse example (it includes gperftools' google/profiler.h), the
-  Fresnel simulation (the reference's image utilities, utils.h, are not part
-  of this library) and the partially coherent examples (out of scope).
+  libnadia_b200.so in the float and the double build.  The PhaseDiverse
+  example and the Fresnel simulation include two headers this library does
+  not provide -- the reference's image utilities (utils.h, from which they
+  call nothing) and gperftools' google/profiler.h -- so they are compiled
+  with test-only stand-ins for those two.  The partially coherent examples
+  are out of scope.
 * PolyCDI's public expand_wl / get_intensity, used by the Poly simulation and
   computed on the host by the drop-in class, equal the reference's
   (PolyCDI.c++:66-89, 296-334; double build, oracle/_ref) bit for bit.
@@ -47,6 +49,28 @@ def test_reference_example_compiles_unchanged(tmp_path, name, double):
     cmd = ["g++", "-std=c++17", "-O1", "-x", "c++", "-I", os.path.join(ROOT, "include", "nadia"),
            "-I", os.path.join(ROOT, "include"), src, "-L", LIBDIR, "-lnadia_b200",
            "-Wl,-rpath," + LIBDIR, "-o", str(tmp_path / name)]
+    if double:
+        cmd.insert(1, "-DDOUBLE_PRECISION")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+
+
+@needs_ref
+@needs_lib
+@pytest.mark.parametrize("double", [False, True], ids=["float", "double"])
+@pytest.mark.parametrize("name", ["PhaseDiverse_example", "FresnelCDI_simulation_example"])
+def test_reference_example_with_stand_in_headers(tmp_path, name, double):
+    inc = tmp_path / "stand_in"
+    (inc / "google").mkdir(parents=True)
+    (inc / "utils.h").write_text("// stand-in: the example includes it and calls nothing from it\n")
+    (inc / "google" / "profiler.h").write_text(
+        "// stand-in for gperftools\n"
+        "inline int ProfilerStart(const char *) { return 1; }\n"
+        "inline void ProfilerStop() {}\n")
+    src = os.path.join(NADIA, "examples", name + ".c")
+    cmd = ["g++", "-std=c++17", "-O1", "-x", "c++", "-I", os.path.join(ROOT, "include", "nadia"),
+           "-I", os.path.join(ROOT, "include"), "-I", str(inc), src, "-L", LIBDIR,
+           "-lnadia_b200", "-Wl,-rpath," + LIBDIR, "-o", str(tmp_path / name)]
     if double:
         cmd.insert(1, "-DDOUBLE_PRECISION")
     r = subprocess.run(cmd, capture_output=True, text=True)
