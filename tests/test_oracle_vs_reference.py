@@ -139,3 +139,31 @@ def test_threaded_fft_build_matches_serial_build(monkeypatch):
 
     same(sc.planar_mixed(make("32_fast"), n=40, ny=56, n_best=0),
          sc.planar_mixed(make("32_fast_mt"), n=40, ny=56, n_best=0))
+
+
+def every_algorithm(make, n=32, ny=40):
+    """Each named algorithm of BaseCDI::set_algorithm (BaseCDI.c++:192-275)
+    for a few iterations from the same start, with the relaxation parameter
+    changed before each switch (it takes effect at the switch)."""
+    c = sc.planar_inputs(n, ny=ny)
+    s = make("planar", n, ny)
+    s.set_support(c.support)
+    s.set_intensity(c.intensity)
+    s.set_beam_stop(c.beam_stop)
+    s.initialise_estimate(2)
+    out = {}
+    for k, alg in enumerate([sc.BIO, sc.BOO, sc.HIO, sc.DM, sc.SF, sc.ASR, sc.HPR, sc.RAAR,
+                             sc.ER]):
+        s.set_relaxation_parameter(0.6 + 0.04 * k)
+        s.set_algorithm(alg)
+        errs = []
+        for _ in range(4):
+            s.iterate()
+            errs.append(s.get_error())
+        out["errors_%d" % alg] = np.array(errs)
+        out["esw_%d" % alg] = s.get_exit_surface_wave()
+    return out
+
+
+def test_every_named_algorithm():
+    same(every_algorithm(orc), every_algorithm(ref))
