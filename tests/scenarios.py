@@ -74,13 +74,13 @@ def planar_custom(make, n=32, seed=4):
             "support": s.get_support()}
 
 
-def fresnel_inputs(n, seed=4):
-    return synth.FresnelCase(n, seed=seed)
+def fresnel_inputs(n, seed=4, ny=None):
+    return synth.FresnelCase(n, seed=seed, ny=ny)
 
 
-def fresnel_mixed(make, n=32, seed=2):
-    f = fresnel_inputs(n)
-    s = make("fresnel", n, n, white_field=f.white_field, wavelength=f.wavelength,
+def fresnel_mixed(make, n=32, seed=2, ny=None):
+    f = fresnel_inputs(n, ny=ny)
+    s = make("fresnel", n, ny or n, white_field=f.white_field, wavelength=f.wavelength,
              focal_detector_length=f.zfd, focal_sample_length=f.zfs, pixel_size=f.pixel,
              normalisation=0.97)
     s.set_support(f.support)

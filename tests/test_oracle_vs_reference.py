@@ -43,6 +43,12 @@ def test_fresnel():
     same(sc.fresnel_mixed(orc, n=64), sc.fresnel_mixed(ref, n=64))
 
 
+def test_fresnel_non_square():
+    # the phase-factor table is (nx/2) x (ny/2) with separate x and y centres
+    # (FresnelCDI.c++:57-126); ny > nx (see test_planar for ny < nx)
+    same(sc.fresnel_mixed(orc, n=40, ny=56), sc.fresnel_mixed(ref, n=40, ny=56))
+
+
 @pytest.mark.parametrize("n", [32, 64])
 def test_planar_transmission_constraint(n):
     same(sc.planar_constrained(orc, n=n), sc.planar_constrained(ref, n=n))
