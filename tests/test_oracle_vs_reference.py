@@ -173,3 +173,35 @@ def every_algorithm(make, n=32, ny=40):
 
 def test_every_named_algorithm():
     same(every_algorithm(orc), every_algorithm(ref))
+
+
+def poly_non_square(make, nx=40, ny=56, seed=8):
+    """PolyCDI on a non-square grid: the padding differs per axis
+    ((lambda_0/lambda_c - 1) * n / 2 for n = nx and ny, PolyCDI.c++:86-87) and
+    the wavelength expansion resamples each axis about its own centre."""
+    from pynadia import synth
+    g = np.random.default_rng(seed)
+    spec = synth.gaussian_spectrum(6, 0.1, 1.0e-10, 2, nx)
+    intensity = g.uniform(0.0, 50.0, (nx, ny)) * (g.random((nx, ny)) > 0.1)
+    support = np.zeros((nx, ny))
+    support[nx // 4:3 * nx // 4, ny // 4:3 * ny // 4] = 1.0
+    s = make("poly", nx, ny, n_best=1)
+    s.set_support(support)
+    s.set_intensity(intensity)
+    s.set_spectrum(spec)
+    s.initialise_estimate(seed)
+    errs = []
+    for alg, its in ((sc.ER, 3), (sc.HIO, 5)):
+        s.set_algorithm(alg)
+        for _ in range(its):
+            s.iterate()
+            errs.append(s.get_error())
+    s.apply_shrinkwrap(1.5, 0.1)
+    s.iterate()
+    errs.append(s.get_error())
+    return {"errors": np.array(errs), "esw": s.get_exit_surface_wave(),
+            "support": s.get_support()}
+
+
+def test_poly_non_square():
+    same(poly_non_square(orc), poly_non_square(ref))
