@@ -264,6 +264,94 @@ def make_solvers(pynadia, case, batch, precision):
     return out
 
 
+def _planar_program(s, cfg):
+    """The program of a named PlanarCDI workload on a reconstruction `s` (the
+    reference's classes or this library's): c1 = HIO 200 with shrinkwrap
+    every 20 (sigma 1.5, t 0.1); c2 = ER 50 / HIO 400 (beta 0.9) / ER 50."""
+    if cfg == "c1":
+        s.set_algorithm(3)
+        for _ in range(10):
+            s.iterate(20)
+            s.apply_shrinkwrap(1.5, 0.1)
+    else:
+        s.set_algorithm(0)
+        s.iterate(50)
+        s.set_relaxation_parameter(0.9)  # takes effect at the next change (BaseCDI.h:264-267)
+        s.set_algorithm(3)
+        s.iterate(400)
+        s.set_algorithm(0)
+        s.iterate(50)
+
+
+def _cpu_config_worker(args):
+    """Seconds per iteration of the reference's double build on one core: the
+    whole c1 program, or a 10-iteration HIO sample of c2."""
+    cfg, variant = args
+    sys.path[:0] = [ORACLE, PKG]
+    import pyoracle as po
+    from pynadia import synth
+    c = synth.planar_case(cfg)
+    s = po.Reference("planar", c.nx, c.ny, variant=variant)
+    s.set_support(c.support)
+    s.set_intensity(c.intensity)
+    s.initialise_estimate(0)
+    t = time.perf_counter()
+    if cfg == "c1":
+        _planar_program(s, cfg)
+        return (time.perf_counter() - t) / 200.0, time.perf_counter() - t
+    s.set_algorithm(3)
+    s.iterate(1)
+    t = time.perf_counter()
+    s.iterate(10)
+    per = (time.perf_counter() - t) / 10.0
+    return per, per * 500
+
+
+def configs_report(pynadia, synth, torch, cpu=True):
+    """The FP64 configurations (256^2 and 1024^2 PlanarCDI): the FP64 form on
+    the GPU (whole program, CUDA events on the reconstruction's stream)
+    beside the reference's double build (-O3 -ffast-math, FFTs through the
+    project's shim) on one host core, timed in a separate process."""
+    out = {}
+    for cfg in ("c1", "c2"):
+        c = synth.planar_case(cfg)
+        s = pynadia.Solver("planar", c.nx, c.ny, precision=pynadia.FP64)
+        s.set_support(c.support)
+        s.set_intensity(c.intensity)
+        s.initialise_estimate(0)
+        s.iterate(1)  # warm the kernels and plans
+        s.synchronize()
+        s.close()
+        s = pynadia.Solver("planar", c.nx, c.ny, precision=pynadia.FP64)
+        s.set_support(c.support)
+        s.set_intensity(c.intensity)
+        s.initialise_estimate(0)
+        st = torch.cuda.ExternalStream(s.stream())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        _planar_program(s, cfg)
+        b.record(st)
+        b.synchronize()
+        sec = a.elapsed_time(b) / 1000.0
+        its = 200 if cfg == "c1" else 500
+        r = {"grid": [c.nx, c.ny], "iterations": its,
+             "program": "HIO 200, shrinkwrap every 20" if cfg == "c1" else "ER 50 / HIO 400 / ER 50",
+             "gpu_fp64_s": sec, "gpu_fp64_ms_per_iteration": 1000.0 * sec / its,
+             "final_error": s.get_error()}
+        s.close()
+        if cpu and reference_build_available("64_fast"):
+            ctx = mp.get_context("spawn")
+            with ctx.Pool(1) as pool:
+                per, whole = pool.map(_cpu_config_worker, [(cfg, "64_fast")])[0]
+            r["cpu_reference_double_s_per_iteration_one_core"] = per
+            r["cpu_reference_double_s"] = whole
+            r["cpu_sample"] = ("whole program" if cfg == "c1"
+                               else "10 HIO iterations, extrapolated to 500")
+            r["gpu_over_cpu_one_core"] = whole / sec
+        out[cfg] = r
+    return out
+
+
 def run_program(pynadia, solvers):
     """1000 HIO iterations with shrinkwrap every 50, all queued asynchronously."""
     for _ in range(ITERS // SW_EVERY):
@@ -943,6 +1031,10 @@ def ours(args, rank, world, local_rank):
         white_field = white_field_report(pynadia, synth) if not args.no_wf else None
         phase_diverse = phase_diverse_report(pynadia, synth) if not args.no_pd else None
         constraint = constraint_report(pynadia, synth) if not args.no_tc else None
+        try:
+            configs = configs_report(pynadia, synth, torch, cpu=not args.no_cpu)
+        except Exception as e:  # noqa: BLE001 -- an auxiliary report
+            configs = {"error": repr(e)}
 
         serving = None
         if args.serve_requests > 0:
@@ -997,6 +1089,7 @@ def ours(args, rank, world, local_rank):
             "gpu_launches": launches, "fp64_plain": fp64, "accuracy": accuracy,
             "serving": serving, "fresnel_batch": fresnel_batch, "white_field": white_field,
             "phase_diverse": phase_diverse, "transmission_constraint": constraint,
+            "fp64_configs": configs,
         }
     if dist:
         dist.barrier()
