@@ -86,3 +86,25 @@ def test_column_pass_bulk_copies(v):
             # the tile's global offset, (t % tps) * L * nx elements, for any nx
             for nx in SIZES:
                 assert (t * L * nx * 8) % 16 == 0 and (t * L * nx * 4) % 16 == 0
+
+
+def test_box_panels_model_matches_the_library(tmp_path):
+    """The Python model of box_panels above against the library's own
+    (fused32_impl.h), compiled for the host, for every panel count to 2048."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "bp.cpp"
+    src.write_text('#include "fused32_impl.h"\n#include <cstdio>\n'
+                   'int main() { for (int n = 1; n <= 2048; ++n) '
+                   'printf("%d %d\\n", n, nadia::f32::box_panels(n)); }\n')
+    exe = tmp_path / "bp"
+    r = subprocess.run(["g++", "-std=c++17", "-I", "/usr/local/cuda/include",
+                        "-I", os.path.join(root, "include"),
+                        "-I", os.path.join(root, "nadia-coecxs_b200", "csrc"), str(src), "-o",
+                        str(exe)], capture_output=True, text=True)
+    if r.returncode != 0:
+        pytest.skip("host compile of fused32_impl.h failed: " + r.stderr[-300:])
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    got = {int(out[i]): int(out[i + 1]) for i in range(0, len(out), 2)}
+    assert all(got[n] == box_panels(n) for n in range(1, 2049))
