@@ -42,6 +42,9 @@ METRIC = "HIO recon/s and p50/p99 latency at 2048^2, FP32 batched vs FP64 plain,
 N = 2048
 ITERS = 1000
 SW_EVERY = 50
+ACC_SEEDS_DEFAULT = 16
+CPU_ITERS = 5  # timed iterations per CPU stream (after one untimed)
+C2_CPU_ITERS = 20
 
 
 def parse():
@@ -73,6 +76,10 @@ def parse():
     p.add_argument("--quick-poly", action="store_true",
                    help="device-resident FP32 PolyCDI steps only (1024^2 padded to 1080^2; "
                         "for profiling)")
+    p.add_argument("--accuracy-only", action="store_true",
+                   help="print the FP32-vs-FP64 accuracy ensemble only")
+    p.add_argument("--accuracy-seeds", type=int, default=ACC_SEEDS_DEFAULT,
+                   help="problems in the accuracy ensemble (0 = skip it)")
     p.add_argument("--quick", action="store_true",
                    help="device-resident steps only (for profiling): no e2e, FP64, CPU legs")
     return p.parse_args()
@@ -108,7 +115,7 @@ def _cpu_worker(args):
     t = time.perf_counter()
     s.apply_shrinkwrap(1.5, 0.1)
     t_sw = time.perf_counter() - t
-    return t_it, t_sw
+    return t_it, t_sw, t_it * iters
 
 
 def cpu_kind():
@@ -165,7 +172,7 @@ def cpu_sample(procs, iters, variant="32_fast", threads=1):
     with ctx.Pool(procs) as pool:
         res = pool.map(_cpu_worker, [(kind, iters, variant, threads)] * procs)
     wall = time.perf_counter() - t0
-    per_recon = [t_it * ITERS + t_sw * (ITERS // SW_EVERY) for t_it, t_sw in res]
+    per_recon = [t_it * ITERS + t_sw * (ITERS // SW_EVERY) for t_it, t_sw, _ in res]
     value = sum(1.0 / s for s in per_recon)
     desc = ("%d independent %dx%d HIO streams, %d timed iterations + 1 shrinkwrap each, "
             "extrapolated to %d iterations with shrinkwrap every %d; %s"
@@ -176,7 +183,9 @@ def cpu_sample(procs, iters, variant="32_fast", threads=1):
                                        if variant.endswith("_mt") else "")
                if kind == "reference" else "oracle restatement (FP64)"))
     return {"value": value, "unit": "recon/s", "cores": procs, "kind": kind, "sample": desc,
-            "s_per_iteration": sum(r[0] for r in res) / len(res), "wall_s": wall}
+            "s_per_iteration": sum(r[0] for r in res) / len(res), "wall_s": wall,
+            "timed_s_per_stream": [round(r[2], 4) for r in res],
+            "shrinkwrap_s_per_stream": [round(r[1], 4) for r in res]}
 
 
 # --------------------------------------------------------------- GPU side
@@ -285,7 +294,7 @@ def _planar_program(s, cfg):
 
 def _cpu_config_worker(args):
     """Seconds per iteration of the reference's double build on one core: the
-    whole c1 program, or a 10-iteration HIO sample of c2."""
+    whole c1 program, or a C2_CPU_ITERS-iteration HIO sample of c2."""
     cfg, variant = args
     sys.path[:0] = [ORACLE, PKG]
     import pyoracle as po
@@ -302,8 +311,8 @@ def _cpu_config_worker(args):
     s.set_algorithm(3)
     s.iterate(1)
     t = time.perf_counter()
-    s.iterate(10)
-    per = (time.perf_counter() - t) / 10.0
+    s.iterate(C2_CPU_ITERS)
+    per = (time.perf_counter() - t) / C2_CPU_ITERS
     return per, per * 500
 
 
@@ -345,8 +354,11 @@ def configs_report(pynadia, synth, torch, cpu=True):
                 per, whole = pool.map(_cpu_config_worker, [(cfg, "64_fast")])[0]
             r["cpu_reference_double_s_per_iteration_one_core"] = per
             r["cpu_reference_double_s"] = whole
+            r["cpu_reference_double_timed_s"] = whole if cfg == "c1" else per * C2_CPU_ITERS
             r["cpu_sample"] = ("whole program" if cfg == "c1"
-                               else "10 HIO iterations, extrapolated to 500")
+                               else "%d HIO iterations, extrapolated to 500" % C2_CPU_ITERS)
+            r["timing"] = ("GPU: CUDA events around the whole program on the reconstruction's "
+                           "stream; CPU: perf_counter in a separate process")
             r["gpu_over_cpu_one_core"] = whole / sec
         out[cfg] = r
     return out
@@ -442,6 +454,33 @@ def serve(pynadia, inputs, rate, n_req, seed, planar_precision, poly_precision,
                        "preparing": st["us_prepare"] / 1e6, "reading_back": st["us_readback"] / 1e6},
             "failed": st["failed"], "precision": {"planar": "FP32" if planar_precision else "FP64",
                                                    "poly": "FP32" if poly_precision else "FP64"}}
+
+
+def latency_report(pynadia, case, n_req=20):
+    """Time to reconstruction of config 3 requests (PlanarCDI FP32 2048^2,
+    1000 HIO iterations, shrinkwrap every 50), one at a time through the
+    request loop: from submit (the pattern, support and beam stop on the
+    host) to the estimate and error on the host, wall clock; p50/p99 over
+    `n_req` requests after one untimed request."""
+    srv = pynadia.Server(16 * 10**9, max_active=1, chunk=50)
+
+    def one(k):
+        t = time.perf_counter()
+        rid = srv.submit("planar", case.intensity, case.support, precision=pynadia.FP32,
+                         beam_stop=case.beam_stop, algorithm="HIO", beta=0.9, iterations=ITERS,
+                         shrinkwrap_every=SW_EVERY, shrinkwrap_sigma=1.5,
+                         shrinkwrap_threshold=0.1, seed=k)
+        srv.wait(rid, -1)
+        srv.result(rid)
+        return 1000.0 * (time.perf_counter() - t)
+
+    one(0)
+    lat = sorted(one(k + 1) for k in range(n_req))
+    srv.close()
+    return {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(math.ceil(0.99 * len(lat))) - 1)],
+            "requests": n_req,
+            "note": "one config-3 request at a time through nadia_server_*: submit on the host "
+                    "to estimate and error on the host; loaded latencies: serving"}
 
 
 def serving_report(pynadia, synth, n_req=48, n_req_fp64=12):
@@ -808,6 +847,127 @@ def quick_poly(pynadia, synth, args):
             "pass_us": {"column_fwd": c1, "column_inv": c2, "row": r}}
 
 
+def accuracy_report(pynadia, synth, seeds=ACC_SEEDS_DEFAULT, n=N):
+    """Config 3's accuracy over an ensemble of `seeds` seeded problems (disk
+    object radius 320, sigma 4, 1e9 photons, 8x8 beam stop; problem k has
+    data seed 1000+k and initialise_estimate(k)), each run in three forms:
+    FP64 plain, FP32 fused, and FP64 from a start perturbed by 1e-12
+    (relative) -- the control that measures how far two FP64 runs part when
+    their starts differ in the last bits.  Schedules:
+      A  config 3: 1000 HIO (beta 0.9), shrinkwrap every 50;
+      B  contractive tail: the same 900 HIO, then 100 ER from each form's own
+         state at 900 (each form in its own basin);
+      C  same basin: the FP64 state at 900 (estimate and support) given to an
+         FP64 and an FP32 reconstruction, then 100 ER (and, separately, 100
+         HIO) in both.
+    Reports each form's final-error distribution (mean, sd, median), the
+    two-sample Kolmogorov-Smirnov p-values FP32 vs FP64 and perturbed-FP64 vs
+    FP64, the iteration where each pair's error tracks part by 1e-4, and for C
+    the largest per-iterate relative difference of the error tracks."""
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+    from scipy import stats
+
+    def case(k):
+        return synth.PlanarCase(n, 320 * n // 2048, 4, 1e9, seed=1000 + k,
+                                support_side=800 * n // 2048, beam_stop=8)
+
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        cases = list(ex.map(case, range(seeds)))
+
+    def make(c, prec, k):
+        s = pynadia.Solver("planar", n, n, precision=prec)
+        s.set_support(c.support)
+        s.set_intensity(c.intensity)
+        s.set_beam_stop(c.beam_stop)
+        s.initialise_estimate(k)
+        s.set_algorithm("HIO")
+        return s
+
+    def hio(solvers, iters):
+        for _ in range(iters // SW_EVERY):
+            pynadia.iterate_many(solvers, SW_EVERY)
+            for s in solvers:
+                s.apply_shrinkwrap(1.5, 0.1)
+
+    def parting(h, ref):
+        d = np.nonzero(np.abs(h - ref) > 1e-4 * np.abs(ref))[0]
+        return int(d[0]) if len(d) else None
+
+    def restore(s, state, alg):
+        s.set_exit_surface_wave(state[0])
+        s.set_support(state[1])
+        s.set_algorithm(alg)
+
+    rows = []
+    t0 = time.perf_counter()
+    for k, c in enumerate(cases):
+        a, b, p = make(c, pynadia.FP64, k), make(c, pynadia.FP32, k), make(c, pynadia.FP64, k)
+        x0 = p.get_exit_surface_wave()
+        g = np.random.default_rng(1000 + k)
+        p.set_exit_surface_wave(x0 * (1 + 1e-12 * g.standard_normal(x0.shape)))
+        forms = (a, b, p)
+        hio(forms, 900)
+        snap = [(s.get_exit_surface_wave(), s.get_support()) for s in forms]
+        hio(forms, ITERS - 900)                                   # A
+        hA = [s.get_error_history(ITERS) for s in forms]
+        xA = [s.get_exit_surface_wave() for s in forms]
+        for s, st in zip(forms, snap):                            # B
+            restore(s, st, "ER")
+        pynadia.iterate_many(list(forms), 100)
+        eB = [float(s.get_error()) for s in forms]
+        row = {"seed": k,
+               "A_final": [float(h[-1]) for h in hA],
+               "A_parting_fp32": parting(hA[1], hA[0]),
+               "A_parting_perturbed": parting(hA[2], hA[0]),
+               "A_phase_aligned_fp32": phase_aligned_error(xA[1], xA[0]),
+               "A_phase_aligned_perturbed": phase_aligned_error(xA[2], xA[0]),
+               "B_final": eB}
+        for alg in ("ER", "HIO"):                                 # C
+            restore(a, snap[0], alg)
+            restore(b, snap[0], alg)
+            pynadia.iterate_many([a, b], 100)
+            h64, h32 = a.get_error_history(100), b.get_error_history(100)
+            row["C_" + alg] = {"max_rel_diff": float(np.max(np.abs(h32 - h64) / h64)),
+                               "final_rel_diff": float(abs(h32[-1] - h64[-1]) / h64[-1]),
+                               "parting": parting(h32, h64)}
+        for s in forms:
+            s.close()
+        rows.append(row)
+
+    def dist(vals):
+        v = np.asarray(vals)
+        return {"mean": float(v.mean()), "sd": float(v.std(ddof=1)), "median": float(np.median(v))}
+
+    A = np.array([r["A_final"] for r in rows])
+    B = np.array([r["B_final"] for r in rows])
+    out = {"seeds": seeds, "grid": [n, n], "wall_s": round(time.perf_counter() - t0, 1)}
+    for name, M in (("A_config3_hio1000", A), ("B_hio900_er100", B)):
+        out[name] = {
+            "final_error": {"fp64": dist(M[:, 0]), "fp32": dist(M[:, 1]),
+                            "fp64_perturbed_1e-12": dist(M[:, 2])},
+            "ks_p_fp32_vs_fp64": float(stats.ks_2samp(M[:, 1], M[:, 0]).pvalue),
+            "ks_p_perturbed_vs_fp64": float(stats.ks_2samp(M[:, 2], M[:, 0]).pvalue),
+            "median_rel_diff_fp32_vs_fp64": float(np.median(np.abs(M[:, 1] - M[:, 0]) / M[:, 0])),
+            "median_rel_diff_perturbed_vs_fp64":
+                float(np.median(np.abs(M[:, 2] - M[:, 0]) / M[:, 0]))}
+    out["A_config3_hio1000"]["parting_iteration"] = {
+        "fp32_vs_fp64": [r["A_parting_fp32"] for r in rows],
+        "perturbed_vs_fp64": [r["A_parting_perturbed"] for r in rows]}
+    out["A_config3_hio1000"]["phase_aligned_rel_error_median"] = {
+        "fp32_vs_fp64": float(np.median([r["A_phase_aligned_fp32"] for r in rows])),
+        "perturbed_vs_fp64": float(np.median([r["A_phase_aligned_perturbed"] for r in rows]))}
+    for alg in ("ER", "HIO"):
+        out["C_same_state_at_900_then_100_" + alg] = {
+            "max_rel_diff_per_iterate": {
+                "max": float(max(r["C_" + alg]["max_rel_diff"] for r in rows)),
+                "median": float(np.median([r["C_" + alg]["max_rel_diff"] for r in rows]))},
+            "final_rel_diff_max": float(max(r["C_" + alg]["final_rel_diff"] for r in rows)),
+            "parting": [r["C_" + alg]["parting"] for r in rows]}
+    out["per_seed"] = rows
+    return out
+
+
 def phase_aligned_error(x, ref):
     import numpy as np
     inner = np.vdot(x, ref)
@@ -830,6 +990,8 @@ def ours(args, rank, world, local_rank):
         return {"white_field": white_field_report(pynadia, synth)}
     if args.pd_only:
         return {"phase_diverse": phase_diverse_report(pynadia, synth)}
+    if args.accuracy_only:
+        return {"accuracy": accuracy_report(pynadia, synth, seeds=args.accuracy_seeds)}
     if args.tc_only:
         return {"transmission_constraint": constraint_report(pynadia, synth)}
     if args.pd_profile:  # a short phase-diverse run without the searches, for ncu
@@ -1023,6 +1185,11 @@ def ours(args, rank, world, local_rank):
                         "stream"}
         for s_ in (a, b, c):
             s_.close()
+        if args.accuracy_seeds > 0:
+            try:
+                accuracy["ensemble"] = accuracy_report(pynadia, synth, seeds=args.accuracy_seeds)
+            except Exception as e:  # noqa: BLE001 -- an auxiliary report
+                accuracy["ensemble"] = {"error": repr(e)}
 
         fresnel_batch = None
         if args.fresnel_batch > 0:
@@ -1042,15 +1209,15 @@ def ours(args, rank, world, local_rank):
 
         cpu = None
         if not args.no_cpu:
-            procs = max(1, min(os.cpu_count() or 1, 8))
-            cpu = cpu_sample(procs, iters=2)
+            procs = max(1, os.cpu_count() or 1)
+            cpu = cpu_sample(procs, iters=CPU_ITERS)
             cpu["host"] = host_probe()
             if cpu["kind"] == "reference" and reference_build_available("64_fast"):
                 # the reference's double build (-DDOUBLE_PRECISION), the
                 # arithmetic of the FP64 form, on the same sample; an
                 # auxiliary figure, so a failure is reported, not raised
                 try:
-                    d = cpu_sample(procs, iters=1, variant="64_fast")
+                    d = cpu_sample(procs, iters=CPU_ITERS, variant="64_fast")
                     cpu["double_build"] = {
                         "value": d["value"], "unit": "recon/s", "cores": procs,
                         "s_per_iteration": d["s_per_iteration"], "sample": d["sample"],
@@ -1063,13 +1230,16 @@ def ours(args, rank, world, local_rank):
                 # reference's --enable-threads build); per-pixel loops stay serial
                 nth = os.cpu_count() or 1
                 try:
-                    d = cpu_sample(1, iters=2, variant="32_fast_mt", threads=nth)
+                    d = cpu_sample(1, iters=CPU_ITERS, variant="32_fast_mt", threads=nth)
                     cpu["float_build_fft_threads"] = {
                         "value": d["value"], "unit": "recon/s", "cores": nth,
                         "s_per_iteration": d["s_per_iteration"], "sample": d["sample"]}
                 except Exception as e:  # noqa: BLE001
                     cpu["float_build_fft_threads"] = {"error": repr(e)}
-        step_ms_sorted = sorted(step_ms)
+        try:
+            latency = latency_report(pynadia, case)
+        except Exception as e:  # noqa: BLE001 -- an auxiliary report
+            latency = {"error": repr(e)}
         line = {
             "metric": METRIC, "value": value, "unit": "recon/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
@@ -1081,10 +1251,7 @@ def ours(args, rank, world, local_rank):
                        "shrinkwrap_every": SW_EVERY, "precision_form": "FP32 fused",
                        "l2": "working set %.2f GB > 126 MB L2, no flush" % (B * N * N * 24 / 1e9),
                        "parallelism": "replicas x%d" % world},
-            "latency_ms": {"p50": step_ms_sorted[len(step_ms) // 2],
-                           "p99": step_ms_sorted[min(len(step_ms) - 1,
-                                                     int(math.ceil(0.99 * len(step_ms))) - 1)],
-                           "note": "per reconstruction in a batch = its batch's step time"},
+            "latency_ms": latency,
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": launches, "fp64_plain": fp64, "accuracy": accuracy,
             "serving": serving, "fresnel_batch": fresnel_batch, "white_field": white_field,
@@ -1106,7 +1273,7 @@ def reference(args, rank, world):
     for _ in range(args.warmup):
         cpu_sample(procs, iters=1)
     for _ in range(args.steps):
-        info = cpu_sample(procs, iters=1)
+        info = cpu_sample(procs, iters=CPU_ITERS)
         vals.append(info["value"])
     value = sum(vals) / len(vals)
     info["value"] = value

@@ -749,7 +749,9 @@ extern "C" int nadia_tuned_tiles(int nx, int ny, int fresnel, int batched, char 
         auto desc = [](const nadia::f32::TileVariant *v) {
             char t[160];
             snprintf(t, sizeof t, "n=%d threads=%d signals/tile=%d radices=%s%s", v->n, v->nt,
-                     v->L, v->radices, v->persistent ? " persistent-TMA" : (v->ping ? " ping" : ""));
+                     v->L, v->radices,
+                     v->single ? " persistent-TMA one stage"
+                               : (v->persistent ? " persistent-TMA" : (v->ping ? " ping" : "")));
             return std::string(t);
         };
         char t[512];

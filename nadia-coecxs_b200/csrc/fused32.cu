@@ -421,8 +421,8 @@ void encode_one(CUtensorMap *m, void *base, bool complex8, int nx, int ny, int r
 
 void encode_tensor_maps(Slot &s, int nx, int ny)
 {
-    const int rows[3] = {4, 8, 16};
-    for (int k = 0; k < 3; ++k) {
+    const int rows[4] = {2, 4, 8, 16};
+    for (int k = 0; k < 4; ++k) {
         if (nx % rows[k]) {
             std::memset(&s.tm[k][0], 0, sizeof(s.tm[k]));
             continue;
@@ -536,9 +536,9 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
     // pick the first variant whose tiles divide the grid (and tune among those)
     std::vector<const TileVariant *> cols, rows;
     for (const auto &v : cv)
-        if (ny % v.L == 0) cols.push_back(&v);
+        if (v.col && ny % v.L == 0) cols.push_back(&v);
     for (const auto &v : rv)
-        if (nx % v.L == 0 && !(plain_rows && v.persistent)) rows.push_back(&v);
+        if (v.row && nx % v.L == 0 && !(plain_rows && v.persistent)) rows.push_back(&v);
     NADIA_REQUIRE(!cols.empty() && !rows.empty(), NADIA_ERR_UNSUPPORTED,
                   "grid shape does not divide into the FP32 tiles");
     ch.col = cols[0];
@@ -549,8 +549,8 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
             int a, b, c, d, ci, ri;
             while (fscanf(f, "%d %d %d %d %d %d", &a, &b, &c, &d, &ci, &ri) == 6)
                 if (a == nx && b == ny && c == (fresnel ? 1 : 0) && d == batch && ci >= 0 &&
-                    ci < (int)cv.size() && ri >= 0 && ri < (int)rv.size() &&
-                    ny % cv[ci].L == 0 && nx % rv[ri].L == 0) {
+                    ci < (int)cv.size() && ri >= 0 && ri < (int)rv.size() && cv[ci].col &&
+                    rv[ri].row && ny % cv[ci].L == 0 && nx % rv[ri].L == 0) {
                     ch.col = &cv[ci];
                     ch.row = &rv[ri];
                     fclose(f);
@@ -612,7 +612,9 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
             }, st, 5);
             if (verbose)
                 fprintf(stderr, "nadia tune: col n=%d NT=%d L=%d radices=%s%s batch=%d: %.2f us\n",
-                        nx, v->nt, v->L, v->radices, v->persistent ? " persistent" : (v->ping ? " ping" : ""), ns, us);
+                        nx, v->nt, v->L, v->radices,
+                        v->single ? " persistent-1stage" : (v->persistent ? " persistent" : (v->ping ? " ping" : "")),
+                        ns, us);
             if (us < best) { best = us; ch.col = v; ch.col_us = us; }
         }
         best = 1e30f;
@@ -703,6 +705,14 @@ Fused32::Impl::Impl(Solver &s) : S(s)
     h_slot.s0 = (float)(1.0 / sqrt((double)nx * (double)ny));
     h_slot.inv_norm2 = 0.0;
     h_slot.flag = flag.p;
+    // test hook for the bounded-wait failure path (Slot::skip_first_load)
+    if (const char *fw = getenv("NADIA_FAULT_WAIT")) {
+        const long polls = strtol(fw, nullptr, 10);
+        if (polls > 0) {
+            h_slot.wait_polls = (unsigned)polls;
+            h_slot.skip_first_load = 1;
+        }
+    }
     if (!poly) encode_tensor_maps(h_slot, nx, ny);
     Slot *sp = slot.p;
     NADIA_CUDA(cudaMemcpyAsync(slot_ptr.p, &sp, sizeof(Slot *), cudaMemcpyHostToDevice, st));

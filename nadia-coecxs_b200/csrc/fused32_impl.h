@@ -18,9 +18,9 @@ namespace f32 {
 // One reconstruction as the fused kernels see it.  It lives in device
 // memory, so graphs captured once keep working when the algorithm changes.
 struct alignas(64) Slot {
-    // tensor maps over P, x and the support for row tiles of 4, 8 and 16 rows
-    // (persistent row pass); box (K, rows, <= 256 panels)
-    CUtensorMap tm[3][3];
+    // tensor maps over P, x and the support for row tiles of 2, 4, 8 and 16
+    // rows (persistent row pass); box (K, rows, <= 256 panels)
+    CUtensorMap tm[4][3];
     float2 *P;              // work array (row transforms of x / column-pass output)
     float2 *x;              // estimate
     const float *sup;       // support
@@ -39,6 +39,13 @@ struct alignas(64) Slot {
     float s0;               // 1/sqrt(nx*ny)
     double inv_norm2;       // 1 / sum of sqrt(I)^2 over measured pixels
     int *flag;              // raised when a device-side wait gives up
+    // polls before a persistent pass's mbarrier wait gives up (0: kWaitPolls)
+    // and a hook for testing that failure path: when set, the first tile of
+    // each CTA is expected on its barrier but its copy is never issued, so
+    // that wait runs out (no copy is left in flight).  Both come from
+    // NADIA_FAULT_WAIT=<polls> at handle creation; unset, they are 0.
+    unsigned wait_polls;
+    int skip_first_load;
     // TransmissionConstraint's per-pixel part (charge flipping, unit
     // magnitude) applied in each support projection of the row pass (the
     // non-persistent variants); for FresnelCDI on the transmission function,
@@ -106,11 +113,13 @@ using RowLaunch = void (*)(int mode, const Slot *const *slots, int nslots, int n
                            const float2 *tw, cudaStream_t st);
 
 // One compiled tile shape of a transform length, usable as column pass
-// (length nx) and as row pass (length ny).
+// (length nx) and as row pass (length ny); a variant that serves only one of
+// the two passes leaves the other launcher null.
 struct TileVariant {
     int n = 0, nt = 0, L = 0, minb = 0;
     bool persistent = false;
     bool ping = false;
+    bool single = false; // persistent column pass with one stage per CTA
     const char *radices = "";
     void (*prepare)() = nullptr;
     ColLaunch col = nullptr;

@@ -250,35 +250,73 @@ void launch_row(int mode, const Slot *const *slots, int nslots, int nx, int ny, 
         k_row<C, kRowPrime><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
 }
 
-// shared memory of the persistent passes: two stages of P and sqrt(I)
+// shared memory of the persistent passes: STAGES stages of P and sqrt(I)
 // (column); two stages of P plus x and the support (row); and mbarriers
-template <class C>
-constexpr size_t persist_col_smem() { return (size_t)C::N * C::L * 24 + 16; }
+template <class C, int STAGES = 2>
+constexpr size_t persist_col_smem() { return (size_t)C::N * C::L * 12 * STAGES + 16; }
 template <class C>
 constexpr size_t persist_row_smem() { return (size_t)C::N * C::L * 28 + 24; }
+
+// CTAs of a persistent kernel resident per SM (at most MINB), measured when
+// the variant is prepared (before any launch, outside graph capture)
+template <class K>
+int resident_ctas(K kernel, int nt, size_t smem, int minb)
+{
+    int occ = 0;
+    NADIA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, nt, smem));
+    NADIA_REQUIRE(occ > 0, NADIA_ERR_CUDA, "a persistent pass does not fit on an SM");
+    return occ < minb ? occ : minb;
+}
+
+template <class C, int STAGES>
+struct PersistCol {
+    static inline int per_sm = 1;
+};
+template <class C>
+struct PersistRow {
+    static inline int per_sm = 1;
+};
+
+template <class C, int STAGES>
+void prepare_persistent_col()
+{
+    NADIA_CUDA(cudaFuncSetAttribute(kp_col<C, false, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)persist_col_smem<C, STAGES>()));
+    NADIA_CUDA(cudaFuncSetAttribute(kp_col<C, true, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)persist_col_smem<C, STAGES>()));
+    PersistCol<C, STAGES>::per_sm =
+        resident_ctas(kp_col<C, false, STAGES>, C::NT, persist_col_smem<C, STAGES>(), C::MINB);
+}
+
+template <class C>
+void prepare_persistent_row()
+{
+    set_smem<C>(k_row<C, kRowFull>);
+    set_smem<C>(k_row<C, kRowPrime>);
+    NADIA_CUDA(cudaFuncSetAttribute(kp_row<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)persist_row_smem<C>()));
+    PersistRow<C>::per_sm = resident_ctas(kp_row<C>, C::NT, persist_row_smem<C>(), C::MINB);
+}
 
 template <class CC, class CR>
 void prepare_persistent()
 {
     prepare_variant<CC, CR>();
-    NADIA_CUDA(cudaFuncSetAttribute(kp_col<CC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)persist_col_smem<CC>()));
-    NADIA_CUDA(cudaFuncSetAttribute(kp_col<CC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)persist_col_smem<CC>()));
-    NADIA_CUDA(cudaFuncSetAttribute(kp_row<CR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)persist_row_smem<CR>()));
+    prepare_persistent_col<CC, 2>();
+    prepare_persistent_row<CR>();
 }
 
-template <class C>
+template <class C, int STAGES>
 void launch_col_persistent(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
                            const float2 *tw, cudaStream_t st)
 {
     const int ntiles = (ny / C::L) * nslots;
-    const int grid = ntiles < sm_count() ? ntiles : sm_count();
+    const int cap = sm_count() * PersistCol<C, STAGES>::per_sm;
+    const int grid = ntiles < cap ? ntiles : cap;
     if (fresnel)
-        kp_col<C, true><<<grid, C::NT, persist_col_smem<C>(), st>>>(slots, nslots, nx, ny, tw);
+        kp_col<C, true, STAGES><<<grid, C::NT, persist_col_smem<C, STAGES>(), st>>>(slots, nslots, nx, ny, tw);
     else
-        kp_col<C, false><<<grid, C::NT, persist_col_smem<C>(), st>>>(slots, nslots, nx, ny, tw);
+        kp_col<C, false, STAGES><<<grid, C::NT, persist_col_smem<C, STAGES>(), st>>>(slots, nslots, nx, ny, tw);
 }
 
 template <class C>
@@ -290,7 +328,8 @@ void launch_row_persistent(int mode, const Slot *const *slots, int nslots, int n
         return;
     }
     const int ntiles = (nx / C::L) * nslots;
-    const int grid = ntiles < sm_count() ? ntiles : sm_count();
+    const int cap = sm_count() * PersistRow<C>::per_sm;
+    const int grid = ntiles < cap ? ntiles : cap;
     kp_row<C><<<grid, C::NT, persist_row_smem<C>(), st>>>(slots, nslots, nx, ny, tw);
 }
 
@@ -333,7 +372,8 @@ TileVariant make_ping(const char *radices)
 }
 
 // The same tile shape as persistent, TMA-pipelined passes (tiles of at most
-// 8192 elements, so both stages fit in shared memory).
+// 8192 elements, so both stages fit in shared memory); MINB CTAs per SM where
+// shared memory allows.
 template <int N, int NT, int L, int MINB, class SW, int... Rs>
 TileVariant make_persistent(const char *radices)
 {
@@ -348,7 +388,46 @@ TileVariant make_persistent(const char *radices)
     t.persistent = true;
     t.radices = radices;
     t.prepare = &prepare_persistent<CC, CR>;
-    t.col = &launch_col_persistent<CC>;
+    t.col = &launch_col_persistent<CC, 2>;
+    t.row = &launch_row_persistent<CR>;
+    return t;
+}
+
+// A persistent column pass with one stage per CTA (MINB CTAs share an SM);
+// no row pass.
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_persistent_single(const char *radices)
+{
+    using CC = TileCfg<N, NT, L, kColMap, Radices<Rs...>, SW, MINB>;
+    static_assert(persist_col_smem<CC, 1>() * MINB <= 226 * 1024, "stages too large");
+    TileVariant t;
+    t.n = N;
+    t.nt = NT;
+    t.L = L;
+    t.minb = MINB;
+    t.persistent = true;
+    t.single = true;
+    t.radices = radices;
+    t.prepare = &prepare_persistent_col<CC, 1>;
+    t.col = &launch_col_persistent<CC, 1>;
+    return t;
+}
+
+// A persistent row pass only: tiles of L rows (L = 2 allowed, below the
+// panel width a column tile needs), MINB CTAs per SM.
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_persistent_row(const char *radices)
+{
+    using CR = TileCfg<N, NT, L, kRowMap, Radices<Rs...>, SW, MINB>;
+    static_assert(persist_row_smem<CR>() * MINB <= 226 * 1024, "row stages too large");
+    TileVariant t;
+    t.n = N;
+    t.nt = NT;
+    t.L = L;
+    t.minb = MINB;
+    t.persistent = true;
+    t.radices = radices;
+    t.prepare = &prepare_persistent_row<CR>;
     t.row = &launch_row_persistent<CR>;
     return t;
 }

@@ -13,8 +13,9 @@
 //     in a few tensor copies; x and the support arrive the same way, on their
 //     own barrier, while the inverse row transform runs.
 //
-// Every mbarrier wait is bounded; on a timeout the CTA raises the slot's
-// error flag, waits (bounded) for its copies in flight and leaves.
+// Every mbarrier wait is bounded (Slot::wait_polls, default kWaitPolls); on
+// a timeout the CTA raises the slot's error flag, waits (bounded) for its
+// copies in flight and leaves.
 #pragma once
 
 #include "tma.cuh"
@@ -42,16 +43,21 @@ __device__ __forceinline__ void raise_flag(const Slot &S)
     if (S.flag) atomicExch(S.flag, 1);
 }
 
-template <class C, bool FRESNEL>
-__global__ void __launch_bounds__(C::NT, 1)
+// STAGES = 2: tile i+1 loads while tile i is transformed.  STAGES = 1: one
+// buffer per CTA (half the shared memory, so two CTAs share an SM and each
+// one's load overlaps the other's arithmetic); the next load is issued once
+// the previous tile's store has read the buffer.
+template <class C, bool FRESNEL, int STAGES>
+__global__ void __launch_bounds__(C::NT, C::MINB)
     kp_col(const Slot *const *slots, int nslots, int nx, int ny, const float2 *__restrict__ tw)
 {
+    static_assert(STAGES == 1 || STAGES == 2, "one or two stages");
     extern __shared__ __align__(1024) unsigned char smraw[];
     constexpr int TW = C::N * C::L;
     float2 *Pb0 = reinterpret_cast<float2 *>(smraw);
-    float2 *Pb1 = Pb0 + TW;
+    float2 *Pb1 = Pb0 + TW * (STAGES - 1);
     float *Mb0 = reinterpret_cast<float *>(Pb1 + TW);
-    float *Mb1 = Mb0 + TW;
+    float *Mb1 = Mb0 + TW * (STAGES - 1);
     uint64_t *bar = reinterpret_cast<uint64_t *>(Mb1 + TW);
     const int tps = ny / C::L;
     const int ntiles = tps * nslots;
@@ -63,33 +69,47 @@ __global__ void __launch_bounds__(C::NT, 1)
     }
     __syncthreads();
 
-    auto issue = [&](int tile, int b) {
+    // the first tile's reconstruction sets the wait limit (and the test hook
+    // that leaves the first tile's copy unissued, see Slot::skip_first_load)
+    const Slot &S0 = *slots[blockIdx.x / tps];
+    const uint32_t polls = S0.wait_polls ? S0.wait_polls : kWaitPolls;
+    const bool skip0 = S0.skip_first_load != 0;
+    auto issue = [&](int tile, int b, bool skip) {
         const Slot &S = *slots[tile / tps];
         const size_t off = (size_t)(tile % tps) * C::L * nx;
         tma::mbar_arrive_expect_tx(&bar[b], TW * 12);
+        if (skip) return;
         tma::bulk_load(b ? (void *)Pb1 : (void *)Pb0, S.P + off, TW * 8, &bar[b]);
         tma::bulk_load(b ? (void *)Mb1 : (void *)Mb0, S.mI + off, TW * 4, &bar[b]);
     };
     int t = blockIdx.x;
-    if (threadIdx.x == 0 && t < ntiles) issue(t, 0);
+    if (STAGES == 2 && threadIdx.x == 0 && t < ntiles) issue(t, 0, skip0);
 
     for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
-        const int b = it & 1;
+        const int b = STAGES == 2 ? (it & 1) : 0;
+        const uint32_t par = STAGES == 2 ? ((it >> 1) & 1) : (it & 1);
         float2 *Pb = b ? Pb1 : Pb0;
         const float *Mb = b ? Mb1 : Mb0;
         const Slot &S = *slots[t / tps];
         const int c0 = (t % tps) * (C::L / kPanel);
         const int tn = t + gridDim.x;
-        if (threadIdx.x == 0 && tn < ntiles) {
-            tma::bulk_wait_read_all();
-            issue(tn, b ^ 1);
+        if (threadIdx.x == 0) {
+            if (STAGES == 1) {
+                tma::bulk_wait_read_all();
+                issue(t, 0, it == 0 && skip0);
+            } else if (tn < ntiles) {
+                tma::bulk_wait_read_all();
+                issue(tn, b ^ 1, false);
+            }
         }
-        const bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, kWaitPolls);
+        const bool ok = tma::mbar_wait(&bar[b], par, polls);
         if (__syncthreads_or(!ok)) {
+            // every copy issued so far lands before the CTA leaves
             if (threadIdx.x == 0) {
                 raise_flag(S);
-                tma::mbar_wait(&bar[b], (it >> 1) & 1, kWaitPolls);
-                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, kWaitPolls);
+                tma::mbar_wait(&bar[b], par, polls);
+                if (STAGES == 2 && tn < ntiles)
+                    tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
             }
             break;
         }
@@ -155,11 +175,11 @@ __device__ __forceinline__ void finish_error(const Slot &S)
 template <int L>
 __host__ __device__ constexpr int tmap_index()
 {
-    return L == 4 ? 0 : (L == 8 ? 1 : 2);
+    return L == 2 ? 0 : (L == 4 ? 1 : (L == 8 ? 2 : 3));
 }
 
 template <class C>
-__global__ void __launch_bounds__(C::NT, 1)
+__global__ void __launch_bounds__(C::NT, C::MINB)
     kp_row(const Slot *const *slots, int nslots, int nx, int ny, const float2 *__restrict__ tw)
 {
     extern __shared__ __align__(1024) unsigned char smraw[];
@@ -185,11 +205,15 @@ __global__ void __launch_bounds__(C::NT, 1)
     for (int sl = blockIdx.x; sl < nslots; sl += gridDim.x) finish_error<C::NT>(*slots[sl]);
     __syncthreads();
 
-    auto issue_p = [&](int tile, int b) {
+    const Slot &S0 = *slots[blockIdx.x / tps];
+    const uint32_t polls = S0.wait_polls ? S0.wait_polls : kWaitPolls;
+    const bool skip0 = S0.skip_first_load != 0;
+    auto issue_p = [&](int tile, int b, bool skip) {
         const Slot &S = *slots[tile / tps];
         const int i0 = (tile % tps) * C::L;
         float2 *dst = b ? Pb1 : Pb0;
         tma::mbar_arrive_expect_tx(&bar[b], TW * 8);
+        if (skip) return;
         for (int c = 0; c < npan; c += boxp)
             tma::tensor_load_3d(dst + (size_t)c * C::L * kPanel, &S.tm[TM][0], 0, i0, c, &bar[b]);
     };
@@ -203,7 +227,7 @@ __global__ void __launch_bounds__(C::NT, 1)
         }
     };
     int t = blockIdx.x;
-    if (threadIdx.x == 0 && t < ntiles) issue_p(t, 0);
+    if (threadIdx.x == 0 && t < ntiles) issue_p(t, 0, skip0);
 
     for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
         const int b = it & 1;
@@ -214,15 +238,16 @@ __global__ void __launch_bounds__(C::NT, 1)
         if (threadIdx.x == 0) {
             tma::bulk_wait_read_all();
             issue_xs(t);
-            if (tn < ntiles) issue_p(tn, b ^ 1);
+            if (tn < ntiles) issue_p(tn, b ^ 1, false);
         }
-        bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, kWaitPolls);
+        bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
         if (__syncthreads_or(!ok)) {
+            // every copy issued so far lands before the CTA leaves
             if (threadIdx.x == 0) {
                 raise_flag(S);
-                tma::mbar_wait(&bar[b], (it >> 1) & 1, kWaitPolls);
-                tma::mbar_wait(&bar[2], it & 1, kWaitPolls);
-                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, kWaitPolls);
+                tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
+                tma::mbar_wait(&bar[2], it & 1, polls);
+                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
             }
             break;
         }
@@ -231,12 +256,12 @@ __global__ void __launch_bounds__(C::NT, 1)
         __syncthreads();
         transform<C, false>(v, Pb, tw);
 
-        ok = tma::mbar_wait(&bar[2], it & 1, kWaitPolls);
+        ok = tma::mbar_wait(&bar[2], it & 1, polls);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
                 raise_flag(S);
-                tma::mbar_wait(&bar[2], it & 1, kWaitPolls);
-                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, kWaitPolls);
+                tma::mbar_wait(&bar[2], it & 1, polls);
+                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
             }
             break;
         }

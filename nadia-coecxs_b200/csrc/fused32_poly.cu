@@ -15,7 +15,7 @@ namespace f32 {
 // Padded sizes with PolyCDI tiles: 256 and 512 (small cases) and 1080, the
 // 1024 x 1024 detector padded by 28 on each side (1080 = 6*6*6*5, so every
 // radix divides the 30 values a thread holds).  Swizzles from
-// swizzle_search.py.
+// tests/swizzle_search.py.
 const std::vector<PolyVariant> &poly_variants(int n)
 {
     static const std::map<int, std::vector<PolyVariant>> reg = [] {

@@ -1,5 +1,5 @@
 // fused32_v2048.cu -- the FP32 tile variants of transform length 2048.
-// Swizzles from swizzle_search.py (conflict-free exchanges).
+// Swizzles from tests/swizzle_search.py (conflict-free exchanges).
 #include "fused32_kernels.cuh"
 
 namespace nadia {
@@ -19,6 +19,11 @@ void add_variants_2048(std::vector<TileVariant> &v)
     v.push_back(make_ping<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
     v.push_back(make_ping<2048, 1024, 4, 1, Swizzle<4, 5, 3, 2>, 8, 8, 8, 4>("8.8.8.4"));
     v.push_back(make_ping<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
+    // two CTAs per SM: one-stage column tiles of 32 values a thread, row tiles of two rows
+    v.push_back(make_persistent_single<2048, 256, 4, 2, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
+    v.push_back(make_persistent_single<2048, 256, 4, 2, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
+    v.push_back(make_persistent_row<2048, 256, 2, 2, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
+    v.push_back(make_persistent_row<2048, 256, 2, 2, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
 }
 
 } // namespace f32

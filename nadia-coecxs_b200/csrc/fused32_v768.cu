@@ -1,5 +1,5 @@
 // fused32_v768.cu -- the FP32 tile variants of transform length 768.
-// Swizzles from swizzle_search.py (conflict-free exchanges).
+// Swizzles from tests/swizzle_search.py (conflict-free exchanges).
 #include "fused32_kernels.cuh"
 
 namespace nadia {

@@ -96,6 +96,18 @@ class PlanarCase:
         self.beam_stop = centre_beam_stop(n, ny, beam_stop) if beam_stop else None
 
 
+def random_phase_start(intensity, support, seed):
+    """The random-phase start estimate of the PlanarCDI workloads: inside the
+    support (> 0) a seeded phase uniform in [-pi, pi) with the constant
+    amplitude sqrt(sum(I) / pixels in the support), so that the estimate
+    carries the measured total intensity (the planar propagators are
+    unitary); zero outside the support.  Complex128, shape of `intensity`."""
+    inside = np.asarray(support) > 0
+    amp = math.sqrt(float(np.sum(intensity)) / max(int(inside.sum()), 1))
+    ph = rng(seed).uniform(-math.pi, math.pi, np.shape(intensity))
+    return np.where(inside, amp * np.exp(1j * ph), 0.0 + 0.0j)
+
+
 def planar_case(cfg):
     """Named workloads: 'c1' (256^2), 'c2' (1024^2), 'c3' (2048^2) and small 'tN' tests."""
     if cfg == "c1":

@@ -2,8 +2,9 @@
 
 Builds
   oracle/liboracle.so           the C restatement (nadia_oracle.c) + canonical FFT
-and, when the reference sources are present (default /root/reference, or
-$NADIA_REFERENCE), the reference's own hot-path sources compiled unmodified
+and, when the reference sources are present ($NADIA_REFERENCE, else a
+checkout named `reference` beside this repository), the reference's own
+hot-path sources compiled unmodified
 against the FFTW shim:
   oracle/_ref/libnadia_ref64.so       -DDOUBLE_PRECISION, -O2 -fno-fast-math  (parity)
   oracle/_ref/libnadia_ref64_fast.so  -DDOUBLE_PRECISION, -O3 -ffast-math     (timing)
@@ -78,7 +79,11 @@ def build_oracle(force=False):
 
 
 def reference_root():
-    root = os.environ.get("NADIA_REFERENCE", "/root/reference")
+    """The reference checkout: $NADIA_REFERENCE, else `reference` beside the
+    repository; None when its sources are absent (the prebuilt oracle/_ref
+    files are used as they are)."""
+    root = os.environ.get("NADIA_REFERENCE") or os.path.join(
+        os.path.dirname(os.path.dirname(HERE)), "reference")
     nadia = os.path.join(root, "NADIA")
     return nadia if os.path.isdir(os.path.join(nadia, "src")) else None
 

@@ -130,15 +130,20 @@ def poly_mixed(make, n=32, padding=2, seed=7):
             "support": s.get_support()}
 
 
-def config1(make, iterations=200, seed=0):
+def config1(make, iterations=200, seed=0, start="reference"):
     """PlanarCDI HIO FP64 at 256^2: disk R=40, sigma 2, 1e8 photons, 100x100
-    initial support, reference initialisation, beta 0.9, shrinkwrap every 20
-    (sigma 1.5, threshold 0.1)."""
+    initial support, beta 0.9, shrinkwrap every 20 (sigma 1.5, threshold
+    0.1).  start="reference": initialise_estimate(seed); start="random_phase":
+    the seeded random-phase estimate of synth.random_phase_start, set through
+    set_exit_surface_wave."""
     c = synth.planar_case("c1")
     s = make("planar", 256, 256)
     s.set_support(c.support)
     s.set_intensity(c.intensity)
-    s.initialise_estimate(seed)
+    if start == "random_phase":
+        s.set_exit_surface_wave(synth.random_phase_start(c.intensity, c.support, seed))
+    else:
+        s.initialise_estimate(seed)
     s.set_algorithm(HIO)
     errs = []
     for it in range(iterations):

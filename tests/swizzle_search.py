@@ -6,9 +6,9 @@ stores of the butterfly outputs and loads of the next pass's inputs -- and
 counts shared-memory wavefronts (16 lanes per wavefront for 8-byte words,
 one wavefront per distinct address per bank).  It searches the family
 a -> a ^ ((((a >> S1) ^ (a >> S2)) & M) << SH) for the smallest count and
-prints the variant table used in fused32_variants.cu.
+prints the swizzle of each variant registered in nadia-coecxs_b200/csrc/fused32_v*.cu.
 
-Usage: python nadia-coecxs_b200/csrc/swizzle_search.py
+Usage: python tests/swizzle_search.py
 """
 K = 4
 

@@ -148,7 +148,11 @@ def fresnel_pair(n):
     return out
 
 
-@pytest.mark.parametrize("n", [256, 1024])
+# the sizes of the FresnelCDI batch workload (512...2048) and 256
+FRESNEL_SIZES = [256, 512, 768, 1024, 1536, 2048]
+
+
+@pytest.mark.parametrize("n", FRESNEL_SIZES)
 def test_fresnel_fp32(n):
     a, b = fresnel_pair(n)
     assert l2rel(b.get_illumination_at_sample(), a.get_illumination_at_sample()) < 1e-6
@@ -169,6 +173,25 @@ def test_fresnel_fp32(n):
     L = np.abs(a.get_illumination_at_sample())
     lit = L > 1e-3 * L.max()
     assert l2rel(b.get_transmission()[lit], a.get_transmission()[lit]) <= 10 * RUN_TOL
+
+
+@pytest.mark.parametrize("n", FRESNEL_SIZES)
+def test_fresnel_teacher_forced_steps(n):
+    """Each FP32 FresnelCDI HIO step started from the FP64 state (which is
+    the oracle's, bit for bit) stays within one step's tolerance."""
+    a, b = fresnel_pair(n)
+    for s in (a, b):
+        s.set_algorithm("HIO")
+    worst = 0.0
+    for _ in range(3):
+        b.set_exit_surface_wave(a.get_exit_surface_wave())
+        a.iterate(1)
+        b.iterate(1)
+        de = abs(b.get_error() - a.get_error()) / a.get_error()
+        dx = l2rel(b.get_exit_surface_wave(), a.get_exit_surface_wave())
+        worst = max(worst, de, dx)
+        assert de <= STEP_TOL and dx <= STEP_TOL
+    print("fresnel teacher-forced n=%d worst step difference %.3g" % (n, worst))
 
 
 def test_fp32_unsupported_paths_report_status():

@@ -171,6 +171,19 @@ def test_config1_256_hio_200_shrinkwrap():
     assert np.array_equal(a["support"], b["support"])
 
 
+def test_config1_random_phase_start():
+    """Config 1 from its seeded random-phase start estimate (the same array
+    given to both through set_exit_surface_wave)."""
+    a = sc.config1(gpu, seed=17, start="random_phase")
+    b = sc.config1(orc, seed=17, start="random_phase")
+    assert sc.rel_err(a["errors"], b["errors"]) <= ERR_TOL
+    assert np.array_equal(a["esw"], b["esw"])
+    assert np.array_equal(a["support"], b["support"])
+    # the start differs from the reference initialisation's
+    c = sc.config1(orc, iterations=1, seed=17)
+    assert not np.array_equal(c["esw"], b["esw"])
+
+
 def config2(make, alg2=sc.HIO, beta2=0.9, iters=(50, 400, 50)):
     c = synth.planar_case("c2")
     s = make("planar", 1024, 1024)

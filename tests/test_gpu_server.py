@@ -144,6 +144,62 @@ def test_same_alone_and_in_the_mix():
         assert erra == errb
 
 
+def test_serving_request_types_same_alone_and_in_the_mix():
+    """The serving workload's own request types -- PlanarCDI FP32 at 1024^2
+    (radius 160) and 2048^2 (radius 320, 8x8 beam stop) and PolyCDI FP32 at
+    1024^2 padded to 1080^2 with the 10-line, 5% FWHM spectrum -- give the
+    same estimate, support and error alone and admitted among one another
+    under a budget that makes them queue (tolerance: exact).  100 HIO
+    iterations each, shrinkwrap every 50."""
+    p1 = synth.PlanarCase(1024, 160, 2, 1e8, seed=100, support_side=400)
+    p2 = synth.PlanarCase(2048, 320, 4, 1e9, seed=200, support_side=800, beam_stop=8)
+    pp = synth.PolyCase(1024, seed=300, padding=28)
+    common = dict(algorithm="HIO", beta=0.9, iterations=100, shrinkwrap_every=50,
+                  shrinkwrap_sigma=1.5, shrinkwrap_threshold=0.1)
+
+    def req(c, kind, seed):
+        def submit(srv):
+            if kind == "poly":
+                return srv.submit("poly", c.intensity, c.support, precision=pynadia.FP32,
+                                  spectrum=c.spectrum, seed=seed, **common)
+            return srv.submit("planar", c.intensity, c.support, precision=pynadia.FP32,
+                              beam_stop=c.beam_stop, seed=seed, **common)
+        return submit
+
+    probes = [req(p1, "planar", 1), req(p2, "planar", 2), req(pp, "poly", 3)]
+    alone = [run_alone(p) for p in probes]
+
+    est = pynadia.estimate_device_bytes
+    budget = (2 * est("planar", 2048, 2048, pynadia.FP32) + est("planar", 1024, 1024, pynadia.FP32)
+              + est("poly", 1024, 1024, pynadia.FP32, 0, (28, 28), 10))
+    srv = pynadia.Server(budget, max_active=4, chunk=25)
+    ids = [req(p2, "planar", 10)(srv), req(pp, "poly", 11)(srv), req(p1, "planar", 12)(srv)]
+    time.sleep(0.02)
+    probe_ids = [probes[0](srv)]
+    ids.append(req(pp, "poly", 13)(srv))
+    probe_ids.append(probes[1](srv))
+    ids.append(req(p1, "planar", 14)(srv))
+    probe_ids.append(probes[2](srv))
+    ids.append(req(p2, "planar", 15)(srv))
+    for rid in ids + probe_ids:
+        assert srv.wait(rid, 600)
+    st = srv.stats()
+    res, errors = {}, []
+    for rid in ids + probe_ids:
+        try:
+            res[rid] = srv.result(rid)
+        except pynadia.NadiaError as e:
+            errors.append((rid, str(e)))
+    srv.close()
+    assert not errors, errors
+    assert st["completed"] == len(ids) + len(probe_ids) and st["failed"] == 0, st
+    assert st["peak_bytes"] <= budget
+    for (ea, sa, erra, _), (eb, sb, errb, _) in zip(alone, [res[r] for r in probe_ids]):
+        assert np.array_equal(ea, eb)
+        assert np.array_equal(sa, sb)
+        assert erra == errb
+
+
 def oracle_sequence(c, n, seed, iterations, every, beta=0.9):
     o = po.Oracle("planar", n, n)
     o.set_support(c.support)

@@ -33,7 +33,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "nadia-coecxs_b200", "csrc")
 K = 4  # panel width
 
-PAT = re.compile(r"make_(variant|ping|persistent|poly)<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+),\s*"
+PAT = re.compile(r"make_(variant|ping|persistent_single|persistent_row|persistent|poly)<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+),\s*"
                  r"Swizzle<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+)>\s*,\s*([\d,\s]+)>")
 
 
@@ -167,8 +167,10 @@ def out_positions(v, mapf, first_radix):
 
 
 def maps_of(v):
-    ms = [("row", rowmap)]
-    if v["L"] % K == 0:
+    """The thread maps a variant runs: row-only variants have no column pass,
+    column-only (one-stage persistent) variants no row pass."""
+    ms = [] if v["kind"] == "persistent_single" else [("row", rowmap)]
+    if v["L"] % K == 0 and v["kind"] != "persistent_row":
         ms.insert(0, ("col", colmap))
     return ms
 
@@ -186,9 +188,15 @@ def test_tile_shape_constraints(v):
     E = N * L // NT
     assert E % reduce(lambda a, b: a * b // gcd(a, b), rad) == 0
     assert all((N // r) % K == 0 for r in rad), "row tiles need N/R divisible by the panel"
-    assert L % K == 0, "column tiles cover whole panels"
+    if v["kind"] != "persistent_row":
+        assert L % K == 0, "column tiles cover whole panels"
     if v["kind"] == "persistent":
         assert N * L * 28 + 24 <= 227 * 1024
+    # several CTAs per SM share its 228 KB (1 KB reserved per CTA)
+    if v["kind"] == "persistent_row":
+        assert v["minb"] * (N * L * 28 + 24 + 1024) <= 228 * 1024
+    if v["kind"] == "persistent_single":
+        assert v["minb"] * (N * L * 12 + 16 + 1024) <= 228 * 1024
 
 
 @pytest.mark.parametrize("v", VARIANTS, ids=vid)
@@ -213,8 +221,9 @@ def test_tile_transform_is_the_dft(v):
 
 @pytest.mark.parametrize("v", VARIANTS, ids=vid)
 def test_swizzle_wavefronts(v):
-    if CSRC not in sys.path:
-        sys.path.insert(0, CSRC)
+    here = os.path.dirname(os.path.abspath(__file__))
+    if here not in sys.path:
+        sys.path.insert(0, here)
     import swizzle_search as ss
     sw = swizzle(v["sw"])
     worst = 0.0
