@@ -7,6 +7,7 @@
 // batch (FP64, PolyCDI, n-best bookkeeping, algorithms with a PfPs term) are
 // stepped one by one on their own streams.
 #include <algorithm>
+#include <cstdlib>
 #include <atomic>
 #include <list>
 #include <map>
@@ -43,8 +44,24 @@ struct Group {
     cudaStream_t st = nullptr; // side stream (null for the first group)
 };
 
+// The members whose lengths have a mixed-length class: one column and one
+// row launch per iteration for all of them, whatever their sizes.
+struct Mixed {
+    std::vector<Solver *> members;
+    DevBuf<f32::Slot *> ptrs;
+    DevBuf<f32::MixItem> col_items, row_items;
+    int ncol_items = 0, nrow_items = 0;
+    bool empty() const { return members.empty(); }
+    void launch(cudaStream_t s) const
+    {
+        f32::mix_launch_col(col_items.p, ncol_items, ptrs.p, s);
+        f32::mix_launch_row(row_items.p, nrow_items, ptrs.p, (int)members.size(), s);
+    }
+};
+
 struct Plan {
     std::vector<unsigned long long> key;
+    Mixed mixed;
     std::vector<Group> groups;
     cudaStream_t st = nullptr;               // batch stream (first member's)
     std::vector<cudaEvent_t> fork, join;     // per side stream
@@ -65,10 +82,12 @@ struct Plan {
     void launch_block(int iters)
     {
         // fork side streams off the batch stream
-        for (size_t i = 1; i < groups.size(); ++i) {
+        for (size_t i = 0; i < groups.size(); ++i) {
+            if (!groups[i].st) continue;
             NADIA_CUDA(cudaEventRecord(fork[i], st));
             NADIA_CUDA(cudaStreamWaitEvent(groups[i].st, fork[i], 0));
         }
+        for (int it = 0; it < iters; ++it) mixed.launch(st);
         for (auto &g : groups) {
             cudaStream_t s = g.st ? g.st : st;
             const int n = (int)g.members.size();
@@ -83,7 +102,8 @@ struct Plan {
                 }
             }
         }
-        for (size_t i = 1; i < groups.size(); ++i) {
+        for (size_t i = 0; i < groups.size(); ++i) {
+            if (!groups[i].st) continue;
             NADIA_CUDA(cudaEventRecord(join[i], groups[i].st));
             NADIA_CUDA(cudaStreamWaitEvent(st, join[i], 0));
         }
@@ -91,7 +111,7 @@ struct Plan {
 
     long long launches_per_iter() const
     {
-        long long l = 0;
+        long long l = mixed.empty() ? 0 : 2;
         for (const auto &g : groups) l += g.launches_per_iter();
         return l;
     }
@@ -105,6 +125,48 @@ bool batchable(const Solver &s)
     return s.prec == NADIA_FP32 && s.n_best == 0 && !s.tc.active &&
            (s.kind != NADIA_POLY || s.f32->impl->pcol != nullptr) &&
            (s.algorithm == NADIA_ER || s.w[PFS] == 0);
+}
+
+// Planar/Fresnel reconstructions whose column length (nx) and row length (ny)
+// both have a mixed-length class run in the mixed passes, alone or not, so
+// their arithmetic never depends on the other handles of a call
+// (NADIA_MIXED=0 in the environment when a batch is first stepped keeps it on
+// the per-size tuned launches, for comparison)
+bool mixable(const Solver &s)
+{
+    const char *env = getenv("NADIA_MIXED");
+    if (env && env[0] == '0') return false;
+    return s.kind != NADIA_POLY && f32::mix_class_of(s.nx) >= 0 && f32::mix_class_of(s.ny) >= 0;
+}
+
+// the work lists: every column tile, then every row tile, of every member,
+// member by member (consecutive items go to consecutive CTAs, so each CTA's
+// share spreads over all members)
+void build_mixed(Mixed &m, cudaStream_t st)
+{
+    std::vector<f32::MixItem> col, row;
+    std::vector<f32::Slot *> hp;
+    for (size_t k = 0; k < m.members.size(); ++k) {
+        Solver *s = m.members[k];
+        const int cc = f32::mix_class_of(s->nx), rc = f32::mix_class_of(s->ny);
+        const int ct = s->ny / f32::mix_tile(cc), rt = s->nx / f32::mix_tile(rc);
+        for (int t = 0; t < ct; ++t) col.push_back({(int)k, t, cc, 0});
+        for (int t = 0; t < rt; ++t) row.push_back({(int)k, t, rc, 0});
+        hp.push_back(s->f32->impl->slot.p);
+    }
+    m.ncol_items = (int)col.size();
+    m.nrow_items = (int)row.size();
+    m.col_items.alloc(col.size());
+    m.row_items.alloc(row.size());
+    m.ptrs.alloc(hp.size());
+    NADIA_CUDA(cudaMemcpyAsync(m.col_items.p, col.data(), col.size() * sizeof(f32::MixItem),
+                               cudaMemcpyHostToDevice, st));
+    NADIA_CUDA(cudaMemcpyAsync(m.row_items.p, row.data(), row.size() * sizeof(f32::MixItem),
+                               cudaMemcpyHostToDevice, st));
+    NADIA_CUDA(cudaMemcpyAsync(m.ptrs.p, hp.data(), hp.size() * sizeof(f32::Slot *),
+                               cudaMemcpyHostToDevice, st));
+    // the host vectors are pageable: finish the copies before they go
+    NADIA_CUDA(cudaStreamSynchronize(st));
 }
 
 } // namespace
@@ -141,6 +203,10 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
         AllocScope scope(p->st);
         std::map<std::tuple<int, int, int, int, int>, size_t> index;
         for (Solver *s : fused) {
+            if (mixable(*s)) {
+                p->mixed.members.push_back(s);
+                continue;
+            }
             // PolyCDI members of a group share the padding too
             auto k = std::make_tuple(s->nx, s->ny, s->kind, s->kind == NADIA_POLY ? s->px : 0,
                                      s->kind == NADIA_POLY ? s->py : 0);
@@ -182,11 +248,17 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
             g.ptrs.alloc(hp.size());
             NADIA_CUDA(cudaMemcpyAsync(g.ptrs.p, hp.data(), hp.size() * sizeof(f32::Slot *),
                                        cudaMemcpyHostToDevice, p->st));
-            if (i > 0) {
+            // the first group shares the batch stream unless the mixed
+            // passes run there
+            if (i > 0 || !p->mixed.empty()) {
                 NADIA_CUDA(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
                 NADIA_CUDA(cudaEventCreateWithFlags(&p->fork[i], cudaEventDisableTiming));
                 NADIA_CUDA(cudaEventCreateWithFlags(&p->join[i], cudaEventDisableTiming));
             }
+        }
+        if (!p->mixed.empty()) {
+            f32::mix_prepare();
+            build_mixed(p->mixed, p->st);
         }
         g_plans.emplace_front(std::move(p));
         while (g_plans.size() > kMaxPlans) g_plans.pop_back();
@@ -201,6 +273,13 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
         if (s->st == plan->st) continue;
         NADIA_CUDA(cudaEventRecord(ev, s->st));
         NADIA_CUDA(cudaStreamWaitEvent(plan->st, ev, 0));
+    }
+    for (Solver *s : plan->mixed.members) {
+        Fused32::Impl &I = *s->f32->impl;
+        I.check_algorithm();
+        I.use_ncol(s->ny / f32::mix_tile(f32::mix_class_of(s->nx)));
+        I.push_slot_async(plan->st);
+        if (!I.p_valid) I.prime(plan->st);
     }
     for (auto &g : plan->groups)
         for (Solver *s : g.members) {
@@ -234,6 +313,7 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
     NADIA_CUDA(cudaEventRecord(ev, plan->st));
     for (Solver *s : fused) {
         s->iters += iterations;
+        s->f32->impl->q_valid = false; // only PfPs iterations carry Q (never batched)
         if (s->st != plan->st) NADIA_CUDA(cudaStreamWaitEvent(s->st, ev, 0));
     }
     NADIA_CUDA(cudaEventDestroy(ev));
@@ -256,12 +336,37 @@ void pass_times(Solver *const *solvers, int count, int reps, double out_us[3])
         std::lock_guard<std::mutex> lock(g_mu);
         plan = g_plans.front().get();
     }
-    Group &g = plan->groups[0];
     cudaStream_t st = plan->st;
-    const int n = (int)g.members.size();
     cudaEvent_t e[4];
     for (auto &x : e) NADIA_CUDA(cudaEventCreate(&x));
     float t[3] = {0, 0, 0};
+    if (!plan->mixed.empty()) {
+        // the members run in the mixed-length passes
+        const Mixed &m = plan->mixed;
+        for (int r = 0; r < reps; ++r) {
+            NADIA_CUDA(cudaEventRecord(e[0], st));
+            f32::mix_launch_col(m.col_items.p, m.ncol_items, m.ptrs.p, st);
+            NADIA_CUDA(cudaEventRecord(e[1], st));
+            NADIA_CUDA(cudaEventRecord(e[2], st));
+            f32::mix_launch_row(m.row_items.p, m.nrow_items, m.ptrs.p, (int)m.members.size(), st);
+            NADIA_CUDA(cudaEventRecord(e[3], st));
+            NADIA_CUDA(cudaEventSynchronize(e[3]));
+            for (int k = 0; k < 3; ++k) {
+                float ms = 0;
+                NADIA_CUDA(cudaEventElapsedTime(&ms, e[k], e[k + 1]));
+                t[k] += ms;
+            }
+        }
+        g_launches += 2LL * reps;
+        for (auto &x : e) cudaEventDestroy(x);
+        out_us[0] = 1000.0 * t[0] / reps;
+        out_us[1] = 0;
+        out_us[2] = 1000.0 * t[2] / reps;
+        for (Solver *s : m.members) s->iters += reps;
+        return;
+    }
+    Group &g = plan->groups[0];
+    const int n = (int)g.members.size();
     for (int r = 0; r < reps; ++r) {
         NADIA_CUDA(cudaEventRecord(e[0], st));
         if (g.pcol) {

@@ -745,13 +745,21 @@ extern "C" int nadia_tuned_tiles(int nx, int ny, int fresnel, int batched, char 
     return guard([&] {
         need(buf, "buf");
         NADIA_REQUIRE(len > 0, NADIA_ERR_INVALID, "empty buffer");
+        if (batched && nadia::f32::mix_class_of(nx) >= 0 && nadia::f32::mix_class_of(ny) >= 0) {
+            // batched Planar/Fresnel grids of these lengths run in the mixed-length passes
+            const std::string t = "column pass: " + nadia::f32::mix_describe(nx) +
+                                  "; row pass: " + nadia::f32::mix_describe(ny);
+            snprintf(buf, (size_t)len, "%s", t.c_str());
+            return;
+        }
         const nadia::f32::Choice &c = nadia::f32::choose(nx, ny, fresnel != 0, batched ? 4 : 1);
         auto desc = [](const nadia::f32::TileVariant *v) {
             char t[160];
-            snprintf(t, sizeof t, "n=%d threads=%d signals/tile=%d radices=%s%s", v->n, v->nt,
+            snprintf(t, sizeof t, "n=%d threads=%d signals/tile=%d radices=%s%s%s", v->n, v->nt,
                      v->L, v->radices,
                      v->single ? " persistent-TMA one stage"
-                               : (v->persistent ? " persistent-TMA" : (v->ping ? " ping" : "")));
+                               : (v->persistent ? " persistent-TMA" : (v->ping ? " ping" : "")),
+                     v->direct ? (v->ping && v->persistent ? " ping, sqrt(I) direct" : ", sqrt(I) direct") : "");
             return std::string(t);
         };
         char t[512];

@@ -383,11 +383,13 @@ __device__ __forceinline__ void pass_compute(float2 (&v)[C::E], const float2 *__
     }
 }
 
-// After pass p: write outputs to shared memory, then load the inputs of pass p+1.
+// After pass p: write outputs to shared memory, then load the inputs of pass
+// p+1.  PING tiles alternate between two buffers (sm0 after even passes, sm1
+// after odd ones).
 template <class C, bool FWD, int p>
-__device__ __forceinline__ void pass_exchange(float2 (&v)[C::E], float2 *sm0)
+__device__ __forceinline__ void pass_exchange(float2 (&v)[C::E], float2 *sm0, float2 *sm1)
 {
-    float2 *sm = (C::PING && (p & 1)) ? sm0 + C::N * C::L : sm0;
+    float2 *sm = (C::PING && (p & 1)) ? sm1 : sm0;
     constexpr int R = C::radix(p, FWD);
     constexpr int Ns = C::span(p, FWD);
     constexpr int NR = C::N / R;
@@ -428,14 +430,25 @@ __device__ __forceinline__ void pass_exchange(float2 (&v)[C::E], float2 *sm0)
     if (!C::PING) __syncthreads();
 }
 
-template <class C, bool FWD, int p = 0>
-__device__ __forceinline__ void transform(float2 (&v)[C::E], float2 *sm, const float2 *__restrict__ tw)
+// The whole transform; before_last() runs right before the last pass's
+// arithmetic (after its inputs have arrived), where a caller can start loads
+// that the values leaving the transform will need.
+template <class C, bool FWD, int p = 0, class H>
+__device__ __forceinline__ void transform_h(float2 (&v)[C::E], float2 *sm0, float2 *sm1,
+                                            const float2 *__restrict__ tw, H &&before_last)
 {
+    if constexpr (p + 1 == C::P) before_last();
     pass_compute<C, FWD, p>(v, tw);
     if constexpr (p + 1 < C::P) {
-        pass_exchange<C, FWD, p>(v, sm);
-        transform<C, FWD, p + 1>(v, sm, tw);
+        pass_exchange<C, FWD, p>(v, sm0, sm1);
+        transform_h<C, FWD, p + 1>(v, sm0, sm1, tw, before_last);
     }
+}
+
+template <class C, bool FWD>
+__device__ __forceinline__ void transform(float2 (&v)[C::E], float2 *sm, const float2 *__restrict__ tw)
+{
+    transform_h<C, FWD>(v, sm, sm + C::N * C::L, tw, [] {});
 }
 
 // Visit the (signal, position) of every value a thread holds at the input of

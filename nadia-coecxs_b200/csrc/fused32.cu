@@ -722,6 +722,7 @@ Fused32::Impl::Impl(Solver &s) : S(s)
 Fused32::Impl::~Impl()
 {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph_pfs) cudaGraphExecDestroy(graph_pfs);
 }
 
 void Fused32::Impl::use_choice(const f32::Choice *c)
@@ -746,12 +747,51 @@ bool Fused32::Impl::push_slot_async(cudaStream_t st)
     h_slot.w_ps = (float)w[PS];
     h_slot.w_psf = (float)w[PSF];
     h_slot.project = h_slot.er || w[PF] != 0 || w[PSF] != 0;
-    if (slot_uploaded && std::memcmp(&h_slot, &slot_on_device, sizeof(Slot)) == 0) return false;
+    h_slot.pfs = pfs_mode() ? 1 : 0;
+    h_slot.w_pfs = (float)w[PFS];
+    bool copied = false;
+    if (h_slot.pfs && qslot) {
+        // Q's column pass: the same reconstruction with Q as its work array
+        Slot q = h_slot;
+        q.P = Q.p;
+        q.partials = qpartials.p;
+        if (!qslot_uploaded || std::memcmp(&q, &qslot_on_device, sizeof(Slot)) != 0) {
+            NADIA_CUDA(cudaMemcpyAsync(qslot.p, &q, sizeof(Slot), cudaMemcpyHostToDevice, st));
+            qslot_on_device = q;
+            qslot_uploaded = true;
+            copied = true;
+        }
+    }
+    if (slot_uploaded && std::memcmp(&h_slot, &slot_on_device, sizeof(Slot)) == 0) return copied;
     // pageable source: the copy is staged before this returns
     NADIA_CUDA(cudaMemcpyAsync(slot.p, &h_slot, sizeof(Slot), cudaMemcpyHostToDevice, st));
     slot_on_device = h_slot;
     slot_uploaded = true;
     return true;
+}
+
+bool Fused32::Impl::pfs_mode() const { return S.algorithm != NADIA_ER && S.w[PFS] != 0; }
+
+// algorithms with a PfPs term: Q (rows of Ps x), its error partials and the
+// descriptor of its column pass, allocated on first use; the row pass runs
+// in a non-persistent variant (it carries two fields)
+void Fused32::Impl::prepare_pfs()
+{
+    if (!Q) {
+        Q.alloc(n);
+        qpartials.alloc(ny / kPanel);
+        qslot.alloc(1);
+        qslot_ptr.alloc(1);
+        NADIA_CUDA(cudaMemsetAsync(Q.p, 0, Q.bytes(), S.st));
+        NADIA_CUDA(cudaMemsetAsync(qpartials.p, 0, qpartials.bytes(), S.st));
+        Slot *qp = qslot.p;
+        NADIA_CUDA(cudaMemcpyAsync(qslot_ptr.p, &qp, sizeof(Slot *), cudaMemcpyHostToDevice, S.st));
+        NADIA_CUDA(cudaStreamSynchronize(S.st));
+        h_slot.Q = Q.p;
+        h_slot.qpartials = qpartials.p;
+        q_valid = false;
+    }
+    if (!pfs_choice) pfs_choice = &choose(nx, ny, S.kind == NADIA_FRESNEL, 1, true);
 }
 
 // Host arrays are in the reference's order (element (x, y) at x*ny + y); the
@@ -840,7 +880,11 @@ void Fused32::upload_beam_stop(const double *mask)
     impl->upload_intensity();
 }
 
-void Fused32::upload_support(const double *h) { impl->put_panel(h, 1, impl->sup.p, false); }
+void Fused32::upload_support(const double *h)
+{
+    impl->put_panel(h, 1, impl->sup.p, false);
+    impl->q_valid = false; // Q holds the rows of Ps x
+}
 
 void Fused32::soften_support()
 {
@@ -848,6 +892,7 @@ void Fused32::soften_support()
     impl->blur(false, impl->sup.p, 3.0, 5);
     NADIA_CUDA(cudaMemcpyAsync(impl->sup.p, impl->tmp2.p, impl->n * sizeof(float),
                                cudaMemcpyDeviceToDevice, impl->S.st));
+    impl->q_valid = false;
     impl->S.sync();
 }
 
@@ -1037,17 +1082,24 @@ void Fused32::copy_x_to(float2 *dst)
 
 void Fused32::Impl::check_algorithm() const
 {
-    NADIA_REQUIRE(S.algorithm == NADIA_ER || S.w[PFS] == 0, NADIA_ERR_UNSUPPORTED,
-                  "algorithms with a PfPs term (DM, custom m1/m5/m6/m7) run in the FP64 form");
+    if (!pfs_mode()) return;
+    NADIA_REQUIRE(S.kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
+                  "PolyCDI algorithms with a PfPs term (DM, custom m1/m5/m6/m7) run in the FP64 form");
+    NADIA_REQUIRE(!h_slot.tc_on, NADIA_ERR_UNSUPPORTED,
+                  "algorithms with a PfPs term run with a transmission constraint in the FP64 form");
 }
 
 void Fused32::Impl::prime(cudaStream_t st)
 {
     const Slot *const *sl = slot_ptr.p;
-    if (S.kind == NADIA_POLY)
+    if (S.kind == NADIA_POLY) {
         prow->row(kRowPrime, sl, 1, nx / prow->L, st, twy);
-    else
+    } else if (pfs_mode()) {
+        pfs_choice->row->row(kRowPrimePfs, sl, 1, nx, ny, twy, st);
+        q_valid = true;
+    } else {
         choice->row->row(kRowPrime, sl, 1, nx, ny, twy, st);
+    }
     g_launches += 1;
     p_valid = true;
 }
@@ -1059,6 +1111,18 @@ void Fused32::Impl::launch_iteration(cudaStream_t st)
     choice->row->row(kRowFull, sl, 1, nx, ny, twy, st);
 }
 
+// BaseCDI::iterate's generic path with a PfPs term (BaseCDI.c++:313-383):
+// the column pass projects both fields (x's rows in P, Ps x's rows in Q),
+// then one row pass forms the combine and both fields' rows for the next
+// iteration
+void Fused32::Impl::launch_iteration_pfs(cudaStream_t st)
+{
+    const bool fr = S.kind == NADIA_FRESNEL;
+    pfs_choice->col->col(fr, qslot_ptr.p, 1, nx, ny, twx, st);
+    pfs_choice->col->col(fr, slot_ptr.p, 1, nx, ny, twx, st);
+    pfs_choice->row->row(kRowPfs, slot_ptr.p, 1, nx, ny, twy, st);
+}
+
 void Fused32::iterate(int count)
 {
     Impl &I = *impl;
@@ -1067,31 +1131,40 @@ void Fused32::iterate(int count)
         return;
     }
     I.check_algorithm();
-    I.use_choice(I.choice);
+    const bool pfs = I.pfs_mode();
+    if (pfs) {
+        I.prepare_pfs();
+        I.use_choice(I.pfs_choice);
+    } else {
+        I.use_choice(I.choice);
+        I.q_valid = false; // Q is not carried by these iterations
+    }
     I.push_slot();
     cudaStream_t st = I.S.st;
-    if (!I.p_valid) I.prime(st);
+    if (!I.p_valid || (pfs && !I.q_valid)) I.prime(st);
+    const int per_iter = pfs ? 3 : 2;
+    cudaGraphExec_t &exec = pfs ? I.graph_pfs : I.graph_exec;
     // replay a captured graph of kGraphIters iterations, then the remainder
     const int G = Impl::kGraphIters;
     int left = count;
     if (left >= G) {
-        if (!I.graph_exec) {
+        if (!exec) {
             cudaGraph_t g = nullptr;
             NADIA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            for (int i = 0; i < G; ++i) I.launch_iteration(st);
+            for (int i = 0; i < G; ++i) pfs ? I.launch_iteration_pfs(st) : I.launch_iteration(st);
             NADIA_CUDA(cudaStreamEndCapture(st, &g));
-            NADIA_CUDA(cudaGraphInstantiate(&I.graph_exec, g, 0));
+            NADIA_CUDA(cudaGraphInstantiate(&exec, g, 0));
             cudaGraphDestroy(g);
         }
         while (left >= G) {
-            NADIA_CUDA(cudaGraphLaunch(I.graph_exec, st));
-            g_launches += 2 * G;
+            NADIA_CUDA(cudaGraphLaunch(exec, st));
+            g_launches += per_iter * G;
             left -= G;
         }
     }
     for (; left > 0; --left) {
-        I.launch_iteration(st);
-        g_launches += 2;
+        pfs ? I.launch_iteration_pfs(st) : I.launch_iteration(st);
+        g_launches += per_iter;
     }
     NADIA_CUDA(cudaGetLastError());
     I.S.iters += count;
@@ -1149,6 +1222,7 @@ void Fused32::Impl::blur(bool cplx, const void *in, double gauss_width, int cut)
 void Fused32::shrinkwrap(double gauss_width, double threshold)
 {
     Impl &I = *impl;
+    I.q_valid = false; // the support changes; Q holds the rows of Ps x
     I.blur(true, I.x.p, gauss_width, 4);
     const int nb = I.blur_blocks(), gb = Impl::kMaxBlocks;
     if (I.nx == I.ny) {

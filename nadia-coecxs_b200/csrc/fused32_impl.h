@@ -35,7 +35,15 @@ struct alignas(64) Slot {
     int ncol;               // column blocks per reconstruction
     float w_id, w_pf, w_ps, w_psf; // combine weights (1+PI, PF, PS, PSF)
     int er;                 // ER: x' = Ps Pf x
-    int project;            // the algorithm projects (else the error is carried over)
+    int project;            // the algorithm projects x (else the error is carried over,
+                            // or, with a PfPs term, taken from the projection of Ps x)
+    // algorithms with a PfPs term: Q holds the row transforms of Ps x (the
+    // second field the column pass projects), qpartials its error partials,
+    // w_pfs its weight in the combine
+    float2 *Q;
+    double *qpartials;
+    float w_pfs;
+    int pfs;
     float s0;               // 1/sqrt(nx*ny)
     double inv_norm2;       // 1 / sum of sqrt(I)^2 over measured pixels
     int *flag;              // raised when a device-side wait gives up
@@ -105,7 +113,10 @@ __host__ __device__ inline size_t panel_index_dev(int x, int y, int nx)
     return ((size_t)(y / 4) * nx + x) * 4 + (y % 4);
 }
 
-enum { kRowFull = 0, kRowPrime = 1 };
+// row-pass modes: the iteration's row pass; the forward row transform of x
+// alone (prime: P = rows of x); and the same two for algorithms with a PfPs
+// term, which also carry Q = rows of Ps x
+enum { kRowFull = 0, kRowPrime = 1, kRowPfs = 2, kRowPrimePfs = 3 };
 
 using ColLaunch = void (*)(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
                            const float2 *tw, cudaStream_t st);
@@ -120,6 +131,7 @@ struct TileVariant {
     bool persistent = false;
     bool ping = false;
     bool single = false; // persistent column pass with one stage per CTA
+    bool direct = false; // persistent column pass reading sqrt(I) from global memory
     const char *radices = "";
     void (*prepare)() = nullptr;
     ColLaunch col = nullptr;
@@ -157,6 +169,23 @@ struct Choice {
 // carry the transmission constraint)
 const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows = false);
 
+// Mixed-length persistent passes (fused32_mixed.cu): one launch per pass over
+// a work list of items (reconstruction index into the slot list, its column
+// or row tile, length class) of Planar/Fresnel reconstructions whose column
+// and row lengths both have a class.
+struct alignas(16) MixItem {
+    int slot, tile, cls, pad;
+};
+int mix_class_of(int n);   // the class of transform length n, or -1
+int mix_tile(int cls);     // signals per tile of a class
+int mix_len(int cls);
+int mix_threads();
+std::string mix_describe(int n);
+void mix_prepare();        // once per device, outside graph capture
+void mix_launch_col(const MixItem *items, int nitems, const Slot *const *slots, cudaStream_t st);
+void mix_launch_row(const MixItem *items, int nitems, const Slot *const *slots, int nslots,
+                    cudaStream_t st);
+
 const float2 *twiddle_table(int n);
 int sm_count();
 // tensor maps of a slot's P, x and support (needs P, x, sup set)
@@ -191,6 +220,18 @@ struct Fused32::Impl {
     DevBuf<int> gx, gy;
     const f32::PolyVariant *pcol = nullptr, *prow = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    // algorithms with a PfPs term (allocated on first use): Q, its error
+    // partials, the descriptor of Q's column pass, and non-persistent row
+    // variants (the PfPs row pass runs in those)
+    DevBuf<float2> Q;
+    DevBuf<double> qpartials;
+    DevBuf<f32::Slot> qslot;
+    DevBuf<f32::Slot *> qslot_ptr;
+    f32::Slot qslot_on_device{};
+    bool qslot_uploaded = false;
+    bool q_valid = false;
+    const f32::Choice *pfs_choice = nullptr;
+    cudaGraphExec_t graph_pfs = nullptr;
 
     explicit Impl(Solver &s);
     ~Impl();
@@ -199,6 +240,7 @@ struct Fused32::Impl {
     // the variants the next launches use (the handle's own, or a batch's);
     // sets the column-block count the row pass sums over
     void use_choice(const f32::Choice *c);
+    void use_ncol(int ncol) { h_slot.ncol = ncol; } // column tiles the row pass sums over
     // host arrays in the reference's order <-> device arrays in the panel
     // layout (stride 1: real, 2: complex; fold: PlanarCDI's centred detector
     // to transform order), converted on the host: plain copies on the device
@@ -212,6 +254,9 @@ struct Fused32::Impl {
     void check_algorithm() const;
     void prime(cudaStream_t st);
     void launch_iteration(cudaStream_t st);
+    bool pfs_mode() const; // the algorithm has a PfPs term (not ER)
+    void prepare_pfs();
+    void launch_iteration_pfs(cudaStream_t st);
 };
 
 } // namespace nadia

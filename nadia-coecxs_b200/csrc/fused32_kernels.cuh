@@ -126,6 +126,31 @@ __device__ __forceinline__ float2 tc_apply(float2 z, const Slot &S, size_t a, in
 }
 
 
+// finish the error metric of the column pass that just ran (block 0 of a
+// slot's row pass): from x's projection, or -- algorithms whose only
+// projection is of Ps x (a PfPs term alone) -- from Q's
+template <int NT>
+__device__ __forceinline__ void finish_error_row(const Slot &S)
+{
+    const double *part = S.project ? S.partials : (S.pfs ? S.qpartials : nullptr);
+    if (part) {
+        double t = 0.0;
+        for (int b = threadIdx.x; b < S.ncol; b += NT) t += part[b];
+        t = block_sum<NT>(t);
+        if (threadIdx.x == 0) {
+            const double e = t * S.inv_norm2;
+            long long it = *S.iter;
+            *S.err = e;
+            S.ring[it % S.ring_len] = e;
+            *S.iter = it + 1;
+        }
+    } else if (threadIdx.x == 0) {
+        long long it = *S.iter;
+        S.ring[it % S.ring_len] = *S.err;
+        *S.iter = it + 1;
+    }
+}
+
 template <class C, int MODE>
 __global__ void __launch_bounds__(C::NT, C::MINB) k_row(const Slot *const *slots, int nx, int ny,
                                                const float2 *__restrict__ tw)
@@ -138,23 +163,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_row(const Slot *const *slots
     float2 v[C::E];
 
     if (MODE == kRowFull) {
-        // finish the error metric of the column pass that just ran
-        if (blockIdx.x == 0 && S.project) {
-            double t = 0.0;
-            for (int b = threadIdx.x; b < S.ncol; b += C::NT) t += S.partials[b];
-            t = block_sum<C::NT>(t);
-            if (threadIdx.x == 0) {
-                const double e = t * S.inv_norm2;
-                long long it = *S.iter;
-                *S.err = e;
-                S.ring[it % S.ring_len] = e;
-                *S.iter = it + 1;
-            }
-        } else if (blockIdx.x == 0 && threadIdx.x == 0) {
-            long long it = *S.iter;
-            S.ring[it % S.ring_len] = *S.err;
-            *S.iter = it + 1;
-        }
+        if (blockIdx.x == 0) finish_error_row<C::NT>(S);
         for_each_slot<C, false, true>([&](int e, int s, int pos) {
             v[e] = P[paddr(i0 + s, pos, nx)];
         });
@@ -184,6 +193,51 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_row(const Slot *const *slots
             x[a] = xn;
             v[e] = xn;
         });
+    } else if (MODE == kRowPfs || MODE == kRowPrimePfs) {
+        // algorithms with a PfPs term (BaseCDI.c++:313-383): y = Pf x from P,
+        // z = Pf Ps x from Q, the five-term combine, then the rows of x' to P
+        // and of Ps x' to Q
+        float2 *__restrict__ Q = S.Q;
+        const float *__restrict__ sup = S.sup;
+        float2 w[C::E];
+        if (MODE == kRowPfs) {
+            if (blockIdx.x == 0) finish_error_row<C::NT>(S);
+            for_each_slot<C, false, true>([&](int e, int s, int pos) {
+                v[e] = P[paddr(i0 + s, pos, nx)];
+                w[e] = Q[paddr(i0 + s, pos, nx)];
+            });
+            transform<C, false>(v, sm, tw);
+            __syncthreads();
+            transform<C, false>(w, sm, tw);
+            const float wid = S.w_id, wpf = S.w_pf, wps = S.w_ps, wpsf = S.w_psf, wpfs = S.w_pfs;
+            for_each_slot<C, false, false>([&](int e, int s, int pos) {
+                const size_t a = paddr(i0 + s, pos, nx);
+                const float f = support_factor(__ldg(&sup[a]));
+                const float2 xk = x[a], y = v[e], z = w[e];
+                const float2 xn = make_float2(
+                    wid * xk.x + wpfs * z.x + wpf * y.x + wps * (f * xk.x) + wpsf * (f * y.x),
+                    wid * xk.y + wpfs * z.y + wpf * y.y + wps * (f * xk.y) + wpsf * (f * y.y));
+                x[a] = xn;
+                v[e] = xn;
+                w[e] = cscale(xn, f);
+            });
+        } else {
+            for_each_slot<C, true, true>([&](int e, int s, int pos) {
+                const size_t a = paddr(i0 + s, pos, nx);
+                v[e] = x[a];
+                w[e] = cscale(v[e], support_factor(__ldg(&sup[a])));
+            });
+        }
+        transform<C, true>(v, sm, tw);
+        for_each_slot<C, true, false>([&](int e, int s, int pos) {
+            P[paddr(i0 + s, pos, nx)] = v[e];
+        });
+        __syncthreads();
+        transform<C, true>(w, sm, tw);
+        for_each_slot<C, true, false>([&](int e, int s, int pos) {
+            Q[paddr(i0 + s, pos, nx)] = w[e];
+        });
+        return;
     } else {
         for_each_slot<C, true, true>([&](int e, int s, int pos) {
             v[e] = x[paddr(i0 + s, pos, nx)];
@@ -226,6 +280,8 @@ void prepare_variant()
     set_smem<CC>(k_col<CC, true>);
     set_smem<CR>(k_row<CR, kRowFull>);
     set_smem<CR>(k_row<CR, kRowPrime>);
+    set_smem<CR>(k_row<CR, kRowPfs>);
+    set_smem<CR>(k_row<CR, kRowPrimePfs>);
 }
 
 template <class C>
@@ -244,16 +300,25 @@ void launch_row(int mode, const Slot *const *slots, int nslots, int nx, int ny, 
                 cudaStream_t st)
 {
     dim3 grid(nx / C::L, nslots);
-    if (mode == kRowFull)
+    switch (mode) {
+    case kRowFull:
         k_row<C, kRowFull><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
-    else
+        break;
+    case kRowPrime:
         k_row<C, kRowPrime><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
+        break;
+    case kRowPfs:
+        k_row<C, kRowPfs><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
+        break;
+    default:
+        k_row<C, kRowPrimePfs><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
+    }
 }
 
 // shared memory of the persistent passes: STAGES stages of P and sqrt(I)
 // (column); two stages of P plus x and the support (row); and mbarriers
-template <class C, int STAGES = 2>
-constexpr size_t persist_col_smem() { return (size_t)C::N * C::L * 12 * STAGES + 16; }
+template <class C, int STAGES = 2, bool MDIRECT = false>
+constexpr size_t persist_col_smem() { return persist_col_bytes<C, STAGES, MDIRECT>(); }
 template <class C>
 constexpr size_t persist_row_smem() { return (size_t)C::N * C::L * 28 + 24; }
 
@@ -268,7 +333,7 @@ int resident_ctas(K kernel, int nt, size_t smem, int minb)
     return occ < minb ? occ : minb;
 }
 
-template <class C, int STAGES>
+template <class C, int STAGES, bool MDIRECT>
 struct PersistCol {
     static inline int per_sm = 1;
 };
@@ -277,15 +342,16 @@ struct PersistRow {
     static inline int per_sm = 1;
 };
 
-template <class C, int STAGES>
+template <class C, int STAGES, bool MDIRECT = false>
 void prepare_persistent_col()
 {
-    NADIA_CUDA(cudaFuncSetAttribute(kp_col<C, false, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)persist_col_smem<C, STAGES>()));
-    NADIA_CUDA(cudaFuncSetAttribute(kp_col<C, true, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)persist_col_smem<C, STAGES>()));
-    PersistCol<C, STAGES>::per_sm =
-        resident_ctas(kp_col<C, false, STAGES>, C::NT, persist_col_smem<C, STAGES>(), C::MINB);
+    constexpr int bytes = (int)persist_col_smem<C, STAGES, MDIRECT>();
+    NADIA_CUDA(cudaFuncSetAttribute(kp_col<C, false, STAGES, MDIRECT>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    NADIA_CUDA(cudaFuncSetAttribute(kp_col<C, true, STAGES, MDIRECT>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    PersistCol<C, STAGES, MDIRECT>::per_sm =
+        resident_ctas(kp_col<C, false, STAGES, MDIRECT>, C::NT, bytes, C::MINB);
 }
 
 template <class C>
@@ -293,6 +359,8 @@ void prepare_persistent_row()
 {
     set_smem<C>(k_row<C, kRowFull>);
     set_smem<C>(k_row<C, kRowPrime>);
+    set_smem<C>(k_row<C, kRowPfs>);
+    set_smem<C>(k_row<C, kRowPrimePfs>);
     NADIA_CUDA(cudaFuncSetAttribute(kp_row<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)persist_row_smem<C>()));
     PersistRow<C>::per_sm = resident_ctas(kp_row<C>, C::NT, persist_row_smem<C>(), C::MINB);
@@ -306,17 +374,18 @@ void prepare_persistent()
     prepare_persistent_row<CR>();
 }
 
-template <class C, int STAGES>
+template <class C, int STAGES, bool MDIRECT = false>
 void launch_col_persistent(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
                            const float2 *tw, cudaStream_t st)
 {
+    constexpr size_t bytes = persist_col_smem<C, STAGES, MDIRECT>();
     const int ntiles = (ny / C::L) * nslots;
-    const int cap = sm_count() * PersistCol<C, STAGES>::per_sm;
+    const int cap = sm_count() * PersistCol<C, STAGES, MDIRECT>::per_sm;
     const int grid = ntiles < cap ? ntiles : cap;
     if (fresnel)
-        kp_col<C, true, STAGES><<<grid, C::NT, persist_col_smem<C, STAGES>(), st>>>(slots, nslots, nx, ny, tw);
+        kp_col<C, true, STAGES, MDIRECT><<<grid, C::NT, bytes, st>>>(slots, nslots, nx, ny, tw);
     else
-        kp_col<C, false, STAGES><<<grid, C::NT, persist_col_smem<C, STAGES>(), st>>>(slots, nslots, nx, ny, tw);
+        kp_col<C, false, STAGES, MDIRECT><<<grid, C::NT, bytes, st>>>(slots, nslots, nx, ny, tw);
 }
 
 template <class C>
@@ -411,6 +480,39 @@ TileVariant make_persistent_single(const char *radices)
     t.prepare = &prepare_persistent_col<CC, 1>;
     t.col = &launch_col_persistent<CC, 1>;
     return t;
+}
+
+// A persistent column pass reading sqrt(I) straight from global memory:
+// STAGES stages of P, and with PING a second exchange buffer (one barrier per
+// exchange); no row pass.
+template <int STAGES, bool PING, int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_persistent_direct_t(const char *radices)
+{
+    using CC = TileCfg<N, NT, L, kColMap, Radices<Rs...>, SW, MINB, PING>;
+    static_assert(persist_col_smem<CC, STAGES, true>() * MINB <= 226 * 1024, "stages too large");
+    TileVariant t;
+    t.n = N;
+    t.nt = NT;
+    t.L = L;
+    t.minb = MINB;
+    t.persistent = true;
+    t.single = STAGES == 1;
+    t.ping = PING;
+    t.direct = true;
+    t.radices = radices;
+    t.prepare = &prepare_persistent_col<CC, STAGES, true>;
+    t.col = &launch_col_persistent<CC, STAGES, true>;
+    return t;
+}
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_persistent_direct(const char *radices)
+{
+    return make_persistent_direct_t<1, false, N, NT, L, MINB, SW, Rs...>(radices);
+}
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_persistent_ping(const char *radices)
+{
+    return make_persistent_direct_t<2, true, N, NT, L, MINB, SW, Rs...>(radices);
 }
 
 // A persistent row pass only: tiles of L rows (L = 2 allowed, below the

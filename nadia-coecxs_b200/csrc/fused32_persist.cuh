@@ -44,10 +44,22 @@ __device__ __forceinline__ void raise_flag(const Slot &S)
 }
 
 // STAGES = 2: tile i+1 loads while tile i is transformed.  STAGES = 1: one
-// buffer per CTA (half the shared memory, so two CTAs share an SM and each
-// one's load overlaps the other's arithmetic); the next load is issued once
-// the previous tile's store has read the buffer.
-template <class C, bool FRESNEL, int STAGES>
+// buffer per CTA (less shared memory, so two CTAs share an SM and each one's
+// load overlaps the other's arithmetic); the next load is issued once the
+// previous tile's store has read the buffer.
+// MDIRECT: sqrt(I) is not staged; each thread reads its values straight from
+// global memory (a warp reads 128 contiguous bytes), issued before the last
+// pass of the forward transform so that the loads overlap that pass.
+// C::PING: the exchanges alternate between the stage and one more tile
+// buffer, one barrier per exchange instead of two.
+// Shared memory: STAGES x (P [+ sqrt(I)]) [+ exchange buffer] + 2 mbarriers.
+template <class C, int STAGES, bool MDIRECT>
+constexpr size_t persist_col_bytes()
+{
+    return (size_t)C::N * C::L * (8 * STAGES + (MDIRECT ? 0 : 4 * STAGES) + (C::PING ? 8 : 0)) + 16;
+}
+
+template <class C, bool FRESNEL, int STAGES, bool MDIRECT>
 __global__ void __launch_bounds__(C::NT, C::MINB)
     kp_col(const Slot *const *slots, int nslots, int nx, int ny, const float2 *__restrict__ tw)
 {
@@ -57,10 +69,12 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     float2 *Pb0 = reinterpret_cast<float2 *>(smraw);
     float2 *Pb1 = Pb0 + TW * (STAGES - 1);
     float *Mb0 = reinterpret_cast<float *>(Pb1 + TW);
-    float *Mb1 = Mb0 + TW * (STAGES - 1);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(Mb1 + TW);
+    float *Mb1 = Mb0 + (MDIRECT ? 0 : TW * (STAGES - 1));
+    float2 *Xb = reinterpret_cast<float2 *>(Mb1 + (MDIRECT ? 0 : TW)); // PING only
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Xb + (C::PING ? TW : 0));
     const int tps = ny / C::L;
     const int ntiles = tps * nslots;
+    constexpr uint32_t kBytes = TW * (MDIRECT ? 8 : 12);
 
     if (threadIdx.x == 0) {
         tma::mbar_init(&bar[0], 1);
@@ -77,10 +91,11 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     auto issue = [&](int tile, int b, bool skip) {
         const Slot &S = *slots[tile / tps];
         const size_t off = (size_t)(tile % tps) * C::L * nx;
-        tma::mbar_arrive_expect_tx(&bar[b], TW * 12);
+        tma::mbar_arrive_expect_tx(&bar[b], kBytes);
         if (skip) return;
         tma::bulk_load(b ? (void *)Pb1 : (void *)Pb0, S.P + off, TW * 8, &bar[b]);
-        tma::bulk_load(b ? (void *)Mb1 : (void *)Mb0, S.mI + off, TW * 4, &bar[b]);
+        if (!MDIRECT)
+            tma::bulk_load(b ? (void *)Mb1 : (void *)Mb0, S.mI + off, TW * 4, &bar[b]);
     };
     int t = blockIdx.x;
     if (STAGES == 2 && threadIdx.x == 0 && t < ntiles) issue(t, 0, skip0);
@@ -114,22 +129,28 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             break;
         }
         float2 v[C::E];
+        float m[C::E];
         for_each_slot<C, true, true>([&](int e, int s, int pos) { v[e] = Pb[raw_col<C>(s, pos)]; });
         __syncthreads();
-        transform<C, true>(v, Pb, tw);
+        const float *mg = S.mI + (size_t)(t % tps) * C::L * nx;
+        transform_h<C, true>(v, Pb, Xb, tw, [&] {
+            if (MDIRECT)
+                for_each_slot<C, true, false>(
+                    [&](int e, int s, int kx) { m[e] = __ldg(&mg[raw_col<C>(s, kx)]); });
+        });
 
         const float s0 = S.s0;
         double diff = 0.0;
         for_each_slot<C, true, false>([&](int e, int s, int kx) {
-            const float m = Mb[raw_col<C>(s, kx)];
+            const float mm = MDIRECT ? m[e] : Mb[raw_col<C>(s, kx)];
             float2 X = v[e];
             if (!FRESNEL) {
-                X = cscale(modulus(cscale(X, s0), m, diff), s0);
+                X = cscale(modulus(cscale(X, s0), mm, diff), s0);
             } else {
                 const int ky = c0 * kPanel + s;
                 const float2 cf = cmul(__ldg(&S.tx[kx]), __ldg(&S.ty[ky]));
                 const float2 w = __ldg(&S.W[paddr(kx, ky, nx)]);
-                const float2 u = modulus(cadd(cscale(cmul(cf, X), s0), w), m, diff);
+                const float2 u = modulus(cadd(cscale(cmul(cf, X), s0), w), mm, diff);
                 X = cscale(cmulc(csub(u, w), cf), s0);
             }
             v[e] = X;
@@ -137,7 +158,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         const double tot = block_sum<C::NT>(diff);
         if (threadIdx.x == 0) S.partials[t % tps] = tot;
 
-        transform<C, false>(v, Pb, tw);
+        transform_h<C, false>(v, Pb, Xb, tw, [] {});
         for_each_slot<C, false, false>([&](int e, int s, int pos) { Pb[raw_col<C>(s, pos)] = v[e]; });
         tma::fence_async_shared();
         __syncthreads();
@@ -153,22 +174,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
 template <int NT>
 __device__ __forceinline__ void finish_error(const Slot &S)
 {
-    if (S.project) {
-        double t = 0.0;
-        for (int b = threadIdx.x; b < S.ncol; b += NT) t += S.partials[b];
-        t = block_sum<NT>(t);
-        if (threadIdx.x == 0) {
-            const double e = t * S.inv_norm2;
-            const long long it = *S.iter;
-            *S.err = e;
-            S.ring[it % S.ring_len] = e;
-            *S.iter = it + 1;
-        }
-    } else if (threadIdx.x == 0) {
-        const long long it = *S.iter;
-        S.ring[it % S.ring_len] = *S.err;
-        *S.iter = it + 1;
-    }
+    finish_error_row<NT>(S);
     __syncthreads();
 }
 

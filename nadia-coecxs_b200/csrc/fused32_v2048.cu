@@ -24,6 +24,12 @@ void add_variants_2048(std::vector<TileVariant> &v)
     v.push_back(make_persistent_single<2048, 256, 4, 2, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
     v.push_back(make_persistent_row<2048, 256, 2, 2, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
     v.push_back(make_persistent_row<2048, 256, 2, 2, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
+    // column passes reading sqrt(I) from global memory: one stage, two CTAs per
+    // SM; or two stages with ping-pong exchanges (one barrier per exchange)
+    v.push_back(make_persistent_direct<2048, 256, 4, 2, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
+    v.push_back(make_persistent_ping<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
+    v.push_back(make_persistent_ping<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
+    v.push_back(make_persistent_ping<2048, 1024, 4, 1, Swizzle<4, 5, 3, 2>, 8, 8, 8, 4>("8.8.8.4"));
 }
 
 } // namespace f32

@@ -195,14 +195,70 @@ def test_fresnel_teacher_forced_steps(n):
 
 
 def test_fp32_unsupported_paths_report_status():
-    b = pynadia.Solver("planar", 256, 256, precision=pynadia.FP32)
-    b.set_algorithm("DM")
-    with pytest.raises(pynadia.NadiaError) as e:
-        b.iterate(1)
-    assert e.value.code == 3
     with pytest.raises(pynadia.NadiaError) as e:
         pynadia.Solver("planar", 320, 320, precision=pynadia.FP32)
     assert e.value.code == 3
+
+
+# algorithms with a PfPs term (BaseCDI.c++:313-317): DM, and custom weight
+# sets whose only projection is of Ps x (m6: x + PfPs x - Ps x; m7: PfPs x),
+# so the error metric comes from that projection, and m1 (PsPf - PfPs)
+PFS_ALGS = [("DM", None), ("m6", (0, 0, 0, 0, 0, 1, 0, 0, 0, 0)),
+            ("m7", (0, 0, 0, 0, 0, 0, 1, 0, 0, 0)), ("m1", (1, 0, 0, 0, 0, 0, 0, 0, 0, 0))]
+
+
+def set_alg(s, name, m):
+    if m is None:
+        s.set_algorithm(name)
+    else:
+        s.set_custom_algorithm(m)
+
+
+@pytest.mark.parametrize("n,ny", [(256, 256), (1024, 1024), (512, 256)])
+@pytest.mark.parametrize("name,m", PFS_ALGS, ids=[a for a, _ in PFS_ALGS])
+def test_pfps_algorithms_match_fp64(n, ny, name, m):
+    a, b = planar_pair(n, ny, beam_stop=8)
+    for s in (a, b):
+        set_alg(s, name, m)
+        s.iterate(1)
+    assert abs(b.get_error() - a.get_error()) <= STEP_TOL * abs(a.get_error())
+    assert l2rel(b.get_exit_surface_wave(), a.get_exit_surface_wave()) <= STEP_TOL
+    for s in (a, b):
+        s.iterate(9)
+    ha, hb = a.get_error_history(10), b.get_error_history(10)
+    assert np.max(np.abs(hb - ha) / ha) <= RUN_TOL
+
+
+def test_pfps_switches_and_shrinkwrap():
+    """HIO -> DM -> shrinkwrap -> DM (graph replay) -> HIO -> DM, FP32 beside
+    FP64: the rows of Ps x are rebuilt whenever the estimate or the support
+    changed outside a PfPs iteration."""
+    a, b = planar_pair(256, beam_stop=6)
+    ea, eb = [], []
+    for s, errs in ((a, ea), (b, eb)):
+        s.set_algorithm("HIO")
+        s.iterate(3)
+        s.set_algorithm("DM")
+        s.iterate(4)
+        s.apply_shrinkwrap(1.5, 0.1)
+        s.iterate(17)
+        s.set_algorithm("HIO")
+        s.iterate(2)
+        s.set_algorithm("DM")
+        s.iterate(2)
+        errs.extend(s.get_error_history(28))
+    ea, eb = np.array(ea), np.array(eb)
+    assert np.max(np.abs(eb - ea) / ea) <= RUN_TOL
+
+
+def test_pfps_fresnel_matches_fp64():
+    a, b = fresnel_pair(256)
+    for s in (a, b):
+        s.set_algorithm("DM")
+        s.iterate(6)
+    ha, hb = a.get_error_history(6), b.get_error_history(6)
+    assert np.max(np.abs(hb - ha) / ha) <= RUN_TOL
+    assert l2rel(b.get_exit_surface_wave(), a.get_exit_surface_wave()) <= RUN_TOL
 
 
 def test_iterate_many_matches_individual_runs():

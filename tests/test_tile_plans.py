@@ -33,8 +33,15 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "nadia-coecxs_b200", "csrc")
 K = 4  # panel width
 
-PAT = re.compile(r"make_(variant|ping|persistent_single|persistent_row|persistent|poly)<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+),\s*"
+PAT = re.compile(r"make_(variant|ping|persistent_single|persistent_direct|persistent_ping|"
+                 r"persistent_row|persistent|poly)<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+),\s*"
                  r"Swizzle<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+)>\s*,\s*([\d,\s]+)>")
+
+
+# the classes of the mixed-length passes (fused32_mixed.cu): mix_class<N, L,
+# Swizzle<...>, radices...> at kMixNT threads
+MIX_PAT = re.compile(r"mix_class<\s*(\d+),\s*(\d+),\s*Swizzle<\s*(\d+),\s*(\d+),\s*(\d+),"
+                     r"\s*(\d+)>\s*,\s*([\d,\s]+)>")
 
 
 def registry():
@@ -47,6 +54,13 @@ def registry():
             rad = tuple(int(r) for r in m.group(10).split(","))
             out.append(dict(kind=m.group(1), N=n, NT=nt, L=L, minb=minb, sw=(s1, s2, msk, sh),
                             rad=rad, file=f))
+    src = open(os.path.join(CSRC, "fused32_mixed.cu")).read()
+    nt = int(re.search(r"constexpr int kMixNT = (\d+);", src).group(1))
+    for m in MIX_PAT.finditer(src):
+        n, L, s1, s2, msk, sh = (int(m.group(i)) for i in range(1, 7))
+        rad = tuple(int(r) for r in m.group(7).split(","))
+        out.append(dict(kind="mixed", N=n, NT=nt, L=L, minb=1, sw=(s1, s2, msk, sh), rad=rad,
+                        file="fused32_mixed.cu"))
     return out
 
 
@@ -166,10 +180,13 @@ def out_positions(v, mapf, first_radix):
     return np.array(pos)
 
 
+COLUMN_ONLY = ("persistent_single", "persistent_direct", "persistent_ping")
+
+
 def maps_of(v):
     """The thread maps a variant runs: row-only variants have no column pass,
     column-only (one-stage persistent) variants no row pass."""
-    ms = [] if v["kind"] == "persistent_single" else [("row", rowmap)]
+    ms = [] if v["kind"] in COLUMN_ONLY else [("row", rowmap)]
     if v["L"] % K == 0 and v["kind"] != "persistent_row":
         ms.insert(0, ("col", colmap))
     return ms
@@ -190,13 +207,17 @@ def test_tile_shape_constraints(v):
     assert all((N // r) % K == 0 for r in rad), "row tiles need N/R divisible by the panel"
     if v["kind"] != "persistent_row":
         assert L % K == 0, "column tiles cover whole panels"
-    if v["kind"] == "persistent":
+    if v["kind"] in ("persistent", "mixed"):
         assert N * L * 28 + 24 <= 227 * 1024
     # several CTAs per SM share its 228 KB (1 KB reserved per CTA)
     if v["kind"] == "persistent_row":
         assert v["minb"] * (N * L * 28 + 24 + 1024) <= 228 * 1024
     if v["kind"] == "persistent_single":
         assert v["minb"] * (N * L * 12 + 16 + 1024) <= 228 * 1024
+    if v["kind"] == "persistent_direct":
+        assert v["minb"] * (N * L * 8 + 16 + 1024) <= 228 * 1024
+    if v["kind"] == "persistent_ping":
+        assert v["minb"] * (N * L * 24 + 16 + 1024) <= 228 * 1024
 
 
 @pytest.mark.parametrize("v", VARIANTS, ids=vid)
