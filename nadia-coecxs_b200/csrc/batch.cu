@@ -44,19 +44,26 @@ struct Group {
     cudaStream_t st = nullptr; // side stream (null for the first group)
 };
 
-// The members whose lengths have a mixed-length class: one column and one
-// row launch per iteration for all of them, whatever their sizes.
+// The members of several grid sizes whose lengths all have a mixed-length
+// class: one column launch per kind (PlanarCDI, FresnelCDI) and one row
+// launch per iteration for all of them, whatever their sizes.
+struct MixList {
+    DevBuf<f32::MixItem> items;
+    DevBuf<int> bounds;
+    int ctas = 0;
+};
 struct Mixed {
     std::vector<Solver *> members;
     DevBuf<f32::Slot *> ptrs;
-    DevBuf<f32::MixItem> col_items, row_items;
-    int ncol_items = 0, nrow_items = 0;
+    MixList col[2], row; // col[1]: FresnelCDI members
     bool empty() const { return members.empty(); }
     void launch(cudaStream_t s) const
     {
-        f32::mix_launch_col(col_items.p, ncol_items, ptrs.p, s);
-        f32::mix_launch_row(row_items.p, nrow_items, ptrs.p, (int)members.size(), s);
+        for (int k = 0; k < 2; ++k)
+            f32::mix_launch_col(k == 1, col[k].items.p, col[k].bounds.p, col[k].ctas, ptrs.p, s);
+        f32::mix_launch_row(row.items.p, row.bounds.p, row.ctas, ptrs.p, (int)members.size(), s);
     }
+    int launches() const { return (col[0].ctas > 0) + (col[1].ctas > 0) + (row.ctas > 0); }
 };
 
 struct Plan {
@@ -111,7 +118,7 @@ struct Plan {
 
     long long launches_per_iter() const
     {
-        long long l = mixed.empty() ? 0 : 2;
+        long long l = mixed.launches();
         for (const auto &g : groups) l += g.launches_per_iter();
         return l;
     }
@@ -128,47 +135,72 @@ bool batchable(const Solver &s)
 }
 
 // Planar/Fresnel reconstructions whose column length (nx) and row length (ny)
-// both have a mixed-length class run in the mixed passes, alone or not, so
-// their arithmetic never depends on the other handles of a call
-// (NADIA_MIXED=0 in the environment when a batch is first stepped keeps it on
-// the per-size tuned launches, for comparison)
+// both have a mixed-length class run with their class's tile configuration,
+// alone or not: in the mixed passes when the call holds several such sizes,
+// in that configuration's single-length passes otherwise; either way the
+// same arithmetic, so a reconstruction's result never depends on the other
+// handles of a call.  (NADIA_MIXED=0 in the environment when a batch is
+// first stepped keeps it on the per-size tuned launches, for comparison.)
 bool mixable(const Solver &s)
 {
     const char *env = getenv("NADIA_MIXED");
     if (env && env[0] == '0') return false;
-    return s.kind != NADIA_POLY && f32::mix_class_of(s.nx) >= 0 && f32::mix_class_of(s.ny) >= 0;
+    return s.kind != NADIA_POLY && f32::mix_variant(s.nx) && f32::mix_variant(s.ny);
 }
 
-// the work lists: every column tile, then every row tile, of every member,
-// member by member (consecutive items go to consecutive CTAs, so each CTA's
-// share spreads over all members)
-void build_mixed(Mixed &m, cudaStream_t st)
+void upload_list(MixList &l, std::vector<f32::MixItem> &items, cudaStream_t st)
 {
-    std::vector<f32::MixItem> col, row;
-    std::vector<f32::Slot *> hp;
-    for (size_t k = 0; k < m.members.size(); ++k) {
-        Solver *s = m.members[k];
-        const int cc = f32::mix_class_of(s->nx), rc = f32::mix_class_of(s->ny);
-        const int ct = s->ny / f32::mix_tile(cc), rt = s->nx / f32::mix_tile(rc);
-        for (int t = 0; t < ct; ++t) col.push_back({(int)k, t, cc, 0});
-        for (int t = 0; t < rt; ++t) row.push_back({(int)k, t, rc, 0});
-        hp.push_back(s->f32->impl->slot.p);
-    }
-    m.ncol_items = (int)col.size();
-    m.nrow_items = (int)row.size();
-    m.col_items.alloc(col.size());
-    m.row_items.alloc(row.size());
-    m.ptrs.alloc(hp.size());
-    NADIA_CUDA(cudaMemcpyAsync(m.col_items.p, col.data(), col.size() * sizeof(f32::MixItem),
+    if (items.empty()) return;
+    std::vector<int> bounds;
+    l.ctas = std::min<int>(f32::mix_ctas(), (int)items.size());
+    f32::mix_order(items, bounds, l.ctas);
+    l.items.alloc(items.size());
+    l.bounds.alloc(bounds.size());
+    NADIA_CUDA(cudaMemcpyAsync(l.items.p, items.data(), items.size() * sizeof(f32::MixItem),
                                cudaMemcpyHostToDevice, st));
-    NADIA_CUDA(cudaMemcpyAsync(m.row_items.p, row.data(), row.size() * sizeof(f32::MixItem),
-                               cudaMemcpyHostToDevice, st));
-    NADIA_CUDA(cudaMemcpyAsync(m.ptrs.p, hp.data(), hp.size() * sizeof(f32::Slot *),
+    NADIA_CUDA(cudaMemcpyAsync(l.bounds.p, bounds.data(), bounds.size() * sizeof(int),
                                cudaMemcpyHostToDevice, st));
     // the host vectors are pageable: finish the copies before they go
     NADIA_CUDA(cudaStreamSynchronize(st));
 }
 
+// the work lists: every column tile (by kind) and every row tile of every
+// member, ordered by class and cut into per-CTA ranges
+void build_mixed(Mixed &m, cudaStream_t st)
+{
+    std::vector<f32::MixItem> col[2], row;
+    std::vector<f32::Slot *> hp;
+    for (size_t k = 0; k < m.members.size(); ++k) {
+        Solver *s = m.members[k];
+        const int cc = f32::mix_class_of(s->nx), rc = f32::mix_class_of(s->ny);
+        const int ct = s->ny / f32::mix_tile(cc), rt = s->nx / f32::mix_tile(rc);
+        auto &cl = col[s->kind == NADIA_FRESNEL ? 1 : 0];
+        for (int t = 0; t < ct; ++t) cl.push_back({(int)k, t, cc, 0});
+        for (int t = 0; t < rt; ++t) row.push_back({(int)k, t, rc, 0});
+        hp.push_back(s->f32->impl->slot.p);
+    }
+    m.ptrs.alloc(hp.size());
+    NADIA_CUDA(cudaMemcpyAsync(m.ptrs.p, hp.data(), hp.size() * sizeof(f32::Slot *),
+                               cudaMemcpyHostToDevice, st));
+    for (int k = 0; k < 2; ++k) upload_list(m.col[k], col[k], st);
+    upload_list(m.row, row, st);
+}
+
+// the fixed choice of a mixable grid: its classes' single-length variants
+const f32::Choice &class_choice(int nx, int ny)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, f32::Choice> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    f32::Choice &c = cache[{nx, ny}];
+    if (!c.col) {
+        c.col = f32::mix_variant(nx);
+        c.row = f32::mix_variant(ny);
+        c.col->prepare();
+        c.row->prepare();
+    }
+    return c;
+}
 } // namespace
 
 void iterate_many(Solver *const *solvers, int count, int iterations)
@@ -202,8 +234,15 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
         // outlives the plan: plans go before their members' streams do)
         AllocScope scope(p->st);
         std::map<std::tuple<int, int, int, int, int>, size_t> index;
+        // mixable members of more than one grid size share the mixed passes
+        std::vector<Solver *> mix;
+        for (Solver *s : fused)
+            if (mixable(*s)) mix.push_back(s);
+        bool several = false;
+        for (Solver *s : mix)
+            several |= s->nx != mix[0]->nx || s->ny != mix[0]->ny;
         for (Solver *s : fused) {
-            if (mixable(*s)) {
+            if (several && mixable(*s)) {
                 p->mixed.members.push_back(s);
                 continue;
             }
@@ -238,8 +277,10 @@ void iterate_many(Solver *const *solvers, int count, int iterations)
                 g.twy = I0.twy;
             } else {
                 // the batched tuning class for every group, whatever its size, so a
-                // handle's arithmetic does not depend on the other handles of the call
-                g.choice = &f32::choose(g.nx, g.ny, g.fresnel, kBatchClass);
+                // handle's arithmetic does not depend on the other handles of the
+                // call; mixable grids use their classes' configuration
+                g.choice = mixable(*g.members[0]) ? &class_choice(g.nx, g.ny)
+                                                  : &f32::choose(g.nx, g.ny, g.fresnel, kBatchClass);
                 g.twx = f32::twiddle_table(g.nx);
                 g.twy = f32::twiddle_table(g.ny);
             }
@@ -345,10 +386,13 @@ void pass_times(Solver *const *solvers, int count, int reps, double out_us[3])
         const Mixed &m = plan->mixed;
         for (int r = 0; r < reps; ++r) {
             NADIA_CUDA(cudaEventRecord(e[0], st));
-            f32::mix_launch_col(m.col_items.p, m.ncol_items, m.ptrs.p, st);
+            for (int k = 0; k < 2; ++k)
+                f32::mix_launch_col(k == 1, m.col[k].items.p, m.col[k].bounds.p, m.col[k].ctas,
+                                    m.ptrs.p, st);
             NADIA_CUDA(cudaEventRecord(e[1], st));
             NADIA_CUDA(cudaEventRecord(e[2], st));
-            f32::mix_launch_row(m.row_items.p, m.nrow_items, m.ptrs.p, (int)m.members.size(), st);
+            f32::mix_launch_row(m.row.items.p, m.row.bounds.p, m.row.ctas, m.ptrs.p,
+                                (int)m.members.size(), st);
             NADIA_CUDA(cudaEventRecord(e[3], st));
             NADIA_CUDA(cudaEventSynchronize(e[3]));
             for (int k = 0; k < 3; ++k) {
@@ -357,7 +401,7 @@ void pass_times(Solver *const *solvers, int count, int reps, double out_us[3])
                 t[k] += ms;
             }
         }
-        g_launches += 2LL * reps;
+        g_launches += (long long)m.launches() * reps;
         for (auto &x : e) cudaEventDestroy(x);
         out_us[0] = 1000.0 * t[0] / reps;
         out_us[1] = 0;

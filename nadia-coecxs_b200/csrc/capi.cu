@@ -745,8 +745,8 @@ extern "C" int nadia_tuned_tiles(int nx, int ny, int fresnel, int batched, char 
     return guard([&] {
         need(buf, "buf");
         NADIA_REQUIRE(len > 0, NADIA_ERR_INVALID, "empty buffer");
-        if (batched && nadia::f32::mix_class_of(nx) >= 0 && nadia::f32::mix_class_of(ny) >= 0) {
-            // batched Planar/Fresnel grids of these lengths run in the mixed-length passes
+        if (batched && nadia::f32::mix_variant(nx) && nadia::f32::mix_variant(ny)) {
+            // batched Planar/Fresnel grids of these lengths run with their classes' tiles
             const std::string t = "column pass: " + nadia::f32::mix_describe(nx) +
                                   "; row pass: " + nadia::f32::mix_describe(ny);
             snprintf(buf, (size_t)len, "%s", t.c_str());

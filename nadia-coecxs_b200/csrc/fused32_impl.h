@@ -181,10 +181,16 @@ int mix_tile(int cls);     // signals per tile of a class
 int mix_len(int cls);
 int mix_threads();
 std::string mix_describe(int n);
+int mix_ctas();            // CTAs of a mixed launch
+// orders items by class and cuts them into `ctas` ranges of equal estimated work
+void mix_order(std::vector<MixItem> &items, std::vector<int> &bounds, int ctas);
+struct TileVariant;
+const TileVariant *mix_variant(int n); // the single-length variant of n's class
 void mix_prepare();        // once per device, outside graph capture
-void mix_launch_col(const MixItem *items, int nitems, const Slot *const *slots, cudaStream_t st);
-void mix_launch_row(const MixItem *items, int nitems, const Slot *const *slots, int nslots,
-                    cudaStream_t st);
+void mix_launch_col(bool fresnel, const MixItem *items, const int *bounds, int ctas,
+                    const Slot *const *slots, cudaStream_t st);
+void mix_launch_row(const MixItem *items, const int *bounds, int ctas, const Slot *const *slots,
+                    int nslots, cudaStream_t st);
 
 const float2 *twiddle_table(int n);
 int sm_count();

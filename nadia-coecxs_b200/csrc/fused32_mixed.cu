@@ -7,8 +7,10 @@
 // pass (P, plus x and the support) fit in shared memory.
 #include "fused32_mixed.cuh"
 
+#include <algorithm>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 namespace nadia {
 namespace f32 {
@@ -56,30 +58,76 @@ MixTw tables()
     for (int c = 0; c < ColFam::K; ++c) t.t[c] = twiddle_table(ColFam::len(c));
     return t;
 }
+
+// estimated work of one tile of a class: values x passes
+double tile_cost(int cls)
+{
+    static const int passes[] = {3, 5, 3, 4, 3};
+    return (double)ColFam::len(cls) * ColFam::tile(cls) * passes[cls];
+}
 } // namespace
+
+int mix_ctas() { return sm_count(); }
+
+// Orders the items by class (stable: member order within a class) and cuts
+// the list into `ctas` contiguous ranges of about equal estimated work;
+// bounds gets ctas + 1 entries.
+void mix_order(std::vector<MixItem> &items, std::vector<int> &bounds, int ctas)
+{
+    std::stable_sort(items.begin(), items.end(),
+                     [](const MixItem &a, const MixItem &b) { return a.cls < b.cls; });
+    double total = 0;
+    for (const auto &m : items) total += tile_cost(m.cls);
+    bounds.assign(ctas + 1, (int)items.size());
+    bounds[0] = 0;
+    double acc = 0;
+    int b = 1;
+    for (size_t i = 0; i < items.size() && b < ctas; ++i) {
+        acc += tile_cost(items[i].cls);
+        while (b < ctas && acc >= total * b / ctas) bounds[b++] = (int)i + 1;
+    }
+}
+
+// The persistent single-length variant with a class's tile configuration:
+// a batch of one grid size runs it (the same arithmetic as the class in the
+// mixed passes, without the other classes' code)
+const TileVariant *mix_variant(int n)
+{
+    const int c = mix_class_of(n);
+    if (c < 0) return nullptr;
+    for (const auto &v : variants(n))
+        if (v.persistent && !v.single && !v.direct && v.col && v.row && v.nt == kMixNT &&
+            v.L == ColFam::tile(c) && std::string(v.radices) == kMixRadices[c])
+            return &v;
+    return nullptr;
+}
 
 void mix_prepare()
 {
-    NADIA_CUDA(cudaFuncSetAttribute(kp_colm<ColFam>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    NADIA_CUDA(cudaFuncSetAttribute(kp_colm<ColFam, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)mix_col_smem<ColFam>()));
+    NADIA_CUDA(cudaFuncSetAttribute(kp_colm<ColFam, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)mix_col_smem<ColFam>()));
     NADIA_CUDA(cudaFuncSetAttribute(kp_rowm<RowFam>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)mix_row_smem<RowFam>()));
     tables(); // the twiddle tables exist before any capture
 }
 
-void mix_launch_col(const MixItem *items, int nitems, const Slot *const *slots, cudaStream_t st)
+void mix_launch_col(bool fresnel, const MixItem *items, const int *bounds, int ctas,
+                    const Slot *const *slots, cudaStream_t st)
 {
-    if (nitems <= 0) return;
-    const int grid = nitems < sm_count() ? nitems : sm_count();
-    kp_colm<ColFam><<<grid, kMixNT, mix_col_smem<ColFam>(), st>>>(items, nitems, slots, tables());
+    if (ctas <= 0) return;
+    if (fresnel)
+        kp_colm<ColFam, true><<<ctas, kMixNT, mix_col_smem<ColFam>(), st>>>(items, bounds, slots, tables());
+    else
+        kp_colm<ColFam, false><<<ctas, kMixNT, mix_col_smem<ColFam>(), st>>>(items, bounds, slots, tables());
 }
 
-void mix_launch_row(const MixItem *items, int nitems, const Slot *const *slots, int nslots,
-                    cudaStream_t st)
+void mix_launch_row(const MixItem *items, const int *bounds, int ctas, const Slot *const *slots,
+                    int nslots, cudaStream_t st)
 {
-    if (nitems <= 0) return;
-    const int grid = nitems < sm_count() ? nitems : sm_count();
-    kp_rowm<RowFam><<<grid, kMixNT, mix_row_smem<RowFam>(), st>>>(items, nitems, slots, nslots,
+    if (ctas <= 0) return;
+    kp_rowm<RowFam><<<ctas, kMixNT, mix_row_smem<RowFam>(), st>>>(items, bounds, slots, nslots,
                                                                  tables());
 }
 

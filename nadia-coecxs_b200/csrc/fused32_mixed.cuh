@@ -4,9 +4,12 @@
 // A launch walks a work list of items (reconstruction, tile, length class).
 // Every length class is a tile configuration of the same thread count, so
 // one kernel holds the code of all of them and picks the class per item; the
-// shared-memory stages are sized for the largest tile.  Items are dealt to
-// CTAs round-robin; the TMA pipeline brings item i+1 (whatever its class)
-// while item i is transformed, as in the single-length persistent passes.
+// shared-memory stages are sized for the largest tile.  The list is ordered
+// by class and each CTA takes one contiguous range of it, cut so that the
+// ranges carry equal estimated work: a CTA runs one class (two where its range
+// crosses a class boundary), so its instruction working set stays that of one
+// tile shape.  The TMA pipeline brings item i+1 (whatever its class) while
+// item i is transformed, as in the single-length persistent passes.
 //
 // The per-tile arithmetic is that of the single-length persistent passes
 // (fused32_persist.cuh) for the class's tile configuration: a reconstruction's
@@ -99,9 +102,10 @@ constexpr size_t mix_row_smem() { return (size_t)F::TW * 28 + 24; }
 // Column pass over a work list (classes: column-map tile configurations).
 // Stages: two of P and sqrt(I), as in kp_col<C, FRESNEL, 2, false>; FresnelCDI
 // items (a slot with phase factors) add the white field and the factors.
-template <class F>
+template <class F, bool FRESNEL>
 __global__ void __launch_bounds__(F::NT, 1)
-    kp_colm(const MixItem *__restrict__ items, int nitems, const Slot *const *slots, MixTw tws)
+    kp_colm(const MixItem *__restrict__ items, const int *__restrict__ bounds,
+            const Slot *const *slots, MixTw tws)
 {
     extern __shared__ __align__(1024) unsigned char smraw[];
     constexpr int TW = F::TW;
@@ -118,7 +122,9 @@ __global__ void __launch_bounds__(F::NT, 1)
     }
     __syncthreads();
 
-    const MixItem first = items[blockIdx.x < nitems ? blockIdx.x : 0];
+    // this CTA's items: [t0, t1) of the list (ordered by class)
+    const int t0 = bounds[blockIdx.x], t1 = bounds[blockIdx.x + 1];
+    const MixItem first = items[t0 < t1 ? t0 : 0];
     const Slot &S0 = *slots[first.slot];
     const uint32_t polls = S0.wait_polls ? S0.wait_polls : kWaitPolls;
     const bool skip0 = S0.skip_first_load != 0;
@@ -134,18 +140,18 @@ __global__ void __launch_bounds__(F::NT, 1)
             tma::bulk_load(b ? (void *)Mb1 : (void *)Mb0, S.mI + off, tw * 4, &bar[b]);
         });
     };
-    int t = blockIdx.x;
-    if (threadIdx.x == 0 && t < nitems) issue(items[t], 0, skip0);
+    int t = t0;
+    if (threadIdx.x == 0 && t < t1) issue(items[t], 0, skip0);
 
-    for (int it = 0; t < nitems; ++it, t += gridDim.x) {
+    for (int it = 0; t < t1; ++it, ++t) {
         const int b = it & 1;
         const uint32_t par = (it >> 1) & 1;
         float2 *Pb = b ? Pb1 : Pb0;
         const float *Mb = b ? Mb1 : Mb0;
         const MixItem m = items[t];
         const Slot &S = *slots[m.slot];
-        const int tn = t + gridDim.x;
-        if (threadIdx.x == 0 && tn < nitems) {
+        const int tn = t + 1;
+        if (threadIdx.x == 0 && tn < t1) {
             tma::bulk_wait_read_all();
             issue(items[tn], b ^ 1, false);
         }
@@ -155,7 +161,7 @@ __global__ void __launch_bounds__(F::NT, 1)
             if (threadIdx.x == 0) {
                 raise_flag(S);
                 tma::mbar_wait(&bar[b], par, polls);
-                if (tn < nitems) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+                if (tn < t1) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
             }
             break;
         }
@@ -169,12 +175,11 @@ __global__ void __launch_bounds__(F::NT, 1)
             __syncthreads();
             transform<C, true>(v, Pb, tw);
             const float s0 = S.s0;
-            const bool fresnel = S.tx != nullptr;
             double diff = 0.0;
             for_each_slot<C, true, false>([&](int e, int s, int kx) {
                 const float mm = Mb[raw_col<C>(s, kx)];
                 float2 X = v[e];
-                if (!fresnel) {
+                if (!FRESNEL) {
                     X = cscale(modulus(cscale(X, s0), mm, diff), s0);
                 } else {
                     const int ky = c0 * kPanel + s;
@@ -207,8 +212,8 @@ __global__ void __launch_bounds__(F::NT, 1)
 // CTAs first finish the error metrics of the reconstructions in `slots`.
 template <class F>
 __global__ void __launch_bounds__(F::NT, 1)
-    kp_rowm(const MixItem *__restrict__ items, int nitems, const Slot *const *slots, int nslots,
-            MixTw tws)
+    kp_rowm(const MixItem *__restrict__ items, const int *__restrict__ bounds,
+            const Slot *const *slots, int nslots, MixTw tws)
 {
     extern __shared__ __align__(1024) unsigned char smraw[];
     constexpr int TW = F::TW;
@@ -227,7 +232,8 @@ __global__ void __launch_bounds__(F::NT, 1)
     for (int sl = blockIdx.x; sl < nslots; sl += gridDim.x) finish_error<F::NT>(*slots[sl]);
     __syncthreads();
 
-    const MixItem first = items[blockIdx.x < nitems ? blockIdx.x : 0];
+    const int t0 = bounds[blockIdx.x], t1 = bounds[blockIdx.x + 1];
+    const MixItem first = items[t0 < t1 ? t0 : 0];
     const Slot &S0 = *slots[first.slot];
     const uint32_t polls = S0.wait_polls ? S0.wait_polls : kWaitPolls;
     const bool skip0 = S0.skip_first_load != 0;
@@ -262,19 +268,19 @@ __global__ void __launch_bounds__(F::NT, 1)
             }
         });
     };
-    int t = blockIdx.x;
-    if (threadIdx.x == 0 && t < nitems) issue_p(items[t], 0, skip0);
+    int t = t0;
+    if (threadIdx.x == 0 && t < t1) issue_p(items[t], 0, skip0);
 
-    for (int it = 0; t < nitems; ++it, t += gridDim.x) {
+    for (int it = 0; t < t1; ++it, ++t) {
         const int b = it & 1;
         float2 *Pb = b ? Pb1 : Pb0;
         const MixItem m = items[t];
         const Slot &S = *slots[m.slot];
-        const int tn = t + gridDim.x;
+        const int tn = t + 1;
         if (threadIdx.x == 0) {
             tma::bulk_wait_read_all();
             issue_xs(m);
-            if (tn < nitems) issue_p(items[tn], b ^ 1, false);
+            if (tn < t1) issue_p(items[tn], b ^ 1, false);
         }
         bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
         if (__syncthreads_or(!ok)) {
@@ -283,7 +289,7 @@ __global__ void __launch_bounds__(F::NT, 1)
                 raise_flag(S);
                 tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
                 tma::mbar_wait(&bar[2], it & 1, polls);
-                if (tn < nitems) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+                if (tn < t1) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
             }
             break;
         }
@@ -303,7 +309,7 @@ __global__ void __launch_bounds__(F::NT, 1)
                 if (threadIdx.x == 0) {
                     raise_flag(S);
                     tma::mbar_wait(&bar[2], it & 1, polls);
-                    if (tn < nitems) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+                    if (tn < t1) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
                 }
                 failed = true;
                 return;
