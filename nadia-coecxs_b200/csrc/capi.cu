@@ -755,8 +755,8 @@ extern "C" int nadia_tuned_tiles(int nx, int ny, int fresnel, int batched, char 
         const nadia::f32::Choice &c = nadia::f32::choose(nx, ny, fresnel != 0, batched ? 4 : 1);
         auto desc = [](const nadia::f32::TileVariant *v) {
             char t[160];
-            snprintf(t, sizeof t, "n=%d threads=%d signals/tile=%d radices=%s%s%s", v->n, v->nt,
-                     v->L, v->radices,
+            snprintf(t, sizeof t, "n=%d threads=%d%s signals/tile=%d radices=%s%s%s", v->n, v->nt,
+                     v->groups > 1 ? (v->groups == 4 ? " x4 groups" : " x2 groups") : "", v->L, v->radices,
                      v->single ? " persistent-TMA one stage"
                                : (v->persistent ? " persistent-TMA" : (v->ping ? " ping" : "")),
                      v->direct ? (v->ping && v->persistent ? " ping, sqrt(I) direct" : ", sqrt(I) direct") : "");

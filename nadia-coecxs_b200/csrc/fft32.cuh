@@ -282,10 +282,22 @@ struct Swizzle {
 // barrier between reading one pass's inputs and writing the next pass's
 // outputs (a thread only overwrites a buffer after a barrier that every
 // thread reaches once it has finished reading that buffer).
-template <int N_, int NT_, int L_, int MAP_, class RL, class SW, int MINB_ = 1, bool PING_ = false>
+// GROUPS > 1: the CTA runs GROUPS independent groups of NT threads, each on
+// its own tile; a group's exchanges synchronise the group alone (named
+// barrier 1 + group), and its threads index butterflies by their rank in it.
+template <int N_, int NT_, int L_, int MAP_, class RL, class SW, int MINB_ = 1, bool PING_ = false,
+          int GROUPS_ = 1>
 struct TileCfg {
-    static constexpr int N = N_, NT = NT_, L = L_, MAP = MAP_, MINB = MINB_;
+    static constexpr int N = N_, NT = NT_, L = L_, MAP = MAP_, MINB = MINB_, GROUPS = GROUPS_;
     static constexpr bool PING = PING_;
+    static __device__ __forceinline__ int tid() { return GROUPS > 1 ? threadIdx.x % NT : threadIdx.x; }
+    static __device__ __forceinline__ void sync()
+    {
+        if constexpr (GROUPS > 1)
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)(threadIdx.x / NT)), "n"(NT) : "memory");
+        else
+            __syncthreads();
+    }
     static constexpr int E = N * L / NT;
     static constexpr int P = RL::P;
     using Rad = RL;
@@ -357,7 +369,7 @@ __device__ __forceinline__ void pass_compute(float2 (&v)[C::E], const float2 *__
     for (int q = 0; q < B; ++q) {
         if (Ns > 1) {
             int s, j;
-            C::map(threadIdx.x + q * C::NT, NR, s, j);
+            C::map(C::tid() + q * C::NT, NR, s, j);
             const int t1 = (j % Ns) * TSTEP;
             // W^(t1*r) applied as formed: W^t1 is loaded and squared/cubed for
             // r = 1..3; W^(4a t1) is loaded for each group of four and
@@ -398,7 +410,7 @@ __device__ __forceinline__ void pass_exchange(float2 (&v)[C::E], float2 *sm0, fl
 #pragma unroll
     for (int q = 0; q < B; ++q) {
         int s, j;
-        C::map(threadIdx.x + q * C::NT, NR, s, j);
+        C::map(C::tid() + q * C::NT, NR, s, j);
         const int base = (j / Ns) * Ns * R + (j % Ns);
         if constexpr (C::Swz::stride_commutes(WSTRIDE)) {
             const int a0 = C::sidx(s, base);
@@ -409,7 +421,7 @@ __device__ __forceinline__ void pass_exchange(float2 (&v)[C::E], float2 *sm0, fl
             for (int r = 0; r < R; ++r) sm[C::sidx(s, base + r * Ns)] = v[q * R + r];
         }
     }
-    __syncthreads();
+    C::sync();
     constexpr int R2 = C::radix(p + 1, FWD);
     constexpr int NR2 = C::N / R2;
     constexpr int B2 = C::E / R2;
@@ -417,7 +429,7 @@ __device__ __forceinline__ void pass_exchange(float2 (&v)[C::E], float2 *sm0, fl
 #pragma unroll
     for (int q = 0; q < B2; ++q) {
         int s, j;
-        C::map(threadIdx.x + q * C::NT, NR2, s, j);
+        C::map(C::tid() + q * C::NT, NR2, s, j);
         if constexpr (C::Swz::stride_commutes(RSTRIDE)) {
             const int a0 = C::sidx(s, j);
 #pragma unroll
@@ -427,7 +439,7 @@ __device__ __forceinline__ void pass_exchange(float2 (&v)[C::E], float2 *sm0, fl
             for (int r = 0; r < R2; ++r) v[q * R2 + r] = sm[C::sidx(s, j + r * NR2)];
         }
     }
-    if (!C::PING) __syncthreads();
+    if (!C::PING) C::sync();
 }
 
 // The whole transform; before_last() runs right before the last pass's
@@ -462,7 +474,7 @@ __device__ __forceinline__ void for_each_slot(F &&f)
 #pragma unroll
     for (int q = 0; q < B; ++q) {
         int s, j;
-        C::map(threadIdx.x + q * C::NT, NR, s, j);
+        C::map(C::tid() + q * C::NT, NR, s, j);
 #pragma unroll
         for (int r = 0; r < R; ++r) f(q * R + r, s, j + r * NR);
     }

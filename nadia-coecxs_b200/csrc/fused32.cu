@@ -421,8 +421,8 @@ void encode_one(CUtensorMap *m, void *base, bool complex8, int nx, int ny, int r
 
 void encode_tensor_maps(Slot &s, int nx, int ny)
 {
-    const int rows[4] = {2, 4, 8, 16};
-    for (int k = 0; k < 4; ++k) {
+    const int rows[5] = {1, 2, 4, 8, 16};
+    for (int k = 0; k < 5; ++k) {
         if (nx % rows[k]) {
             std::memset(&s.tm[k][0], 0, sizeof(s.tm[k]));
             continue;
@@ -623,8 +623,9 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
                 v->row(kRowFull, dptrs.p, ns, nx, ny, twy, s);
             }, st, 5);
             if (verbose)
-                fprintf(stderr, "nadia tune: row n=%d NT=%d L=%d radices=%s%s batch=%d: %.2f us\n",
-                        ny, v->nt, v->L, v->radices, v->persistent ? " persistent" : (v->ping ? " ping" : ""), ns, us);
+                fprintf(stderr, "nadia tune: row n=%d NT=%d L=%d G=%d radices=%s%s batch=%d: %.2f us\n",
+                        ny, v->nt, v->L, v->groups, v->radices,
+                        v->persistent ? " persistent" : (v->ping ? " ping" : ""), ns, us);
             if (us < best) { best = us; ch.row = v; ch.row_us = us; }
         }
         NADIA_CUDA(cudaGetLastError());

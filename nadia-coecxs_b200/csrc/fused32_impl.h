@@ -18,9 +18,9 @@ namespace f32 {
 // One reconstruction as the fused kernels see it.  It lives in device
 // memory, so graphs captured once keep working when the algorithm changes.
 struct alignas(64) Slot {
-    // tensor maps over P, x and the support for row tiles of 2, 4, 8 and 16
-    // rows (persistent row pass); box (K, rows, <= 256 panels)
-    CUtensorMap tm[4][3];
+    // tensor maps over P, x and the support for row tiles of 1, 2, 4, 8 and
+    // 16 rows (persistent row passes); box (K, rows, <= 256 panels)
+    CUtensorMap tm[5][3];
     float2 *P;              // work array (row transforms of x / column-pass output)
     float2 *x;              // estimate
     const float *sup;       // support
@@ -132,6 +132,7 @@ struct TileVariant {
     bool ping = false;
     bool single = false; // persistent column pass with one stage per CTA
     bool direct = false; // persistent column pass reading sqrt(I) from global memory
+    int groups = 1;      // independent thread groups a CTA (grouped row pass)
     const char *radices = "";
     void (*prepare)() = nullptr;
     ColLaunch col = nullptr;

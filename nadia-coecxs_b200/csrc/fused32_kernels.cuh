@@ -515,6 +515,51 @@ TileVariant make_persistent_ping(const char *radices)
     return make_persistent_direct_t<2, true, N, NT, L, MINB, SW, Rs...>(radices);
 }
 
+// The row pass in G independent groups of NT threads a CTA (tiles of L rows
+// per group); no column pass.
+template <class C>
+void prepare_grouped_row()
+{
+    set_smem<C>(k_row<C, kRowFull>);
+    set_smem<C>(k_row<C, kRowPrime>);
+    set_smem<C>(k_row<C, kRowPfs>);
+    set_smem<C>(k_row<C, kRowPrimePfs>);
+    NADIA_CUDA(cudaFuncSetAttribute(kg_row<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)grouped_row_smem<C>()));
+}
+
+template <class C>
+void launch_row_grouped(int mode, const Slot *const *slots, int nslots, int nx, int ny,
+                        const float2 *tw, cudaStream_t st)
+{
+    if (mode != kRowFull) {
+        launch_row<C>(mode, slots, nslots, nx, ny, tw, st);
+        return;
+    }
+    const int ntiles = (nx / C::L) * nslots;
+    const int ctas = (ntiles + C::GROUPS - 1) / C::GROUPS;
+    const int grid = ctas < sm_count() ? ctas : sm_count();
+    kg_row<C><<<grid, C::NT * C::GROUPS, grouped_row_smem<C>(), st>>>(slots, nslots, nx, ny, tw);
+}
+
+template <int N, int NT, int L, int G, class SW, int... Rs>
+TileVariant make_grouped_row(const char *radices)
+{
+    using CR = TileCfg<N, NT, L, kRowMap, Radices<Rs...>, SW, 1, false, G>;
+    static_assert(grouped_row_smem<CR>() <= 227 * 1024, "grouped row stages too large");
+    TileVariant t;
+    t.n = N;
+    t.nt = NT;
+    t.L = L;
+    t.minb = 1;
+    t.persistent = true;
+    t.groups = G;
+    t.radices = radices;
+    t.prepare = &prepare_grouped_row<CR>;
+    t.row = &launch_row_grouped<CR>;
+    return t;
+}
+
 // A persistent row pass only: tiles of L rows (L = 2 allowed, below the
 // panel width a column tile needs), MINB CTAs per SM.
 template <int N, int NT, int L, int MINB, class SW, int... Rs>

@@ -181,7 +181,7 @@ __device__ __forceinline__ void finish_error(const Slot &S)
 template <int L>
 __host__ __device__ constexpr int tmap_index()
 {
-    return L == 2 ? 0 : (L == 4 ? 1 : (L == 8 ? 2 : 3));
+    return L == 1 ? 0 : (L == 2 ? 1 : (L == 4 ? 2 : (L == 8 ? 3 : 4)));
 }
 
 template <class C>
@@ -301,6 +301,163 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         }
     }
     if (threadIdx.x == 0) tma::bulk_wait_all();
+}
+
+// OR of a predicate over the thread's group (the CTA when C::GROUPS == 1),
+// which also synchronises the group
+template <class C>
+__device__ __forceinline__ bool group_or(bool v)
+{
+    if constexpr (C::GROUPS > 1) {
+        uint32_t out;
+        asm volatile("{\n\t.reg .pred p, q;\n\t"
+                     "setp.ne.u32 p, %1, 0;\n\t"
+                     "bar.red.or.pred q, %2, %3, p;\n\t"
+                     "selp.u32 %0, 1, 0, q;\n\t}"
+                     : "=r"(out)
+                     : "r"((uint32_t)v), "r"(1 + (int)(threadIdx.x / C::NT)), "n"(C::NT)
+                     : "memory");
+        return out != 0;
+    } else {
+        return __syncthreads_or(v);
+    }
+}
+
+// The row pass in C::GROUPS independent groups of C::NT threads.  Each group
+// owns a quarter (or half) of the shared memory and runs the pipeline of
+// kp_row on its own: its tiles of C::L rows (tile g, g + G, ... of the CTA's
+// share), its own mbarriers, its own TMA issue thread (the group's first),
+// and exchanges behind its own named barrier.  Nothing synchronises the
+// groups after the error metrics are finished, so one group's barrier and
+// load waits overlap the others' arithmetic.
+template <class C>
+constexpr size_t grouped_row_smem()
+{
+    return (size_t)C::GROUPS * ((size_t)C::N * C::L * 28 + 24);
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::NT * C::GROUPS, 1)
+    kg_row(const Slot *const *slots, int nslots, int nx, int ny, const float2 *__restrict__ tw)
+{
+    static_assert(C::GROUPS > 1, "grouped tiles");
+    constexpr int G = C::GROUPS;
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    constexpr int TW = C::N * C::L;
+    constexpr int TM = tmap_index<C::L>();
+    const int g = threadIdx.x / C::NT, u = threadIdx.x % C::NT;
+    float2 *Pb0 = reinterpret_cast<float2 *>(smraw + (size_t)g * TW * 28);
+    float2 *Pb1 = Pb0 + TW;
+    float2 *Xb = Pb1 + TW;
+    float *Sb = reinterpret_cast<float *>(Xb + TW);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + (size_t)G * TW * 28) + 3 * g;
+    const int tps = nx / C::L;
+    const int ntiles = tps * nslots;
+    const int npan = ny / kPanel;
+    const int boxp = box_panels(npan);
+
+    if (u == 0) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::mbar_init(&bar[2], 1);
+        tma::fence_barrier_init();
+    }
+    // slots whose error this CTA finishes (the column pass ran before)
+    for (int sl = blockIdx.x; sl < nslots; sl += gridDim.x) finish_error<C::NT * G>(*slots[sl]);
+    __syncthreads();
+
+    int t = blockIdx.x * G + g;
+    const int stride = gridDim.x * G;
+    if (t >= ntiles) return; // a group without tiles (no CTA-wide barrier follows)
+    const Slot &S0 = *slots[t / tps];
+    const uint32_t polls = S0.wait_polls ? S0.wait_polls : kWaitPolls;
+    const bool skip0 = S0.skip_first_load != 0;
+    auto issue_p = [&](int tile, int b, bool skip) {
+        const Slot &S = *slots[tile / tps];
+        const int i0 = (tile % tps) * C::L;
+        float2 *dst = b ? Pb1 : Pb0;
+        tma::mbar_arrive_expect_tx(&bar[b], TW * 8);
+        if (skip) return;
+        for (int c = 0; c < npan; c += boxp)
+            tma::tensor_load_3d(dst + (size_t)c * C::L * kPanel, &S.tm[TM][0], 0, i0, c, &bar[b]);
+    };
+    auto issue_xs = [&](int tile) {
+        const Slot &S = *slots[tile / tps];
+        const int i0 = (tile % tps) * C::L;
+        tma::mbar_arrive_expect_tx(&bar[2], TW * 12);
+        for (int c = 0; c < npan; c += boxp) {
+            tma::tensor_load_3d(Xb + (size_t)c * C::L * kPanel, &S.tm[TM][1], 0, i0, c, &bar[2]);
+            tma::tensor_load_3d(Sb + (size_t)c * C::L * kPanel, &S.tm[TM][2], 0, i0, c, &bar[2]);
+        }
+    };
+    if (u == 0) issue_p(t, 0, skip0);
+
+    for (int it = 0; t < ntiles; ++it, t += stride) {
+        const int b = it & 1;
+        float2 *Pb = b ? Pb1 : Pb0;
+        const Slot &S = *slots[t / tps];
+        const int i0 = (t % tps) * C::L;
+        const int tn = t + stride;
+        if (u == 0) {
+            tma::bulk_wait_read_all();
+            issue_xs(t);
+            if (tn < ntiles) issue_p(tn, b ^ 1, false);
+        }
+        bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
+        if (group_or<C>(!ok)) {
+            // every copy issued so far lands before the group leaves
+            if (u == 0) {
+                raise_flag(S);
+                tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
+                tma::mbar_wait(&bar[2], it & 1, polls);
+                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+            }
+            break;
+        }
+        float2 v[C::E];
+        for_each_slot<C, false, true>([&](int e, int s, int pos) { v[e] = Pb[raw_row<C>(s, pos)]; });
+        C::sync();
+        transform<C, false>(v, Pb, tw);
+
+        ok = tma::mbar_wait(&bar[2], it & 1, polls);
+        if (group_or<C>(!ok)) {
+            if (u == 0) {
+                raise_flag(S);
+                tma::mbar_wait(&bar[2], it & 1, polls);
+                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+            }
+            break;
+        }
+        const float wid = S.w_id, wpf = S.w_pf, wps = S.w_ps, wpsf = S.w_psf;
+        const bool er = S.er;
+        for_each_slot<C, false, false>([&](int e, int s, int pos) {
+            const int a = raw_row<C>(s, pos);
+            const float f = support_factor(Sb[a]);
+            const float2 y = v[e];
+            float2 xn;
+            if (er) {
+                xn = cscale(y, f);
+            } else {
+                const float2 xk = Xb[a];
+                xn = make_float2(wid * xk.x + wpf * y.x + wps * (f * xk.x) + wpsf * (f * y.x),
+                                 wid * xk.y + wpf * y.y + wps * (f * xk.y) + wpsf * (f * y.y));
+            }
+            Xb[a] = xn;
+            v[e] = xn;
+        });
+        transform<C, true>(v, Pb, tw);
+        for_each_slot<C, true, false>([&](int e, int s, int pos) { Pb[raw_row<C>(s, pos)] = v[e]; });
+        tma::fence_async_shared();
+        C::sync();
+        if (u == 0) {
+            for (int c = 0; c < npan; c += boxp) {
+                tma::tensor_store_3d(&S.tm[TM][0], 0, i0, c, Pb + (size_t)c * C::L * kPanel);
+                tma::tensor_store_3d(&S.tm[TM][1], 0, i0, c, Xb + (size_t)c * C::L * kPanel);
+            }
+            tma::bulk_commit();
+        }
+    }
+    if (u == 0) tma::bulk_wait_all();
 }
 
 } // namespace f32
