@@ -39,6 +39,37 @@ __device__ __forceinline__ float2 modulus(float2 u, float m, double &diff)
     return r;
 }
 
+// The PlanarCDI column-pass projection of an unnormalised transform value X:
+// Psi = s0 X goes through the modulus projection, and the value handed to
+// the inverse transform is s0 times the projected Psi, that is X s0 m / |X|
+// ((s0 m, 0) where X = 0); the 1/sqrt(N) factors are folded into the
+// magnitude ratio.  Adds (|Psi| - m)^2 to diff for measured pixels (the
+// difference formed in FP32, its square summed in FP64).
+__device__ __forceinline__ float2 planar_modulus(float2 X, float m, float s0, double &diff)
+{
+    const float a2 = X.x * X.x + X.y * X.y;
+    const bool measured = !(m < 0.f);
+    const bool zero = !(a2 > 0.f);
+    const float inv = rsqrtf(zero ? 1.f : a2);
+    const float sm = s0 * m;
+    const float sc = measured ? sm * inv : 1.f;
+    float2 r = make_float2(X.x * sc, X.y * sc);
+    if (measured && zero) r = make_float2(sm, 0.f);
+    const float mag = zero ? 0.f : a2 * inv;
+    const float d = measured ? fmaf(s0, mag, -m) : 0.f;
+    diff = fma((double)d, (double)d, diff);
+    return r;
+}
+
+// The combine of BaseCDI.c++:346-383 without a PfPs term, with the support
+// factor f folded into two weights: x' = (1 + PI + PS f) x + (PF + PSF f) y
+__device__ __forceinline__ float2 combine2(float2 xk, float2 y, float f, float wid, float wpf,
+                                           float wps, float wpsf)
+{
+    const float a = fmaf(wps, f, wid), b = fmaf(wpsf, f, wpf);
+    return make_float2(fmaf(a, xk.x, b * y.x), fmaf(a, xk.y, b * y.y));
+}
+
 // FP64 block sum; result valid in thread 0
 template <int NT>
 __device__ __forceinline__ double block_sum(double v)
@@ -84,7 +115,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_col(const Slot *const *slots
         float2 X = v[e];
         if (!FRESNEL) {
             // Planar: Psi = X s0; back-propagated value = projected Psi * s0
-            X = cscale(modulus(cscale(X, s0), m, diff), s0);
+            X = planar_modulus(X, m, s0, diff);
         } else {
             const float2 cf = cmul(__ldg(&S.tx[kx]), __ldg(&S.ty[ky]));
             const float2 w = S.W[a];

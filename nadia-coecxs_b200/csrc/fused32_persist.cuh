@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             const float mm = MDIRECT ? m[e] : Mb[raw_col<C>(s, kx)];
             float2 X = v[e];
             if (!FRESNEL) {
-                X = cscale(modulus(cscale(X, s0), mm, diff), s0);
+                X = planar_modulus(X, mm, s0, diff);
             } else {
                 const int ky = c0 * kPanel + s;
                 const float2 cf = cmul(__ldg(&S.tx[kx]), __ldg(&S.ty[ky]));
@@ -282,8 +282,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
                 xn = cscale(y, f);
             } else {
                 const float2 xk = Xb[a];
-                xn = make_float2(wid * xk.x + wpf * y.x + wps * (f * xk.x) + wpsf * (f * y.x),
-                                 wid * xk.y + wpf * y.y + wps * (f * xk.y) + wpsf * (f * y.y));
+                xn = combine2(xk, y, f, wid, wpf, wps, wpsf);
             }
             Xb[a] = xn;
             v[e] = xn;
@@ -439,8 +438,7 @@ __global__ void __launch_bounds__(C::NT * C::GROUPS, 1)
                 xn = cscale(y, f);
             } else {
                 const float2 xk = Xb[a];
-                xn = make_float2(wid * xk.x + wpf * y.x + wps * (f * xk.x) + wpsf * (f * y.x),
-                                 wid * xk.y + wpf * y.y + wps * (f * xk.y) + wpsf * (f * y.y));
+                xn = combine2(xk, y, f, wid, wpf, wps, wpsf);
             }
             Xb[a] = xn;
             v[e] = xn;

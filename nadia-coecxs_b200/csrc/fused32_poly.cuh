@@ -195,8 +195,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_row(const Slot *const *
                     xn = cscale(y, f);
                 } else {
                     const float2 xk = x[a];
-                    xn = make_float2(wid * xk.x + wpf * y.x + wps * (f * xk.x) + wpsf * (f * y.x),
-                                     wid * xk.y + wpf * y.y + wps * (f * xk.y) + wpsf * (f * y.y));
+                    xn = combine2(xk, y, f, wid, wpf, wps, wpsf);
                 }
                 x[a] = xn;
             }
