@@ -348,8 +348,8 @@ void launch_row(int mode, const Slot *const *slots, int nslots, int nx, int ny, 
 
 // shared memory of the persistent passes: STAGES stages of P and sqrt(I)
 // (column); two stages of P plus x and the support (row); and mbarriers
-template <class C, int STAGES = 2, bool MDIRECT = false>
-constexpr size_t persist_col_smem() { return persist_col_bytes<C, STAGES, MDIRECT>(); }
+template <class C, int STAGES = 2, int MMODE = 0>
+constexpr size_t persist_col_smem() { return persist_col_bytes<C, STAGES, MMODE>(); }
 template <class C>
 constexpr size_t persist_row_smem() { return (size_t)C::N * C::L * 28 + 24; }
 
@@ -364,7 +364,7 @@ int resident_ctas(K kernel, int nt, size_t smem, int minb)
     return occ < minb ? occ : minb;
 }
 
-template <class C, int STAGES, bool MDIRECT>
+template <class C, int STAGES, int MMODE>
 struct PersistCol {
     static inline int per_sm = 1;
 };
@@ -373,16 +373,16 @@ struct PersistRow {
     static inline int per_sm = 1;
 };
 
-template <class C, int STAGES, bool MDIRECT = false>
+template <class C, int STAGES, int MMODE = 0>
 void prepare_persistent_col()
 {
-    constexpr int bytes = (int)persist_col_smem<C, STAGES, MDIRECT>();
-    NADIA_CUDA(cudaFuncSetAttribute(kp_col<C, false, STAGES, MDIRECT>,
+    constexpr int bytes = (int)persist_col_smem<C, STAGES, MMODE>();
+    NADIA_CUDA(cudaFuncSetAttribute(kp_col<C, false, STAGES, MMODE>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    NADIA_CUDA(cudaFuncSetAttribute(kp_col<C, true, STAGES, MDIRECT>,
+    NADIA_CUDA(cudaFuncSetAttribute(kp_col<C, true, STAGES, MMODE>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    PersistCol<C, STAGES, MDIRECT>::per_sm =
-        resident_ctas(kp_col<C, false, STAGES, MDIRECT>, C::NT, bytes, C::MINB);
+    PersistCol<C, STAGES, MMODE>::per_sm =
+        resident_ctas(kp_col<C, false, STAGES, MMODE>, C::NT, bytes, C::MINB);
 }
 
 template <class C>
@@ -405,18 +405,18 @@ void prepare_persistent()
     prepare_persistent_row<CR>();
 }
 
-template <class C, int STAGES, bool MDIRECT = false>
+template <class C, int STAGES, int MMODE = 0>
 void launch_col_persistent(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
                            const float2 *tw, cudaStream_t st)
 {
-    constexpr size_t bytes = persist_col_smem<C, STAGES, MDIRECT>();
+    constexpr size_t bytes = persist_col_smem<C, STAGES, MMODE>();
     const int ntiles = (ny / C::L) * nslots;
-    const int cap = sm_count() * PersistCol<C, STAGES, MDIRECT>::per_sm;
+    const int cap = sm_count() * PersistCol<C, STAGES, MMODE>::per_sm;
     const int grid = ntiles < cap ? ntiles : cap;
     if (fresnel)
-        kp_col<C, true, STAGES, MDIRECT><<<grid, C::NT, bytes, st>>>(slots, nslots, nx, ny, tw);
+        kp_col<C, true, STAGES, MMODE><<<grid, C::NT, bytes, st>>>(slots, nslots, nx, ny, tw);
     else
-        kp_col<C, false, STAGES, MDIRECT><<<grid, C::NT, bytes, st>>>(slots, nslots, nx, ny, tw);
+        kp_col<C, false, STAGES, MMODE><<<grid, C::NT, bytes, st>>>(slots, nslots, nx, ny, tw);
 }
 
 template <class C>
@@ -520,7 +520,7 @@ template <int STAGES, bool PING, int N, int NT, int L, int MINB, class SW, int..
 TileVariant make_persistent_direct_t(const char *radices)
 {
     using CC = TileCfg<N, NT, L, kColMap, Radices<Rs...>, SW, MINB, PING>;
-    static_assert(persist_col_smem<CC, STAGES, true>() * MINB <= 226 * 1024, "stages too large");
+    static_assert(persist_col_smem<CC, STAGES, 1>() * MINB <= 226 * 1024, "stages too large");
     TileVariant t;
     t.n = N;
     t.nt = NT;
@@ -531,8 +531,8 @@ TileVariant make_persistent_direct_t(const char *radices)
     t.ping = PING;
     t.direct = true;
     t.radices = radices;
-    t.prepare = &prepare_persistent_col<CC, STAGES, true>;
-    t.col = &launch_col_persistent<CC, STAGES, true>;
+    t.prepare = &prepare_persistent_col<CC, STAGES, 1>;
+    t.col = &launch_col_persistent<CC, STAGES, 1>;
     return t;
 }
 template <int N, int NT, int L, int MINB, class SW, int... Rs>
@@ -588,6 +588,26 @@ TileVariant make_grouped_row(const char *radices)
     t.radices = radices;
     t.prepare = &prepare_grouped_row<CR>;
     t.row = &launch_row_grouped<CR>;
+    return t;
+}
+
+// A persistent column pass with two stages of P, one stage of sqrt(I)
+// refilled after each modulus, and ping-pong exchanges; no row pass.
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_persistent_mstage(const char *radices)
+{
+    using CC = TileCfg<N, NT, L, kColMap, Radices<Rs...>, SW, MINB, true>;
+    static_assert(persist_col_smem<CC, 2, 2>() <= 227 * 1024, "stages too large");
+    TileVariant t;
+    t.n = N;
+    t.nt = NT;
+    t.L = L;
+    t.minb = MINB;
+    t.persistent = true;
+    t.ping = true;
+    t.radices = radices;
+    t.prepare = &prepare_persistent_col<CC, 2, 2>;
+    t.col = &launch_col_persistent<CC, 2, 2>;
     return t;
 }
 

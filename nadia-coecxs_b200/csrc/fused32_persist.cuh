@@ -47,38 +47,50 @@ __device__ __forceinline__ void raise_flag(const Slot &S)
 // buffer per CTA (less shared memory, so two CTAs share an SM and each one's
 // load overlaps the other's arithmetic); the next load is issued once the
 // previous tile's store has read the buffer.
-// MDIRECT: sqrt(I) is not staged; each thread reads its values straight from
-// global memory (a warp reads 128 contiguous bytes), issued before the last
-// pass of the forward transform so that the loads overlap that pass.
+// MMODE (how sqrt(I) reaches the modulus):
+//   0  staged with P in every stage;
+//   1  not staged: each thread reads its values straight from global memory
+//      (a warp reads 128 contiguous bytes), issued before the last pass of
+//      the forward transform so that the loads overlap that pass;
+//   2  one stage of its own (on mbarrier 2), refilled with the next tile's
+//      values as soon as the current tile's modulus has read it, so that the
+//      load overlaps the inverse transform and the next forward transform.
 // C::PING: the exchanges alternate between the stage and one more tile
 // buffer, one barrier per exchange instead of two.
-// Shared memory: STAGES x (P [+ sqrt(I)]) [+ exchange buffer] + 2 mbarriers.
-template <class C, int STAGES, bool MDIRECT>
+// Shared memory: STAGES x P, sqrt(I) (STAGES, 0 or 1 tiles), [exchange
+// buffer], 3 mbarriers.
+template <class C, int STAGES, int MMODE>
 constexpr size_t persist_col_bytes()
 {
-    return (size_t)C::N * C::L * (8 * STAGES + (MDIRECT ? 0 : 4 * STAGES) + (C::PING ? 8 : 0)) + 16;
+    return (size_t)C::N * C::L *
+               (8 * STAGES + (MMODE == 0 ? 4 * STAGES : (MMODE == 2 ? 4 : 0)) + (C::PING ? 8 : 0)) +
+           24;
 }
 
-template <class C, bool FRESNEL, int STAGES, bool MDIRECT>
+template <class C, bool FRESNEL, int STAGES, int MMODE>
 __global__ void __launch_bounds__(C::NT, C::MINB)
     kp_col(const Slot *const *slots, int nslots, int nx, int ny, const float2 *__restrict__ tw)
 {
     static_assert(STAGES == 1 || STAGES == 2, "one or two stages");
+    static_assert(MMODE != 2 || STAGES == 2, "a sqrt(I) stage of its own pairs with two P stages");
+    constexpr bool MDIRECT = MMODE == 1;
+    constexpr bool MSTAGE = MMODE == 2;
     extern __shared__ __align__(1024) unsigned char smraw[];
     constexpr int TW = C::N * C::L;
     float2 *Pb0 = reinterpret_cast<float2 *>(smraw);
     float2 *Pb1 = Pb0 + TW * (STAGES - 1);
     float *Mb0 = reinterpret_cast<float *>(Pb1 + TW);
-    float *Mb1 = Mb0 + (MDIRECT ? 0 : TW * (STAGES - 1));
-    float2 *Xb = reinterpret_cast<float2 *>(Mb1 + (MDIRECT ? 0 : TW)); // PING only
+    float *Mb1 = Mb0 + (MMODE == 0 ? TW * (STAGES - 1) : 0);
+    float2 *Xb = reinterpret_cast<float2 *>(Mb1 + (MMODE == 1 ? 0 : TW)); // PING only
     uint64_t *bar = reinterpret_cast<uint64_t *>(Xb + (C::PING ? TW : 0));
     const int tps = ny / C::L;
     const int ntiles = tps * nslots;
-    constexpr uint32_t kBytes = TW * (MDIRECT ? 8 : 12);
+    constexpr uint32_t kBytes = TW * (MMODE == 0 ? 12 : 8);
 
     if (threadIdx.x == 0) {
         tma::mbar_init(&bar[0], 1);
         tma::mbar_init(&bar[1], 1);
+        tma::mbar_init(&bar[2], 1);
         tma::fence_barrier_init();
     }
     __syncthreads();
@@ -94,11 +106,19 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         tma::mbar_arrive_expect_tx(&bar[b], kBytes);
         if (skip) return;
         tma::bulk_load(b ? (void *)Pb1 : (void *)Pb0, S.P + off, TW * 8, &bar[b]);
-        if (!MDIRECT)
+        if (MMODE == 0)
             tma::bulk_load(b ? (void *)Mb1 : (void *)Mb0, S.mI + off, TW * 4, &bar[b]);
     };
+    auto issue_m = [&](int tile) { // MSTAGE: sqrt(I) of `tile` into its stage
+        const Slot &S = *slots[tile / tps];
+        tma::mbar_arrive_expect_tx(&bar[2], TW * 4);
+        tma::bulk_load(Mb0, S.mI + (size_t)(tile % tps) * C::L * nx, TW * 4, &bar[2]);
+    };
     int t = blockIdx.x;
-    if (STAGES == 2 && threadIdx.x == 0 && t < ntiles) issue(t, 0, skip0);
+    if (STAGES == 2 && threadIdx.x == 0 && t < ntiles) {
+        issue(t, 0, skip0);
+        if (MSTAGE) issue_m(t);
+    }
 
     for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
         const int b = STAGES == 2 ? (it & 1) : 0;
@@ -125,6 +145,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
                 tma::mbar_wait(&bar[b], par, polls);
                 if (STAGES == 2 && tn < ntiles)
                     tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+                if (MSTAGE) tma::mbar_wait(&bar[2], it & 1, polls);
             }
             break;
         }
@@ -139,10 +160,21 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
                     [&](int e, int s, int kx) { m[e] = __ldg(&mg[raw_col<C>(s, kx)]); });
         });
 
+        if (MSTAGE) {
+            const bool okm = tma::mbar_wait(&bar[2], it & 1, polls);
+            if (__syncthreads_or(!okm)) {
+                if (threadIdx.x == 0) {
+                    raise_flag(S);
+                    tma::mbar_wait(&bar[2], it & 1, polls);
+                    if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+                }
+                break;
+            }
+        }
         const float s0 = S.s0;
         double diff = 0.0;
         for_each_slot<C, true, false>([&](int e, int s, int kx) {
-            const float mm = MDIRECT ? m[e] : Mb[raw_col<C>(s, kx)];
+            const float mm = MDIRECT ? m[e] : (MSTAGE ? Mb0 : Mb)[raw_col<C>(s, kx)];
             float2 X = v[e];
             if (!FRESNEL) {
                 X = planar_modulus(X, mm, s0, diff);
@@ -155,8 +187,14 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             }
             v[e] = X;
         });
-        const double tot = block_sum<C::NT>(diff);
-        if (threadIdx.x == 0) S.partials[t % tps] = tot;
+        const double tot = block_sum<C::NT>(diff); // every thread has read sqrt(I)
+        if (threadIdx.x == 0) {
+            S.partials[t % tps] = tot;
+            if (MSTAGE && tn < ntiles) {
+                tma::fence_async_shared();
+                issue_m(tn);
+            }
+        }
 
         transform_h<C, false>(v, Pb, Xb, tw, [] {});
         for_each_slot<C, false, false>([&](int e, int s, int pos) { Pb[raw_col<C>(s, pos)] = v[e]; });

@@ -33,7 +33,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "nadia-coecxs_b200", "csrc")
 K = 4  # panel width
 
-PAT = re.compile(r"make_(variant|ping|persistent_single|persistent_direct|persistent_ping|"
+PAT = re.compile(r"make_(variant|ping|persistent_single|persistent_direct|persistent_ping|persistent_mstage|"
                  r"persistent_row|grouped_row|persistent|poly)<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+),\s*"
                  r"Swizzle<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+)>\s*,\s*([\d,\s]+)>")
 
@@ -180,7 +180,7 @@ def out_positions(v, mapf, first_radix):
     return np.array(pos)
 
 
-COLUMN_ONLY = ("persistent_single", "persistent_direct", "persistent_ping")
+COLUMN_ONLY = ("persistent_single", "persistent_direct", "persistent_ping", "persistent_mstage")
 
 
 def maps_of(v):
@@ -219,7 +219,9 @@ def test_tile_shape_constraints(v):
     if v["kind"] == "persistent_direct":
         assert v["minb"] * (N * L * 8 + 16 + 1024) <= 228 * 1024
     if v["kind"] == "persistent_ping":
-        assert v["minb"] * (N * L * 24 + 16 + 1024) <= 228 * 1024
+        assert v["minb"] * (N * L * 24 + 24 + 1024) <= 228 * 1024
+    if v["kind"] == "persistent_mstage":
+        assert N * L * 28 + 24 <= 227 * 1024
 
 
 @pytest.mark.parametrize("v", VARIANTS, ids=vid)
