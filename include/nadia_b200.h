@@ -21,8 +21,9 @@
  *     loop; NADIA_FP32 runs the fused single-precision path (complex FP32
  *     transforms and projections, FP64 error and support reductions).
  *   - Sizes must be even (the reference's quadrant swap assumes it,
- *     NADIA/src/Complex_2D.c++:327-331) and every prime factor of a transform
- *     length must be at most 64.
+ *     NADIA/src/Complex_2D.c++:327-331), except for PlanarCDI in the FP64
+ *     form, which reproduces what the swap does on odd sizes; every prime
+ *     factor of a transform length must be at most 64.
  */
 #ifndef NADIA_B200_H
 #define NADIA_B200_H

@@ -4,6 +4,10 @@
 #include "plain64.h"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
 
 namespace nadia {
 namespace plain {
@@ -915,10 +919,78 @@ void Fft2d::exec(double2 *a, bool forward, cudaStream_t s) const
     NADIA_CUDA(cudaGetLastError());
 }
 
+// Odd grids: Complex_2D::invert's swap loop (Complex_2D.c++:318-353) then
+// visits some elements twice and never moves the last column (for odd ny),
+// so its result depends on the loop order.  The loop is replayed once on the
+// host over element indices: out[k] = in[src[k]] multiplied cnt[k] times by
+// the scale factor, one multiplication after the other as the loop does.
+__global__ void k_invert_gather(const double2 *__restrict__ in, double2 *__restrict__ out,
+                                const int *__restrict__ src, const unsigned char *__restrict__ cnt,
+                                size_t n, double s)
+{
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        double2 v = in[src[k]];
+        for (int c = cnt[k]; c > 0; --c) v = make_double2(v.x * s, v.y * s);
+        out[k] = v;
+    }
+}
+
+namespace {
+struct OddInvert {
+    DevBuf<int> src;
+    DevBuf<unsigned char> cnt;
+    DevBuf<double2> tmp;
+};
+
+// the replayed loop for an odd grid on the current device (built once)
+OddInvert &odd_invert(int nx, int ny)
+{
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int>, OddInvert> cache;
+    int dev = 0;
+    NADIA_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    OddInvert &t = cache[std::make_tuple(dev, nx, ny)];
+    if (!t.src) {
+        const size_t n = (size_t)nx * ny;
+        std::vector<int> src(n);
+        std::vector<unsigned char> cnt(n, 0);
+        for (size_t k = 0; k < n; ++k) src[k] = (int)k;
+        const int mx = nx / 2, my = ny / 2;
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < my; ++j) {
+                int jn = j + my, in = i + mx;
+                if (i >= mx) in = in - 2 * mx;
+                const size_t p = (size_t)in * ny + jn, q = (size_t)i * ny + j;
+                const int ts = src[p];
+                const unsigned char tc = cnt[p];
+                src[p] = src[q];
+                cnt[p] = (unsigned char)(cnt[q] + 1);
+                src[q] = ts;
+                cnt[q] = (unsigned char)(tc + 1);
+            }
+        t.src.alloc(n);
+        t.cnt.alloc(n);
+        t.tmp.alloc(n);
+        upload_now(t.src.p, src.data(), n * sizeof(int));
+        upload_now(t.cnt.p, cnt.data(), n);
+    }
+    return t;
+}
+} // namespace
+
 void invert(double2 *a, int nx, int ny, bool sc, cudaStream_t s)
 {
     double f = 1;
     if (sc) f = 1.0 / (sqrt((double)(nx * ny)));
+    if ((nx | ny) & 1) {
+        OddInvert &t = odd_invert(nx, ny);
+        const size_t n = (size_t)nx * ny;
+        k_invert_gather<<<grid_of(n), kThreads, 0, s>>>(a, t.tmp.p, t.src.p, t.cnt.p, n, f);
+        NADIA_CUDA(cudaMemcpyAsync(a, t.tmp.p, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        return;
+    }
     k_invert<<<grid_of((size_t)nx * (ny / 2)), kThreads, 0, s>>>(a, nx, ny, f);
 }
 

@@ -88,9 +88,14 @@ Solver::Solver(int kind_, int nx_, int ny_, int prec_, int n_best_)
                   "FresnelCDI_WF runs in the FP64 form");
     NADIA_REQUIRE(prec == NADIA_FP64 || prec == NADIA_FP32, NADIA_ERR_INVALID,
                   "unknown precision");
-    NADIA_REQUIRE(nx >= 2 && ny >= 2 && nx % 2 == 0 && ny % 2 == 0, NADIA_ERR_INVALID,
-                  "grid sizes must be even and at least 2 (the quadrant swap of "
-                  "Complex_2D::invert assumes even sizes)");
+    NADIA_REQUIRE(nx >= 2 && ny >= 2, NADIA_ERR_INVALID, "grid sizes must be at least 2");
+    // Complex_2D::invert assumes even sizes (Complex_2D.c++:327-331); PlanarCDI
+    // in the FP64 form reproduces what it does on odd ones, the other kinds
+    // index quarter tables or padded grids past their ends there
+    NADIA_REQUIRE((nx % 2 == 0 && ny % 2 == 0) || (kind == NADIA_PLANAR && prec == NADIA_FP64),
+                  NADIA_ERR_INVALID,
+                  "odd grid sizes run in PlanarCDI's FP64 form only; other kinds and the FP32 "
+                  "form need even sizes");
     NADIA_REQUIRE(n_best >= 0 && n_best <= 64, NADIA_ERR_INVALID, "n_best must be in [0, 64]");
     FftPlan tmpx = make_plan(nx), tmpy = make_plan(ny);
     (void)tmpx; (void)tmpy;
@@ -380,6 +385,8 @@ void Solver::set_transmission_constraint(int unity, int flip, int flip_sign, int
     AllocScope scope(st);
     NADIA_REQUIRE(nregions >= 0 && nregions <= plain::kMaxRegions, NADIA_ERR_INVALID,
                   "between 0 and 16 complex-constraint regions");
+    NADIA_REQUIRE(nregions == 0 || n % 4 == 0, NADIA_ERR_UNSUPPORTED,
+                  "complex-constraint regions need a pixel count divisible by 4");
     if (prec == NADIA_FP32) {
         // the per-pixel part runs inside the fused row pass; regions need
         // whole-image sums between the projection and its update
@@ -889,9 +896,10 @@ void Solver::plain_project(double2 *c)
         plain_scale(padded.p);
         plain_propagate_from(padded.p, true);
         plain::unpad(padded.p, nx, ny, px, py, c, st);
-    } else if (kind == NADIA_PLANAR) {
+    } else if (kind == NADIA_PLANAR && nx % 2 == 0 && ny % 2 == 0) {
         // propagate_to, scale_intensity, propagate_from with the element-wise
-        // steps between the transforms in one kernel
+        // steps between the transforms in one kernel (the swap pairs of an
+        // even grid)
         fft.exec(c, true, st);
         plain::detector_planar(c, isqrt.p, bs_ptr(), nx, ny, partials.p, d_err.p, st);
         fft.exec(c, false, st);

@@ -162,6 +162,27 @@ def test_poly_vs_oracle(n, padding):
     compare(sc.poly_mixed(gpu, n=n, padding=padding), sc.poly_mixed(orc, n=n, padding=padding))
 
 
+@pytest.mark.parametrize("n,ny", [(35, 35), (33, 45), (30, 45)])
+def test_planar_odd_sizes_vs_oracle(n, ny):
+    """Odd grids (PlanarCDI, FP64 form): the reference's quadrant swap on odd
+    sizes replayed exactly; the rest of the loop as on even grids."""
+    compare(sc.planar_mixed(gpu, n=n, ny=ny), sc.planar_mixed(orc, n=n, ny=ny),
+            exact_keys=("esw", "support", "init"))
+
+
+def test_odd_sizes_refused_elsewhere():
+    for kind, prec in (("planar", pynadia.FP32), ("fresnel", pynadia.FP64)):
+        with pytest.raises(pynadia.NadiaError) as e:
+            if kind == "fresnel":
+                f = synth.FresnelCase(32, seed=1)
+                pynadia.Solver(kind, 33, 33, precision=prec, white_field=np.ones((33, 33)),
+                               wavelength=f.wavelength, focal_detector_length=f.zfd,
+                               focal_sample_length=f.zfs, pixel_size=f.pixel)
+            else:
+                pynadia.Solver(kind, 33, 33, precision=prec)
+        assert e.value.code in (1, 3)
+
+
 def test_config1_256_hio_200_shrinkwrap():
     """PlanarCDI HIO FP64, 256^2, 200 iterations, shrinkwrap every 20."""
     a = sc.config1(gpu)

@@ -35,6 +35,14 @@ def test_planar(n, ny):
     same(sc.planar_mixed(orc, n=n, ny=ny), sc.planar_mixed(ref, n=n, ny=ny))
 
 
+# odd sizes: Complex_2D::invert's swap loop then visits some elements twice
+# and leaves the last column alone (Complex_2D.c++:318-353; the reference
+# warns and runs), reproduced loop for loop
+@pytest.mark.parametrize("n,ny", [(35, 35), (33, 45), (30, 45)])
+def test_planar_odd_sizes(n, ny):
+    same(sc.planar_mixed(orc, n=n, ny=ny), sc.planar_mixed(ref, n=n, ny=ny))
+
+
 def test_planar_custom():
     same(sc.planar_custom(orc, n=48), sc.planar_custom(ref, n=48))
 
