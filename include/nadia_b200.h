@@ -23,7 +23,7 @@
  *   - Sizes must be even (the reference's quadrant swap assumes it,
  *     NADIA/src/Complex_2D.c++:327-331), except for PlanarCDI in the FP64
  *     form, which reproduces what the swap does on odd sizes; every prime
- *     factor of a transform length must be at most 64.
+ *     factor of a transform length must be at most 1021.
  */
 #ifndef NADIA_B200_H
 #define NADIA_B200_H

@@ -139,11 +139,12 @@ inline void upload_now(void *dst, const void *src, size_t bytes)
 }
 
 constexpr int kMaxPasses = 40;
-constexpr int kMaxRadix = 64;
+constexpr int kMaxRadix = 64;    // generic radices up to this keep their inputs in registers
+constexpr int kMaxPrime = 1021;  // the largest prime factor a transform length may have
 
 // Radix plan of a transform length: 8s, then the remaining 4 or 2, then odd
 // primes in ascending order.  Returns the number of passes, or -1 when n has
-// a prime factor above kMaxRadix.
+// a prime factor above kMaxPrime.
 inline int plan_radices(int n, int *radix)
 {
     int p = 0;
@@ -153,7 +154,7 @@ inline int plan_radices(int n, int *radix)
     if (n % 2 == 0) { radix[p++] = 2; n /= 2; }
     for (int f = 3; n > 1; f += 2) {
         while (n % f == 0) {
-            if (f > kMaxRadix) return -1;
+            if (f > kMaxPrime) return -1;
             radix[p++] = f;
             n /= f;
         }
@@ -174,7 +175,7 @@ inline FftPlan make_plan(int n)
     p.n = n;
     p.np = plan_radices(n, p.radix);
     NADIA_REQUIRE(p.np >= 0, NADIA_ERR_INVALID,
-                  "transform length " + std::to_string(n) + " has a prime factor above 64");
+                  "transform length " + std::to_string(n) + " has a prime factor above 1021");
     return p;
 }
 

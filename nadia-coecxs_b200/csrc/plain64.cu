@@ -120,6 +120,40 @@ __device__ void pass_generic(const double2 *src, double2 *dst, int n, int L, int
         const double2 *s = src + (size_t)sig * n;
         double2 *d = dst + (size_t)sig * n;
         const int k = j % Ns;
+        if (R > kMaxRadix) {
+            // large primes: the same sums, each twiddled input formed again
+            // from shared memory where it is used (identical arithmetic)
+            auto in = [&](int r) {
+                double2 x = s[j + r * m];
+                if (k > 0 && r > 0) {
+                    double2 w = __ldg(&W[k * r * tstep]);
+                    if (!fwd) w.y = -w.y;
+                    x = cmul(x, w);
+                }
+                return x;
+            };
+            const int base = (j / Ns) * Ns * R + k;
+            double2 y0 = in(0);
+            for (int r = 1; r < R; ++r) {
+                const double2 x = in(r);
+                y0.x = y0.x + x.x;
+                y0.y = y0.y + x.y;
+            }
+            double2 *out0 = d + base;
+            for (int sidx = 1; sidx < R; ++sidx) {
+                double2 acc = in(0);
+                for (int r = 1; r < R; ++r) {
+                    double2 w = __ldg(&W[((r * sidx) % R) * q]);
+                    if (!fwd) w.y = -w.y;
+                    double2 pp = cmul(in(r), w);
+                    acc.x = acc.x + pp.x;
+                    acc.y = acc.y + pp.y;
+                }
+                out0[sidx * Ns] = acc;
+            }
+            out0[0] = y0;
+            continue;
+        }
         double2 v[kMaxRadix];
         for (int r = 0; r < R; ++r) v[r] = s[j + r * m];
         if (k > 0) {

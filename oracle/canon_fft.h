@@ -41,7 +41,7 @@
 #include <string.h>
 
 #define CANON_MAX_PASSES 40
-#define CANON_MAX_RADIX 64
+#define CANON_MAX_RADIX 1021 /* the largest prime factor supported */
 
 /* Radix plan for length n.  Returns the number of passes, or -1 when n has a
  * prime factor larger than CANON_MAX_RADIX (not supported). */

@@ -162,6 +162,14 @@ def test_poly_vs_oracle(n, padding):
     compare(sc.poly_mixed(gpu, n=n, padding=padding), sc.poly_mixed(orc, n=n, padding=padding))
 
 
+def test_large_prime_lengths_vs_oracle():
+    """Transform lengths with prime factors above 64 (134 = 2 x 67, 2 x 131):
+    the prime butterflies' direct sums formed from shared memory."""
+    compare(sc.planar_mixed(gpu, n=134, ny=262, hio=6, raar=3, er=2),
+            sc.planar_mixed(orc, n=134, ny=262, hio=6, raar=3, er=2),
+            exact_keys=("esw", "support", "init"))
+
+
 @pytest.mark.parametrize("n,ny", [(35, 35), (33, 45), (30, 45)])
 def test_planar_odd_sizes_vs_oracle(n, ny):
     """Odd grids (PlanarCDI, FP64 form): the reference's quadrant swap on odd
@@ -287,10 +295,10 @@ def test_error_history_matches_get_error():
 
 def test_errors_are_status_codes():
     with pytest.raises(pynadia.NadiaError) as e:
-        gpu("planar", 33, 32)
+        gpu("fresnel", 33, 32)   # odd sizes: PlanarCDI only
     assert e.value.code == 1
     with pytest.raises(pynadia.NadiaError) as e:
-        gpu("planar", 134, 134)  # 67 is a prime above 64
+        gpu("planar", 2 * 1031, 64)  # 1031 is a prime above 1021
     assert e.value.code == 1
     p = gpu("poly", 32, 32)
     with pytest.raises(pynadia.NadiaError) as e:

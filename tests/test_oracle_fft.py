@@ -56,6 +56,15 @@ def test_parseval_and_round_trip():
     assert np.abs(back - a).max() < 1e-13
 
 
+@pytest.mark.parametrize("n", [134, 262, 3 * 127])
+def test_large_prime_factors(n):
+    """Prime factors above 64 (67, 131, 127): the prime butterfly's direct sum."""
+    g = np.random.default_rng(n)
+    a = g.standard_normal((n, 8)) + 1j * g.standard_normal((n, 8))
+    f = po.canon_fft2d(a, True)
+    assert np.abs(f - np.fft.fft2(a)).max() / np.abs(f).max() < 1e-12
+
+
 def test_unsupported_prime():
     with pytest.raises(ValueError):
-        po.canon_fft2d(np.zeros((67, 4), complex))
+        po.canon_fft2d(np.zeros((1031, 4), complex))   # 1031: a prime above 1021
