@@ -507,6 +507,21 @@ FRESNEL_SIZES = (512, 768, 1024, 1536, 2048)
 
 
 def fresnel_batch_report(pynadia, synth, n_items=64, iters=300):
+    """Config 4 twice: per-size launches on concurrent streams (the default)
+    and one launch per pass over a work list of every size (NADIA_MIXED=1)."""
+    out = _fresnel_batch(pynadia, synth, n_items, iters)
+    os.environ["NADIA_MIXED"] = "1"
+    try:
+        mixed = _fresnel_batch(pynadia, synth, n_items, iters)
+        out["one_launch_per_pass"] = {k: mixed[k] for k in ("seconds", "recon_per_s",
+                                                          "hbm_gbs_algorithmic", "roofline_frac",
+                                                          "tiles")}
+    finally:
+        del os.environ["NADIA_MIXED"]
+    return out
+
+
+def _fresnel_batch(pynadia, synth, n_items, iters):
     """64 FresnelCDI reconstructions in one nadia_iterate_many call, grids
     drawn uniformly from {512,768,1024,1536,2048}^2 (seeded), 8 keV, sample
     1 mm from focus, detector 1 m, 13.5 um pixels, disk objects of radius 30%

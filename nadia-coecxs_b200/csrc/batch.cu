@@ -134,17 +134,18 @@ bool batchable(const Solver &s)
            (s.algorithm == NADIA_ER || s.w[PFS] == 0);
 }
 
+// With NADIA_MIXED=1 in the environment when a batch is first stepped,
 // Planar/Fresnel reconstructions whose column length (nx) and row length (ny)
 // both have a mixed-length class run with their class's tile configuration,
 // alone or not: in the mixed passes when the call holds several such sizes,
 // in that configuration's single-length passes otherwise; either way the
 // same arithmetic, so a reconstruction's result never depends on the other
-// handles of a call.  (NADIA_MIXED=0 in the environment when a batch is
-// first stepped keeps it on the per-size tuned launches, for comparison.)
+// handles of a call.  Otherwise (the default: faster on B200) every size
+// group runs the batched tuner choice for its grid, the same alone or not.
 bool mixable(const Solver &s)
 {
     const char *env = getenv("NADIA_MIXED");
-    if (env && env[0] == '0') return false;
+    if (!(env && env[0] == '1')) return false;
     return s.kind != NADIA_POLY && f32::mix_variant(s.nx) && f32::mix_variant(s.ny);
 }
 

@@ -1,5 +1,6 @@
 // capi.cu -- the extern "C" entry points of libnadia_b200 (include/nadia_b200.h).
 // Each converts exceptions into status codes and never exits the process.
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <new>
@@ -745,7 +746,9 @@ extern "C" int nadia_tuned_tiles(int nx, int ny, int fresnel, int batched, char 
     return guard([&] {
         need(buf, "buf");
         NADIA_REQUIRE(len > 0, NADIA_ERR_INVALID, "empty buffer");
-        if (batched && nadia::f32::mix_variant(nx) && nadia::f32::mix_variant(ny)) {
+        const char *mixed = getenv("NADIA_MIXED");
+        if (batched && mixed && mixed[0] == '1' && nadia::f32::mix_variant(nx) &&
+            nadia::f32::mix_variant(ny)) {
             // batched Planar/Fresnel grids of these lengths run with their classes' tiles
             const std::string t = "column pass: " + nadia::f32::mix_describe(nx) +
                                   "; row pass: " + nadia::f32::mix_describe(ny);

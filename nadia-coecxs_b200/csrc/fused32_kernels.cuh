@@ -43,8 +43,9 @@ __device__ __forceinline__ float2 modulus(float2 u, float m, double &diff)
 // Psi = s0 X goes through the modulus projection, and the value handed to
 // the inverse transform is s0 times the projected Psi, that is X s0 m / |X|
 // ((s0 m, 0) where X = 0); the 1/sqrt(N) factors are folded into the
-// magnitude ratio.  Adds (|Psi| - m)^2 to diff for measured pixels (the
-// difference formed in FP32, its square summed in FP64).
+// magnitude ratio; unmeasured pixels (m < 0) keep Psi, so they leave as
+// s0^2 X.  Adds (|Psi| - m)^2 to diff for measured pixels (the difference
+// formed in FP32, its square summed in FP64).
 __device__ __forceinline__ float2 planar_modulus(float2 X, float m, float s0, double &diff)
 {
     const float a2 = X.x * X.x + X.y * X.y;
@@ -52,7 +53,7 @@ __device__ __forceinline__ float2 planar_modulus(float2 X, float m, float s0, do
     const bool zero = !(a2 > 0.f);
     const float inv = rsqrtf(zero ? 1.f : a2);
     const float sm = s0 * m;
-    const float sc = measured ? sm * inv : 1.f;
+    const float sc = measured ? sm * inv : s0 * s0; // unmeasured: Psi kept, s0 Psi = s0^2 X
     float2 r = make_float2(X.x * sc, X.y * sc);
     if (measured && zero) r = make_float2(sm, 0.f);
     const float mag = zero ? 0.f : a2 * inv;

@@ -2,7 +2,8 @@
 {512, 768, 1024, 1536, 2048}^2, disk objects of radius 30% of the grid, own
 seeds, HIO) in one nadia_iterate_many call: each member ends exactly where it
 ends when stepped alone through the same entry point (tolerance: bit for bit),
-and the autotuner reports the tiles it chose for every size."""
+with one launch per size and pass or one launch per pass over every size,
+and the library reports the tiles it runs for every size."""
 import numpy as np
 import pytest
 
@@ -28,7 +29,10 @@ def make(n, seed):
     return s
 
 
-def test_uneven_sizes_batch_equals_alone():
+@pytest.mark.parametrize("mixed", ["0", "1"], ids=["per-size launches", "one launch per pass"])
+def test_uneven_sizes_batch_equals_alone(mixed, monkeypatch):
+    # NADIA_MIXED=1: one launch per pass over a work list of every size
+    monkeypatch.setenv("NADIA_MIXED", mixed)
     rng = np.random.default_rng(4)
     sizes = [int(x) for x in rng.choice(SIZES, 7)] + [512]
     batch = [make(n, 10 + i) for i, n in enumerate(sizes)]

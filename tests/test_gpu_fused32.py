@@ -1,10 +1,11 @@
 """The fused FP32 form against the FP64 form (which matches the oracle bit for
 bit, tests/test_gpu_plain64.py).
 
-Tolerances: one iteration from the same state agrees to 2e-5 relative in
-the estimate (L2) and 2e-5 in the error metric -- the size of FP32 transform
-rounding; short runs (<= 20 iterations) keep every iterate's error metric
-within 1e-4 relative, the bar set for the FP32 form."""
+Tolerances: one iteration from the same state agrees to 5e-6 relative in
+the estimate (L2) and in the error metric -- a few times the measured FP32
+step error (about 1e-6: transforms of 2048 points in FP32 round at about
+6e-8 per pass); short runs (<= 20 iterations) keep every iterate's error
+metric within 1e-4 relative, the bar set for the FP32 form."""
 import numpy as np
 import pytest
 
@@ -14,7 +15,7 @@ from pynadia import synth
 
 pytestmark = pytest.mark.gpu
 
-STEP_TOL = 2e-5
+STEP_TOL = 5e-6
 RUN_TOL = 1e-4
 
 
