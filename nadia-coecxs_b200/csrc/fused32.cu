@@ -419,8 +419,28 @@ void encode_one(CUtensorMap *m, void *base, bool complex8, int nx, int ny, int r
 }
 } // namespace
 
+// panel-layout array (K, nx, ny/K) viewed by the grouped column pass: box
+// (cols of a panel, box_rows(nx) rows, 1 panel)
+void encode_cols(CUtensorMap *m, void *base, bool complex8, int nx, int ny, int cols)
+{
+    const int npan = ny / kPanel;
+    const cuuint64_t esz = complex8 ? 8 : 4;
+    cuuint64_t dims[3] = {(cuuint64_t)kPanel, (cuuint64_t)nx, (cuuint64_t)npan};
+    cuuint64_t strides[2] = {kPanel * esz, (cuuint64_t)nx * kPanel * esz};
+    cuuint32_t box[3] = {(cuuint32_t)cols, (cuuint32_t)box_rows(nx), 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode_fn()(m, complex8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                             3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    NADIA_REQUIRE(r == CUDA_SUCCESS, NADIA_ERR_CUDA,
+                  "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+}
+
 void encode_tensor_maps(Slot &s, int nx, int ny)
 {
+    encode_cols(&s.tc[0], s.P, true, nx, ny, 2);
+    encode_cols(&s.tc[1], (void *)s.mI, false, nx, ny, 4);
     const int rows[5] = {1, 2, 4, 8, 16};
     for (int k = 0; k < 5; ++k) {
         if (nx % rows[k]) {
@@ -675,7 +695,7 @@ Fused32::Impl::Impl(Solver &s) : S(s)
     sup.alloc(n);
     mI.alloc(n);
     ncol = poly ? 0 : ny / choice->col->L;
-    partials.alloc(ny / kPanel);
+    partials.alloc(ny / 2); // one per column tile (tiles of two columns at least)
     iter.alloc(1);
     flag.alloc(1);
     slot.alloc(1);
@@ -780,7 +800,7 @@ void Fused32::Impl::prepare_pfs()
 {
     if (!Q) {
         Q.alloc(n);
-        qpartials.alloc(ny / kPanel);
+        qpartials.alloc(ny / 2);
         qslot.alloc(1);
         qslot_ptr.alloc(1);
         NADIA_CUDA(cudaMemsetAsync(Q.p, 0, Q.bytes(), S.st));

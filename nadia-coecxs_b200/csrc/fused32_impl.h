@@ -21,6 +21,9 @@ struct alignas(64) Slot {
     // tensor maps over P, x and the support for row tiles of 1, 2, 4, 8 and
     // 16 rows (persistent row passes); box (K, rows, <= 256 panels)
     CUtensorMap tm[5][3];
+    // grouped column pass: P as column pairs (box (2, <= 256 rows, 1 panel))
+    // and sqrt(I) as whole panels (box (4, <= 256 rows, 1 panel))
+    CUtensorMap tc[2];
     float2 *P;              // work array (row transforms of x / column-pass output)
     float2 *x;              // estimate
     const float *sup;       // support
@@ -98,6 +101,15 @@ struct Gauss {
     float w[6];
     int cut;
 };
+
+// rows (x) per tensor box of the grouped column pass: the largest divisor of
+// nx that is at most 256
+__host__ __device__ inline int box_rows(int nx)
+{
+    for (int d = nx < 256 ? nx : 256; d > 1; --d)
+        if (nx % d == 0) return d;
+    return 1;
+}
 
 // panels per tensor box: the largest divisor of the panel count that is at
 // most 256 (the TMA box limit), so the boxes tile a row tile exactly

@@ -574,6 +574,49 @@ void launch_row_grouped(int mode, const Slot *const *slots, int nslots, int nx, 
     kg_row<C><<<grid, C::NT * C::GROUPS, grouped_row_smem<C>(), st>>>(slots, nslots, nx, ny, tw);
 }
 
+template <class C>
+void prepare_grouped_col()
+{
+    NADIA_CUDA(cudaFuncSetAttribute(kg_col<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)grouped_col_smem<C>()));
+    NADIA_CUDA(cudaFuncSetAttribute(kg_col<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)grouped_col_smem<C>()));
+}
+
+template <class C>
+void launch_col_grouped(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
+                        const float2 *tw, cudaStream_t st)
+{
+    const int ntiles = (ny / C::L) * nslots;
+    const int ctas = (ntiles + C::GROUPS - 1) / C::GROUPS;
+    const int grid = ctas < sm_count() ? ctas : sm_count();
+    if (fresnel)
+        kg_col<C, true><<<grid, C::NT * C::GROUPS, grouped_col_smem<C>(), st>>>(slots, nslots, nx, ny, tw);
+    else
+        kg_col<C, false><<<grid, C::NT * C::GROUPS, grouped_col_smem<C>(), st>>>(slots, nslots, nx, ny, tw);
+}
+
+// The column pass in G independent groups of NT threads a CTA, each on half
+// panels (two columns); no row pass.
+template <int N, int NT, int L, int G, class SW, int... Rs>
+TileVariant make_grouped_col(const char *radices)
+{
+    static_assert(L == 2, "half-panel tiles");
+    using CC = TileCfg<N, NT, 2, kRowMap, Radices<Rs...>, SW, 1, false, G>;
+    static_assert(grouped_col_smem<CC>() <= 227 * 1024, "grouped column stages too large");
+    TileVariant t;
+    t.n = N;
+    t.nt = NT;
+    t.L = 2;
+    t.minb = 1;
+    t.persistent = true;
+    t.groups = G;
+    t.radices = radices;
+    t.prepare = &prepare_grouped_col<CC>;
+    t.col = &launch_col_grouped<CC>;
+    return t;
+}
+
 template <int N, int NT, int L, int G, class SW, int... Rs>
 TileVariant make_grouped_row(const char *radices)
 {

@@ -496,5 +496,160 @@ __global__ void __launch_bounds__(C::NT * C::GROUPS, 1)
     if (u == 0) tma::bulk_wait_all();
 }
 
+// FP64 sum over the thread's group; the result is valid in the group's
+// first thread.  Synchronises the group.
+template <class C>
+__device__ __forceinline__ double group_sum(double v)
+{
+    __shared__ double red[C::GROUPS][C::NT / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    const int g = threadIdx.x / C::NT, u = threadIdx.x % C::NT;
+    if ((u & 31) == 0) red[g][u >> 5] = v;
+    C::sync();
+    double t = 0;
+    if (u == 0)
+        for (int w = 0; w < C::NT / 32; ++w) t += red[g][w];
+    return t;
+}
+
+// The column pass in C::GROUPS independent groups of C::NT threads: a group's
+// tile is half a panel (two whole columns of length nx = C::N, C::L == 2).
+// Per group: two stages of P (column pairs through the tensor map tc[0]),
+// one stage of sqrt(I) (the tile's whole panel through tc[1], refilled for
+// the next tile as soon as the modulus has read it), its own mbarriers, its
+// own TMA issue thread and named-barrier exchanges.  Error partials are kept
+// per half panel.
+template <class C>
+constexpr size_t grouped_col_smem()
+{
+    return (size_t)C::GROUPS * ((size_t)C::N * C::L * 16 + (size_t)C::N * 16) + 24 * C::GROUPS;
+}
+
+template <class C, bool FRESNEL>
+__global__ void __launch_bounds__(C::NT * C::GROUPS, 1)
+    kg_col(const Slot *const *slots, int nslots, int nx, int ny, const float2 *__restrict__ tw)
+{
+    static_assert(C::GROUPS > 1 && C::L == 2, "grouped tiles of two columns");
+    constexpr int G = C::GROUPS;
+    constexpr int TW = C::N * C::L;
+    constexpr size_t GB = (size_t)TW * 16 + (size_t)C::N * 16;
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    const int g = threadIdx.x / C::NT, u = threadIdx.x % C::NT;
+    float2 *Pb0 = reinterpret_cast<float2 *>(smraw + (size_t)g * GB);
+    float2 *Pb1 = Pb0 + TW;
+    float *Mb = reinterpret_cast<float *>(Pb1 + TW);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + (size_t)G * GB) + 3 * g;
+    const int tps = ny / C::L; // half-panel tiles per reconstruction
+    const int ntiles = tps * nslots;
+    const int bx = box_rows(nx);
+
+    if (u == 0) {
+        tma::mbar_init(&bar[0], 1);
+        tma::mbar_init(&bar[1], 1);
+        tma::mbar_init(&bar[2], 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+
+    int t = blockIdx.x * G + g;
+    const int stride = gridDim.x * G;
+    if (t >= ntiles) return; // a group without tiles (no CTA-wide barrier follows)
+    const Slot &S0 = *slots[t / tps];
+    const uint32_t polls = S0.wait_polls ? S0.wait_polls : kWaitPolls;
+    const bool skip0 = S0.skip_first_load != 0;
+    auto issue_p = [&](int tile, int b, bool skip) {
+        const Slot &S = *slots[tile / tps];
+        const int tt = tile % tps, panel = tt >> 1, half = tt & 1;
+        float2 *dst = b ? Pb1 : Pb0;
+        tma::mbar_arrive_expect_tx(&bar[b], TW * 8);
+        if (skip) return;
+        for (int x0 = 0; x0 < nx; x0 += bx)
+            tma::tensor_load_3d(dst + (size_t)x0 * 2, &S.tc[0], 2 * half, x0, panel, &bar[b]);
+    };
+    auto issue_m = [&](int tile) {
+        const Slot &S = *slots[tile / tps];
+        const int panel = (tile % tps) >> 1;
+        tma::mbar_arrive_expect_tx(&bar[2], C::N * 16);
+        for (int x0 = 0; x0 < nx; x0 += bx)
+            tma::tensor_load_3d(Mb + (size_t)x0 * 4, &S.tc[1], 0, x0, panel, &bar[2]);
+    };
+    if (u == 0) {
+        issue_p(t, 0, skip0);
+        issue_m(t);
+    }
+
+    for (int it = 0; t < ntiles; ++it, t += stride) {
+        const int b = it & 1;
+        float2 *Pb = b ? Pb1 : Pb0;
+        const Slot &S = *slots[t / tps];
+        const int tt = t % tps, panel = tt >> 1, half = tt & 1;
+        const int tn = t + stride;
+        if (u == 0 && tn < ntiles) {
+            tma::bulk_wait_read_all();
+            issue_p(tn, b ^ 1, false);
+        }
+        bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
+        if (group_or<C>(!ok)) {
+            // every copy issued so far lands before the group leaves
+            if (u == 0) {
+                raise_flag(S);
+                tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
+                tma::mbar_wait(&bar[2], it & 1, polls);
+                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+            }
+            break;
+        }
+        float2 v[C::E];
+        for_each_slot<C, true, true>([&](int e, int s, int pos) { v[e] = Pb[pos * 2 + s]; });
+        C::sync();
+        transform<C, true>(v, Pb, tw);
+
+        ok = tma::mbar_wait(&bar[2], it & 1, polls);
+        if (group_or<C>(!ok)) {
+            if (u == 0) {
+                raise_flag(S);
+                tma::mbar_wait(&bar[2], it & 1, polls);
+                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+            }
+            break;
+        }
+        const float s0 = S.s0;
+        double diff = 0.0;
+        for_each_slot<C, true, false>([&](int e, int s, int kx) {
+            const float mm = Mb[kx * 4 + 2 * half + s];
+            float2 X = v[e];
+            if (!FRESNEL) {
+                X = planar_modulus(X, mm, s0, diff);
+            } else {
+                const int ky = panel * kPanel + 2 * half + s;
+                const float2 cf = cmul(__ldg(&S.tx[kx]), __ldg(&S.ty[ky]));
+                const float2 w = __ldg(&S.W[paddr(kx, ky, nx)]);
+                const float2 uu = modulus(cadd(cscale(cmul(cf, X), s0), w), mm, diff);
+                X = cscale(cmulc(csub(uu, w), cf), s0);
+            }
+            v[e] = X;
+        });
+        const double tot = group_sum<C>(diff); // the group has read sqrt(I)
+        if (u == 0) {
+            S.partials[tt] = tot;
+            if (tn < ntiles) {
+                tma::fence_async_shared();
+                issue_m(tn);
+            }
+        }
+        transform<C, false>(v, Pb, tw);
+        for_each_slot<C, false, false>([&](int e, int s, int pos) { Pb[pos * 2 + s] = v[e]; });
+        tma::fence_async_shared();
+        C::sync();
+        if (u == 0) {
+            for (int x0 = 0; x0 < nx; x0 += bx)
+                tma::tensor_store_3d(&S.tc[0], 2 * half, x0, panel, Pb + (size_t)x0 * 2);
+            tma::bulk_commit();
+        }
+    }
+    if (u == 0) tma::bulk_wait_all();
+}
+
 } // namespace f32
 } // namespace nadia

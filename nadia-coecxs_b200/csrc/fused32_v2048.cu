@@ -34,6 +34,9 @@ void add_variants_2048(std::vector<TileVariant> &v)
     // ping-pong exchanges (one barrier per exchange)
     v.push_back(make_persistent_mstage<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
     v.push_back(make_persistent_mstage<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
+    // column passes in two independent groups of 256 threads (half panels)
+    v.push_back(make_grouped_col<2048, 256, 2, 2, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
+    v.push_back(make_grouped_col<2048, 256, 2, 2, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
     // row passes in independent groups: four of 128 threads (one row each) or
     // two of 256 (two rows each), every group with its own pipeline
     v.push_back(make_grouped_row<2048, 128, 1, 4, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));

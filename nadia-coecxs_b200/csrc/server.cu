@@ -47,7 +47,7 @@ size_t footprint_bytes(int kind, int nx, int ny, int prec, int n_best, int pad_n
                  16 * (size_t)(pad_nx + pad_ny);
     } else {
         b += n * (8 + 8 + 4 + 4);                     // P, x, support, sqrt(I)
-        b += 8 * (size_t)(ny / 4) + 8 + 4 + 2 * 8;    // partials, counter, flag, slot pointer
+        b += 8 * (size_t)(ny / 2) + 8 + 4 + 2 * 8;    // partials, counter, flag, slot pointer
         b += sizeof(f32::Slot);
         const size_t tiles = ((size_t)(nx + 31) / 32) * ((ny + 31) / 32);
         b += 2 * 4 * n + 4 * (std::max<size_t>(tiles, 592) + 2); // shrinkwrap scratch
