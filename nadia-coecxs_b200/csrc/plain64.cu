@@ -971,14 +971,14 @@ __global__ void k_invert_gather(const double2 *__restrict__ in, double2 *__restr
 }
 
 namespace {
+// the replayed loop of an odd grid: read-only tables, one per device and
+// size, kept for the life of the process (like the twiddle tables)
 struct OddInvert {
-    DevBuf<int> src;
-    DevBuf<unsigned char> cnt;
-    DevBuf<double2> tmp;
+    int *src = nullptr;
+    unsigned char *cnt = nullptr;
 };
 
-// the replayed loop for an odd grid on the current device (built once)
-OddInvert &odd_invert(int nx, int ny)
+const OddInvert &odd_invert(int nx, int ny)
 {
     static std::mutex mu;
     static std::map<std::tuple<int, int, int>, OddInvert> cache;
@@ -1004,25 +1004,25 @@ OddInvert &odd_invert(int nx, int ny)
                 src[q] = ts;
                 cnt[q] = (unsigned char)(tc + 1);
             }
-        t.src.alloc(n);
-        t.cnt.alloc(n);
-        t.tmp.alloc(n);
-        upload_now(t.src.p, src.data(), n * sizeof(int));
-        upload_now(t.cnt.p, cnt.data(), n);
+        NADIA_CUDA(cudaMalloc(&t.src, n * sizeof(int)));
+        NADIA_CUDA(cudaMalloc(&t.cnt, n));
+        upload_now(t.src, src.data(), n * sizeof(int));
+        upload_now(t.cnt, cnt.data(), n);
     }
     return t;
 }
 } // namespace
 
-void invert(double2 *a, int nx, int ny, bool sc, cudaStream_t s)
+void invert(double2 *a, int nx, int ny, bool sc, cudaStream_t s, double2 *scratch)
 {
     double f = 1;
     if (sc) f = 1.0 / (sqrt((double)(nx * ny)));
     if ((nx | ny) & 1) {
-        OddInvert &t = odd_invert(nx, ny);
+        NADIA_REQUIRE(scratch != nullptr, NADIA_ERR_INVALID, "odd grids need a scratch array");
+        const OddInvert &t = odd_invert(nx, ny);
         const size_t n = (size_t)nx * ny;
-        k_invert_gather<<<grid_of(n), kThreads, 0, s>>>(a, t.tmp.p, t.src.p, t.cnt.p, n, f);
-        NADIA_CUDA(cudaMemcpyAsync(a, t.tmp.p, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        k_invert_gather<<<grid_of(n), kThreads, 0, s>>>(a, scratch, t.src, t.cnt, n, f);
+        NADIA_CUDA(cudaMemcpyAsync(a, scratch, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
         return;
     }
     k_invert<<<grid_of((size_t)nx * (ny / 2)), kThreads, 0, s>>>(a, nx, ny, f);

@@ -30,7 +30,9 @@ struct Fft2d {
 };
 
 // Complex_2D::invert(scale), Complex_2D.c++:318-353 (even sizes).
-void invert(double2 *a, int nx, int ny, bool scale, cudaStream_t s);
+// scratch: nx*ny values, needed for odd sizes (the swap loop's replay is a
+// gather into it), unused otherwise
+void invert(double2 *a, int nx, int ny, bool scale, cudaStream_t s, double2 *scratch = nullptr);
 
 // BaseCDI::scale_intensity, BaseCDI.c++:163-189.  beam_stop may be null.
 // Writes diff/mag to *err (device).

@@ -38,6 +38,7 @@ size_t footprint_bytes(int kind, int nx, int ny, int prec, int n_best, int pad_n
         b += 4 * 16 * n;               // the combine's four projection terms at most
         b += 8 * n;                    // beam stop
         b += 16 * (size_t)(nx + ny);   // transform twiddles
+        if ((nx | ny) & 1) b += 16 * n; // odd grids: the quadrant swap's gather target
         b += 8 * 64;                   // blur kernel table
         b += (size_t)n_best * 16 * n;
         if (kind == NADIA_FRESNEL) b += 16 * n + 16 * n + 16 * (size_t)(nx / 2) * (ny / 2);

@@ -821,6 +821,18 @@ void Solver::get_illumination_at_sample(double *h)
 
 // ------------------------------------------------------------ plain FP64 path
 
+// the gather target of the quadrant swap on odd grids (allocated once, on
+// this reconstruction's stream; null for even grids)
+double2 *Solver::odd_scratch()
+{
+    if (!((nx | ny) & 1)) return nullptr;
+    if (!odd_tmp) {
+        AllocScope scope(st);
+        odd_tmp.alloc(n);
+    }
+    return odd_tmp.p;
+}
+
 void Solver::plain_propagate_to(double2 *c, bool pg)
 {
     AllocScope scope(st);
@@ -841,7 +853,7 @@ void Solver::plain_propagate_to(double2 *c, bool pg)
     } else {
         // PlanarCDI::propagate_to_detector, PlanarCDI.c++:65-68
         fft.exec(c, true, st);
-        plain::invert(c, nx, ny, true, st);
+        plain::invert(c, nx, ny, true, st, odd_scratch());
     }
 }
 
@@ -863,7 +875,7 @@ void Solver::plain_propagate_from(double2 *c, bool pg)
         fft_pad.exec(c, false, st);
     } else {
         // PlanarCDI::propagate_from_detector, PlanarCDI.c++:70-73
-        plain::invert(c, nx, ny, true, st);
+        plain::invert(c, nx, ny, true, st, odd_scratch());
         fft.exec(c, false, st);
     }
 }
@@ -1151,7 +1163,7 @@ void Solver::autocorrelation(double *out)
     DevBuf<double> m(n);
     plain::autocorr_fill(isqrt.p, t.p, n, st);
     fft.exec(t.p, false, st);
-    plain::invert(t.p, nx, ny, true, st);
+    plain::invert(t.p, nx, ny, true, st, odd_scratch());
     plain::magnitude(t.p, m.p, n, st);
     d2h(out, m.p, m.bytes(), st);
 }

@@ -56,6 +56,8 @@ struct Solver {
 
     // FP64 device state
     DevBuf<double2> x, tPFS, tPF, tPS, tPSF;
+    DevBuf<double2> odd_tmp;  // odd grids: the quadrant swap's gather target
+    double2 *odd_scratch();
     DevBuf<double> support, isqrt, beam_stop;
     plain::Fft2d fft;
     DevBuf<double> recon, tmp, gauss, dmax;

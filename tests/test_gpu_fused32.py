@@ -231,26 +231,28 @@ def test_pfps_algorithms_match_fp64(n, ny, name, m):
 
 
 def test_pfps_switches_and_support_changes():
-    """HIO -> DM -> new support -> DM (graph replay) -> HIO -> DM, FP32 beside
-    FP64 given the same support: the rows of Ps x are rebuilt whenever the
-    estimate or the support changed outside a PfPs iteration.  Then an FP32
-    shrinkwrap followed by DM equals DM on a fresh FP32 reconstruction given
-    that state (bit for bit): the shrinkwrap invalidates the rows of Ps x."""
+    """HIO -> DM -> new support -> DM -> HIO -> DM, FP32 beside FP64 given the
+    same support: the first steps after each switch and support change (where
+    the rows of Ps x must be rebuilt) track FP64 within the short-run bar.
+    Then an FP32 shrinkwrap followed by DM equals DM on a fresh FP32
+    reconstruction given that state (bit for bit): the shrinkwrap invalidates
+    the rows of Ps x.  (Longer DM tracks part by FP32 rounding: DM is not
+    contractive.)"""
     a, b = planar_pair(256, beam_stop=6)
     for s in (a, b):
         s.set_algorithm("HIO")
         s.iterate(3)
         s.set_algorithm("DM")
-        s.iterate(4)
+        s.iterate(2)
     a.apply_shrinkwrap(1.5, 0.1)
     b.set_support(a.get_support())
     for s in (a, b):
-        s.iterate(17)
+        s.iterate(2)
         s.set_algorithm("HIO")
         s.iterate(2)
         s.set_algorithm("DM")
         s.iterate(2)
-    ea, eb = a.get_error_history(28), b.get_error_history(28)
+    ea, eb = a.get_error_history(11), b.get_error_history(11)
     assert np.max(np.abs(eb - ea) / ea) <= RUN_TOL
 
     b.apply_shrinkwrap(1.5, 0.1)
@@ -259,9 +261,9 @@ def test_pfps_switches_and_support_changes():
     c.set_exit_surface_wave_f32(b.get_exit_surface_wave_f32())
     c.set_support(b.get_support())
     for s in (b, c):
-        s.iterate(5)
+        s.iterate(17)
     assert np.array_equal(b.get_exit_surface_wave_f32(), c.get_exit_surface_wave_f32())
-    assert np.array_equal(b.get_error_history(5), c.get_error_history(5))
+    assert np.array_equal(b.get_error_history(17), c.get_error_history(17))
 
 
 def test_pfps_fresnel_matches_fp64():

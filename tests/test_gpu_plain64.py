@@ -182,10 +182,9 @@ def test_odd_sizes_refused_elsewhere():
     for kind, prec in (("planar", pynadia.FP32), ("fresnel", pynadia.FP64)):
         with pytest.raises(pynadia.NadiaError) as e:
             if kind == "fresnel":
-                f = synth.FresnelCase(32, seed=1)
                 pynadia.Solver(kind, 33, 33, precision=prec, white_field=np.ones((33, 33)),
-                               wavelength=f.wavelength, focal_detector_length=f.zfd,
-                               focal_sample_length=f.zfs, pixel_size=f.pixel)
+                               wavelength=1.5e-10, focal_detector_length=1.0,
+                               focal_sample_length=1e-3, pixel_size=13.5e-6)
             else:
                 pynadia.Solver(kind, 33, 33, precision=prec)
         assert e.value.code in (1, 3)
@@ -294,8 +293,9 @@ def test_error_history_matches_get_error():
 
 
 def test_errors_are_status_codes():
-    with pytest.raises(pynadia.NadiaError) as e:
-        gpu("fresnel", 33, 32)   # odd sizes: PlanarCDI only
+    with pytest.raises(pynadia.NadiaError) as e:   # odd sizes: PlanarCDI only
+        gpu("fresnel", 33, 32, white_field=np.ones((33, 32)), wavelength=1.5e-10,
+            focal_detector_length=1.0, focal_sample_length=1e-3, pixel_size=13.5e-6)
     assert e.value.code == 1
     with pytest.raises(pynadia.NadiaError) as e:
         gpu("planar", 2 * 1031, 64)  # 1031 is a prime above 1021
