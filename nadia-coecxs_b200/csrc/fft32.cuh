@@ -225,6 +225,7 @@ template <bool FWD> struct Dft<15, FWD> : Pfa<3, 5, FWD> {};
 
 template <int... Rs>
 struct Radices {
+    static constexpr bool TWD = false; // twiddles formed as products (see pass_compute)
     static constexpr int P = sizeof...(Rs);
     static constexpr int get(int p)
     {
@@ -247,6 +248,13 @@ struct Radices {
         }
         return l;
     }
+};
+
+// The same radix list with every inter-pass twiddle loaded from the table
+// (one load a twiddle instead of loads and products)
+template <int... Rs>
+struct RadicesTW : Radices<Rs...> {
+    static constexpr bool TWD = true;
 };
 
 // Tile transform configuration.  MAP selects how butterflies are dealt to
@@ -290,6 +298,7 @@ template <int N_, int NT_, int L_, int MAP_, class RL, class SW, int MINB_ = 1, 
 struct TileCfg {
     static constexpr int N = N_, NT = NT_, L = L_, MAP = MAP_, MINB = MINB_, GROUPS = GROUPS_;
     static constexpr bool PING = PING_;
+    static constexpr bool TWD = RL::TWD;
     static __device__ __forceinline__ int tid() { return GROUPS > 1 ? threadIdx.x % NT : threadIdx.x; }
     static __device__ __forceinline__ void sync()
     {
@@ -371,6 +380,16 @@ __device__ __forceinline__ void pass_compute(float2 (&v)[C::E], const float2 *__
             int s, j;
             C::map(C::tid() + q * C::NT, NR, s, j);
             const int t1 = (j % Ns) * TSTEP;
+            if constexpr (C::TWD) {
+                // every W^(t1*r) from the table (t1*r < N)
+                float2 w[R];
+#pragma unroll
+                for (int r = 1; r < R; ++r) w[r] = twiddle<FWD>(tw, t1 * r);
+#pragma unroll
+                for (int r = 1; r < R; ++r) v[q * R + r] = cmul(v[q * R + r], w[r]);
+                Dft<R, FWD>::run(&v[q * R]);
+                continue;
+            }
             // W^(t1*r) applied as formed: W^t1 is loaded and squared/cubed for
             // r = 1..3; W^(4a t1) is loaded for each group of four and
             // multiplied by those (at most two products per twiddle, few

@@ -474,12 +474,12 @@ TileVariant make_ping(const char *radices)
 
 // The same tile shape as persistent, TMA-pipelined passes (tiles of at most
 // 8192 elements, so both stages fit in shared memory); MINB CTAs per SM where
-// shared memory allows.
-template <int N, int NT, int L, int MINB, class SW, int... Rs>
-TileVariant make_persistent(const char *radices)
+// shared memory allows.  RL: the radix list type (Radices or RadicesTW).
+template <int N, int NT, int L, int MINB, class SW, class RL>
+TileVariant make_persistent_rl(const char *radices)
 {
-    using CC = TileCfg<N, NT, L, kColMap, Radices<Rs...>, SW, MINB>;
-    using CR = TileCfg<N, NT, L, kRowMap, Radices<Rs...>, SW, MINB>;
+    using CC = TileCfg<N, NT, L, kColMap, RL, SW, MINB>;
+    using CR = TileCfg<N, NT, L, kRowMap, RL, SW, MINB>;
     static_assert(persist_row_smem<CR>() <= 227 * 1024, "persistent row tile too large");
     TileVariant t;
     t.n = N;
@@ -492,6 +492,17 @@ TileVariant make_persistent(const char *radices)
     t.col = &launch_col_persistent<CC, 2>;
     t.row = &launch_row_persistent<CR>;
     return t;
+}
+
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_persistent(const char *radices)
+{
+    return make_persistent_rl<N, NT, L, MINB, SW, Radices<Rs...>>(radices);
+}
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_persistent_tw(const char *radices)
+{
+    return make_persistent_rl<N, NT, L, MINB, SW, RadicesTW<Rs...>>(radices);
 }
 
 // A persistent column pass with one stage per CTA (MINB CTAs share an SM);
@@ -617,10 +628,10 @@ TileVariant make_grouped_col(const char *radices)
     return t;
 }
 
-template <int N, int NT, int L, int G, class SW, int... Rs>
-TileVariant make_grouped_row(const char *radices)
+template <int N, int NT, int L, int G, class SW, class RL>
+TileVariant make_grouped_row_rl(const char *radices)
 {
-    using CR = TileCfg<N, NT, L, kRowMap, Radices<Rs...>, SW, 1, false, G>;
+    using CR = TileCfg<N, NT, L, kRowMap, RL, SW, 1, false, G>;
     static_assert(grouped_row_smem<CR>() <= 227 * 1024, "grouped row stages too large");
     TileVariant t;
     t.n = N;
@@ -633,6 +644,17 @@ TileVariant make_grouped_row(const char *radices)
     t.prepare = &prepare_grouped_row<CR>;
     t.row = &launch_row_grouped<CR>;
     return t;
+}
+
+template <int N, int NT, int L, int G, class SW, int... Rs>
+TileVariant make_grouped_row(const char *radices)
+{
+    return make_grouped_row_rl<N, NT, L, G, SW, Radices<Rs...>>(radices);
+}
+template <int N, int NT, int L, int G, class SW, int... Rs>
+TileVariant make_grouped_row_tw(const char *radices)
+{
+    return make_grouped_row_rl<N, NT, L, G, SW, RadicesTW<Rs...>>(radices);
 }
 
 // A persistent column pass with two stages of P, one stage of sqrt(I)

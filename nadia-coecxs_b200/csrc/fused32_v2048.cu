@@ -43,6 +43,9 @@ void add_variants_2048(std::vector<TileVariant> &v)
     v.push_back(make_grouped_row<2048, 128, 1, 4, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
     v.push_back(make_grouped_row<2048, 256, 2, 2, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16"));
     v.push_back(make_grouped_row<2048, 256, 2, 2, Swizzle<4, 5, 7, 1>, 16, 16, 8>("16.16.8"));
+    // the best column and row shapes with every twiddle loaded from the table
+    v.push_back(make_persistent_tw<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16 tw"));
+    v.push_back(make_grouped_row_tw<2048, 128, 1, 4, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16 tw"));
 }
 
 } // namespace f32

@@ -34,7 +34,7 @@ CSRC = os.path.join(ROOT, "nadia-coecxs_b200", "csrc")
 K = 4  # panel width
 
 PAT = re.compile(r"make_(variant|ping|persistent_single|persistent_direct|persistent_ping|persistent_mstage|"
-                 r"persistent_row|grouped_row|grouped_col|persistent|poly)<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+),\s*"
+                 r"persistent_row|grouped_row_tw|grouped_row|grouped_col|persistent_tw|persistent|poly)<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+),\s*"
                  r"Swizzle<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+)>\s*,\s*([\d,\s]+)>")
 
 
@@ -187,7 +187,8 @@ def maps_of(v):
     """The thread maps a variant runs: row-only variants have no column pass,
     column-only (one-stage persistent) variants no row pass."""
     ms = [] if v["kind"] in COLUMN_ONLY else [("row", rowmap)]
-    if v["L"] % K == 0 and v["kind"] not in ("persistent_row", "grouped_row", "grouped_col"):
+    if v["L"] % K == 0 and v["kind"] not in ("persistent_row", "grouped_row", "grouped_row_tw",
+                                              "grouped_col"):
         ms.insert(0, ("col", colmap))
     return ms
 
@@ -205,13 +206,13 @@ def test_tile_shape_constraints(v):
     E = N * L // NT
     assert E % reduce(lambda a, b: a * b // gcd(a, b), rad) == 0
     assert all((N // r) % K == 0 for r in rad), "row tiles need N/R divisible by the panel"
-    if v["kind"] not in ("persistent_row", "grouped_row", "grouped_col"):
+    if v["kind"] not in ("persistent_row", "grouped_row", "grouped_row_tw", "grouped_col"):
         assert L % K == 0, "column tiles cover whole panels"
-    if v["kind"] == "grouped_row":   # minb holds the group count
+    if v["kind"] in ("grouped_row", "grouped_row_tw"):   # minb holds the group count
         assert v["minb"] * (N * L * 28 + 24) <= 227 * 1024
     if v["kind"] == "grouped_col":   # half panels: two P stages, one sqrt(I) panel
         assert L == 2 and v["minb"] * (N * L * 16 + N * 16 + 24) <= 227 * 1024
-    if v["kind"] in ("persistent", "mixed"):
+    if v["kind"] in ("persistent", "persistent_tw", "mixed"):
         assert N * L * 28 + 24 <= 227 * 1024
     # several CTAs per SM share its 228 KB (1 KB reserved per CTA)
     if v["kind"] == "persistent_row":
