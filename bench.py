@@ -604,6 +604,26 @@ def white_field_report(pynadia, synth, n=2048, iters=26):
     out = {"grid": [n, n], "iterations": iters, "gpu_fp64_ms_per_iteration": 1000.0 * sec / iters,
            "gpu_fp64_recon_per_s": 1.0 / sec, "final_error": err,
            "hbm_gbs_algorithmic": gbs, "roofline_frac": gbs / peak}
+    # the FP32 form: one column pass (P 8 + support 4 read, P 8 written) and one
+    # row pass (P 8 + sqrt(I) 4 read, x 8 + P 8 written) = 48 B/px, eight
+    # transforms; the same problem and iteration count
+    s = pynadia.Solver("fresnel_wf", n, n, precision=pynadia.FP32, **kw)
+    s.set_wf_support(f.z_diameter)
+    s.set_intensity(f.intensity)
+    s.initialise_estimate(0)
+    s.iterate(2)
+    s.synchronize()
+    st = torch.cuda.ExternalStream(s.stream())
+    a.record(st)
+    s.iterate(iters)
+    b.record(st)
+    b.synchronize()
+    sec32 = a.elapsed_time(b) / 1000.0
+    gbs32 = 48.0 * n * n * iters / sec32 / 1e9
+    out["fp32"] = {"ms_per_iteration": 1000.0 * sec32 / iters, "recon_per_s": 1.0 / sec32,
+                   "final_error": s.get_error(), "over_fp64": sec / sec32,
+                   "hbm_gbs_algorithmic": gbs32, "roofline_frac": gbs32 / peak}
+    s.close()
     sys.path.insert(0, ORACLE)
     import pyoracle as po
     if po.reference_available("32_fast"):

@@ -1,7 +1,9 @@
 // FresnelCDI_WF.h -- drop-in for the reference's FresnelCDI_WF
 // (NADIA/include/FresnelCDI_WF.h): recovery of the detector-plane white field
-// that FresnelCDI takes as its illumination, on the GPU in the FP64 form.
-// The estimate handed to the constructor is the detector-plane field.
+// that FresnelCDI takes as its illumination, on the GPU: in the float build
+// in the fused FP32 form where the grid has FP32 tiles (BaseCDI::precision_for),
+// else in the FP64 form.  The estimate handed to the constructor is the
+// detector-plane field.
 #ifndef NADIA_DROPIN_FRESNELCDI_WF_H
 #define NADIA_DROPIN_FRESNELCDI_WF_H
 
@@ -18,7 +20,7 @@ public:
         : BaseCDI(initial_guess, n_best)
     {
         nadia_solver *s = nullptr;
-        nadia_cxx::check(nadia_fresnel_wf_create(nx, ny, NADIA_FP64, beam_wavelength,
+        nadia_cxx::check(nadia_fresnel_wf_create(nx, ny, precision_for(nx, ny), beam_wavelength,
                                                  zone_focal_length, focal_detector_length,
                                                  pixel_size, n_best, &s));
         adopt(s);

@@ -129,7 +129,7 @@ std::list<std::unique_ptr<Plan>> g_plans; // most recently used first
 
 bool batchable(const Solver &s)
 {
-    return s.prec == NADIA_FP32 && s.n_best == 0 && !s.tc.active &&
+    return s.prec == NADIA_FP32 && s.n_best == 0 && !s.tc.active && s.kind != NADIA_FRESNEL_WF &&
            (s.kind != NADIA_POLY || s.f32->impl->pcol != nullptr) &&
            (s.algorithm == NADIA_ER || s.w[PFS] == 0);
 }

@@ -680,6 +680,7 @@ Fused32::Impl::Impl(Solver &s) : S(s)
     ny = s.ny;
     n = s.n;
     const bool poly = s.kind == NADIA_POLY;
+    const bool wf = s.kind == NADIA_FRESNEL_WF;
     if (poly) {
         // the transforms run on the padded grid, sized by set_spectrum
         NADIA_REQUIRE(nx % 8 == 0 && ny % 4 == 0, NADIA_ERR_UNSUPPORTED,
@@ -688,14 +689,27 @@ Fused32::Impl::Impl(Solver &s) : S(s)
         NADIA_REQUIRE(supported(nx) && supported(ny), NADIA_ERR_UNSUPPORTED,
                       "the FP32 form supports grid sizes 256, 512, 768, 1024, 1536, 2048 and "
                       "4096 per axis; use NADIA_FP64 for other sizes");
-        choice = &choose(nx, ny, s.kind == NADIA_FRESNEL, 1);
+        if (wf) {
+            // the first tile shape of each length that has FresnelCDI_WF passes
+            for (const auto &v : variants(nx))
+                if (!wfc && v.wf_col) wfc = &v;
+            for (const auto &v : variants(ny))
+                if (!wfr && v.wf_row) wfr = &v;
+            NADIA_REQUIRE(wfc && wfr, NADIA_ERR_UNSUPPORTED, "no FresnelCDI_WF tile shape");
+            wfc->prepare();
+            wfr->prepare();
+        } else {
+            choice = &choose(nx, ny, s.kind == NADIA_FRESNEL, 1);
+        }
     }
     P.alloc(n);
     x.alloc(n);
     sup.alloc(n);
     mI.alloc(n);
-    ncol = poly ? 0 : ny / choice->col->L;
-    partials.alloc(ny / 2); // one per column tile (tiles of two columns at least)
+    // error partials: one per column tile (tiles of two columns at least), or
+    // for FresnelCDI_WF one per row tile
+    ncol = poly ? 0 : (wf ? nx / wfr->L : ny / choice->col->L);
+    partials.alloc(wf ? nx : ny / 2);
     iter.alloc(1);
     flag.alloc(1);
     slot.alloc(1);
@@ -770,6 +784,7 @@ bool Fused32::Impl::push_slot_async(cudaStream_t st)
     h_slot.project = h_slot.er || w[PF] != 0 || w[PSF] != 0;
     h_slot.pfs = pfs_mode() ? 1 : 0;
     h_slot.w_pfs = (float)w[PFS];
+    if (S.kind == NADIA_FRESNEL_WF) h_slot.project = 1; // its fixed iteration projects
     bool copied = false;
     if (h_slot.pfs && qslot) {
         // Q's column pass: the same reconstruction with Q as its work array
@@ -791,7 +806,10 @@ bool Fused32::Impl::push_slot_async(cudaStream_t st)
     return true;
 }
 
-bool Fused32::Impl::pfs_mode() const { return S.algorithm != NADIA_ER && S.w[PFS] != 0; }
+bool Fused32::Impl::pfs_mode() const
+{
+    return S.kind != NADIA_FRESNEL_WF && S.algorithm != NADIA_ER && S.w[PFS] != 0;
+}
 
 // algorithms with a PfPs term: Q (rows of Ps x), its error partials and the
 // descriptor of its column pass, allocated on first use; the row pass runs
@@ -977,6 +995,35 @@ void Fused32::set_fresnel_geometry(double factor)
     I.put_panel(h.data(), 2, I.ill.p, false);
 }
 
+// FresnelCDI_WF's coefficient (FresnelCDI_WF.c++:31-79): sin(phi) - i cos(phi)
+// = -i e^{i phi} with phi = (rho_x^2 + rho_y^2)(1/z12 + 1/z23) pi / lambda,
+// rho = scaling * (mid - k_) and k_ the reference's folded index; kept as
+// b(k) = e^{i phi(k)} / m per axis of length m (the constant -i and the
+// factor's 1/sqrt(N) with invert's 1/sqrt(N) are folded, see fused32_wf.cuh)
+void Fused32::set_wf_geometry()
+{
+    Impl &I = *impl;
+    Solver &S = I.S;
+    auto make = [&](int m, double scaling, DevBuf<float2> &buf) {
+        std::vector<float2> t(m);
+        const double mid = (m - 1) / 2.0;
+        for (int k = 0; k < m; ++k) {
+            const int k_ = (int)(mid - fabs(mid - k));
+            const double a = scaling * (mid - k_);
+            const double r2 = a * a;
+            const double ph = (r2 / S.z12 + r2 / S.z23) * (M_PI / S.wavelength);
+            t[k] = make_float2((float)(cos(ph) / m), (float)(sin(ph) / m));
+        }
+        buf.alloc(m);
+        upload_now(buf.p, t.data(), m * sizeof(float2));
+    };
+    make(I.nx, S.wavelength * S.z23 / (S.pixel * I.nx), I.tx);
+    make(I.ny, S.wavelength * S.z23 / (S.pixel * I.ny), I.ty);
+    I.h_slot.tx = I.tx.p;
+    I.h_slot.ty = I.ty.p;
+    I.push_slot();
+}
+
 void Fused32::scale_illumination(double f)
 {
     Impl &I = *impl;
@@ -1113,7 +1160,9 @@ void Fused32::Impl::check_algorithm() const
 void Fused32::Impl::prime(cudaStream_t st)
 {
     const Slot *const *sl = slot_ptr.p;
-    if (S.kind == NADIA_POLY) {
+    if (S.kind == NADIA_FRESNEL_WF) {
+        wfr->wf_row(kRowPrime, sl, 1, nx, ny, twy, st);
+    } else if (S.kind == NADIA_POLY) {
         prow->row(kRowPrime, sl, 1, nx / prow->L, st, twy);
     } else if (pfs_mode()) {
         pfs_choice->row->row(kRowPrimePfs, sl, 1, nx, ny, twy, st);
@@ -1123,6 +1172,16 @@ void Fused32::Impl::prime(cudaStream_t st)
     }
     g_launches += 1;
     p_valid = true;
+}
+
+// FresnelCDI_WF::iterate (FresnelCDI_WF.c++:122-182): the column pass, the row
+// pass, and the error metric of the row pass's modulus
+void Fused32::Impl::launch_iteration_wf(cudaStream_t st)
+{
+    const Slot *const *sl = slot_ptr.p;
+    wfc->wf_col(sl, 1, nx, ny, twx, st);
+    wfr->wf_row(kRowFull, sl, 1, nx, ny, twy, st);
+    k_wf_finish<256><<<1, 256, 0, st>>>(sl);
 }
 
 void Fused32::Impl::launch_iteration(cudaStream_t st)
@@ -1151,9 +1210,12 @@ void Fused32::iterate(int count)
         iterate_poly(count);
         return;
     }
+    const bool wf = I.S.kind == NADIA_FRESNEL_WF;
     I.check_algorithm();
     const bool pfs = I.pfs_mode();
-    if (pfs) {
+    if (wf) {
+        I.use_ncol(I.nx / I.wfr->L);
+    } else if (pfs) {
         I.prepare_pfs();
         I.use_choice(I.pfs_choice);
     } else {
@@ -1163,7 +1225,15 @@ void Fused32::iterate(int count)
     I.push_slot();
     cudaStream_t st = I.S.st;
     if (!I.p_valid || (pfs && !I.q_valid)) I.prime(st);
-    const int per_iter = pfs ? 3 : 2;
+    const int per_iter = (pfs || wf) ? 3 : 2;
+    auto one = [&] {
+        if (wf)
+            I.launch_iteration_wf(st);
+        else if (pfs)
+            I.launch_iteration_pfs(st);
+        else
+            I.launch_iteration(st);
+    };
     cudaGraphExec_t &exec = pfs ? I.graph_pfs : I.graph_exec;
     // replay a captured graph of kGraphIters iterations, then the remainder
     const int G = Impl::kGraphIters;
@@ -1172,7 +1242,7 @@ void Fused32::iterate(int count)
         if (!exec) {
             cudaGraph_t g = nullptr;
             NADIA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            for (int i = 0; i < G; ++i) pfs ? I.launch_iteration_pfs(st) : I.launch_iteration(st);
+            for (int i = 0; i < G; ++i) one();
             NADIA_CUDA(cudaStreamEndCapture(st, &g));
             NADIA_CUDA(cudaGraphInstantiate(&exec, g, 0));
             cudaGraphDestroy(g);
@@ -1184,7 +1254,7 @@ void Fused32::iterate(int count)
         }
     }
     for (; left > 0; --left) {
-        pfs ? I.launch_iteration_pfs(st) : I.launch_iteration(st);
+        one();
         g_launches += per_iter;
     }
     NADIA_CUDA(cudaGetLastError());

@@ -19,6 +19,8 @@ public:
     void set_spectrum();
     void upload_illumination();
     void set_fresnel_geometry(double factor);
+    // FresnelCDI_WF's zone-plate factors (FresnelCDI_WF.c++:31-79), per axis
+    void set_wf_geometry();
     void scale_illumination(double f);
     void fresnel_initialise(const double *t);
     void fresnel_set_transmission(const double *t);

@@ -134,6 +134,8 @@ using ColLaunch = void (*)(bool fresnel, const Slot *const *slots, int nslots, i
                            const float2 *tw, cudaStream_t st);
 using RowLaunch = void (*)(int mode, const Slot *const *slots, int nslots, int nx, int ny,
                            const float2 *tw, cudaStream_t st);
+using WfColLaunch = void (*)(const Slot *const *slots, int nslots, int nx, int ny,
+                             const float2 *tw, cudaStream_t st);
 
 // One compiled tile shape of a transform length, usable as column pass
 // (length nx) and as row pass (length ny); a variant that serves only one of
@@ -149,6 +151,9 @@ struct TileVariant {
     void (*prepare)() = nullptr;
     ColLaunch col = nullptr;
     RowLaunch row = nullptr;
+    // FresnelCDI_WF passes in this tile shape (plain variants only)
+    WfColLaunch wf_col = nullptr;
+    RowLaunch wf_row = nullptr;
 };
 
 // PolyCDI passes of one tile shape: forward column transform of the padded
@@ -238,6 +243,8 @@ struct Fused32::Impl {
     DevBuf<float> q, wl, ratio;
     DevBuf<int> gx, gy;
     const f32::PolyVariant *pcol = nullptr, *prow = nullptr;
+    // FresnelCDI_WF: the tile shapes of its column and row passes
+    const f32::TileVariant *wfc = nullptr, *wfr = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     // algorithms with a PfPs term (allocated on first use): Q, its error
     // partials, the descriptor of Q's column pass, and non-persistent row
@@ -276,6 +283,7 @@ struct Fused32::Impl {
     bool pfs_mode() const; // the algorithm has a PfPs term (not ER)
     void prepare_pfs();
     void launch_iteration_pfs(cudaStream_t st);
+    void launch_iteration_wf(cudaStream_t st);
 };
 
 } // namespace nadia

@@ -286,6 +286,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_row(const Slot *const *slots
 } // namespace nadia
 
 #include "fused32_persist.cuh"
+#include "fused32_wf.cuh"
 
 namespace nadia {
 namespace f32 {
@@ -314,6 +315,27 @@ void prepare_variant()
     set_smem<CR>(k_row<CR, kRowPrime>);
     set_smem<CR>(k_row<CR, kRowPfs>);
     set_smem<CR>(k_row<CR, kRowPrimePfs>);
+    set_smem<CC>(k_wf_col<CC>);
+    set_smem<CR>(k_wf_row<CR, kRowFull>);
+    set_smem<CR>(k_wf_row<CR, kRowPrime>);
+}
+
+template <class C>
+void launch_wf_col(const Slot *const *slots, int nslots, int nx, int ny, const float2 *tw,
+                   cudaStream_t st)
+{
+    k_wf_col<C><<<dim3(ny / C::L, nslots), C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
+}
+
+template <class C>
+void launch_wf_row(int mode, const Slot *const *slots, int nslots, int nx, int ny, const float2 *tw,
+                   cudaStream_t st)
+{
+    const dim3 grid(nx / C::L, nslots);
+    if (mode == kRowFull)
+        k_wf_row<C, kRowFull><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
+    else
+        k_wf_row<C, kRowPrime><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
 }
 
 template <class C>
@@ -450,6 +472,8 @@ TileVariant make_variant(const char *radices)
     t.prepare = &prepare_variant<CC, CR>;
     t.col = &launch_col<CC>;
     t.row = &launch_row<CR>;
+    t.wf_col = &launch_wf_col<CC>;
+    t.wf_row = &launch_wf_row<CR>;
     return t;
 }
 

@@ -84,8 +84,6 @@ Solver::Solver(int kind_, int nx_, int ny_, int prec_, int n_best_)
 {
     NADIA_REQUIRE(kind >= NADIA_PLANAR && kind <= NADIA_FRESNEL_WF, NADIA_ERR_INVALID,
                   "unknown kind");
-    NADIA_REQUIRE(kind != NADIA_FRESNEL_WF || prec == NADIA_FP64, NADIA_ERR_UNSUPPORTED,
-                  "FresnelCDI_WF runs in the FP64 form");
     NADIA_REQUIRE(prec == NADIA_FP64 || prec == NADIA_FP32, NADIA_ERR_INVALID,
                   "unknown precision");
     NADIA_REQUIRE(nx >= 2 && ny >= 2, NADIA_ERR_INVALID, "grid sizes must be at least 2");
@@ -465,6 +463,10 @@ void Solver::fresnel_wf_init(double wl, double zone_focal, double focal_detector
     z12 = zone_focal;
     z23 = focal_detector;
     pixel = pixel_;
+    if (prec == NADIA_FP32) {
+        f32->set_wf_geometry();
+        return;
+    }
     const int qy = ny / 2;
     const double x_mid = (nx - 1) / 2.0, y_mid = (ny - 1) / 2.0;
     const double scaling_x = wl * z23 / (pixel * nx);
@@ -501,7 +503,10 @@ void Solver::fresnel_wf_set_support(double z_diameter, double size)
             if (r < size * z_diameter / 2.0) h_support[(size_t)i * ny + j] = 1;
         }
     upload_support();
-    plain_convolve(support.p, 3, 5);
+    if (prec == NADIA_FP64)
+        plain_convolve(support.p, 3, 5);
+    else
+        f32->soften_support();
     h_support_valid = false;
 }
 

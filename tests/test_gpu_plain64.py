@@ -138,7 +138,7 @@ def test_transmission_constraint_refusals():
     assert e.value.code == 2
 
 
-def test_fresnel_wf_fixed_algorithm_and_fp64_only():
+def test_fresnel_wf_fixed_algorithm():
     f = sc.fresnel_wf_inputs(32)
     kw = dict(wavelength=f.wavelength, zone_focal_length=f.z12, focal_detector_length=f.z23,
               pixel_size=f.pixel)
@@ -147,7 +147,7 @@ def test_fresnel_wf_fixed_algorithm_and_fp64_only():
         with pytest.raises(pynadia.NadiaError) as e:
             call()
         assert e.value.code == 3
-    with pytest.raises(pynadia.NadiaError) as e:
+    with pytest.raises(pynadia.NadiaError) as e:  # no FP32 tiles for 32-point transforms
         pynadia.Solver("fresnel_wf", 32, 32, precision=pynadia.FP32, **kw)
     assert e.value.code == 3
 
