@@ -50,8 +50,10 @@ const PolyVariant *pick(int n, int tiles_of)
 // PolyCDI::set_spectrum (PolyCDI.c++:66-89) on the FP32 form: the padded
 // grid, the |Psi|^2 buffer and the gather tables of expand_wl
 // (PolyCDI.c++:296-334): for wavelength l and unpadded row i (padded row
-// i + px) the sampled row is (int)(lf*(i + px - nx/2) + nx/2) with
-// lf = lambda_l / lambda_c, or none when outside [0, mx); likewise columns.
+// i + px) the sampled row is ga = (int)(lf*(i + px - nx/2) + nx/2) with
+// lf = lambda_l / lambda_c, or none when outside [0, mx); likewise columns
+// (gb).  The tables hold the row and column parts of the sample's address
+// in q's panel layout (k_poly_expand).
 void Fused32::set_spectrum()
 {
     Impl &I = *impl;
@@ -88,11 +90,14 @@ void Fused32::set_spectrum()
         const double lf = S.spectrum[2 * l] / S.lambdac;
         for (int i = 0; i < S.nx; ++i) {
             const double xval = lf * ((i + S.px) - S.nx / 2.0) + S.nx / 2.0;
-            gx[(size_t)l * S.nx + i] = (xval >= 0 && xval < mx) ? (int)xval : -1;
+            gx[(size_t)l * S.nx + i] = (xval >= 0 && xval < mx) ? (int)xval * kPanel : kNoSample;
         }
         for (int j = 0; j < S.ny; ++j) {
             const double yval = lf * ((j + S.py) - S.ny / 2.0) + S.ny / 2.0;
-            gy[(size_t)l * S.ny + j] = (yval >= 0 && yval < my) ? (int)yval : -1;
+            const int gb = (int)yval;
+            gy[(size_t)l * S.ny + j] = (yval >= 0 && yval < my)
+                                           ? (gb / kPanel) * kPanel * mx + gb % kPanel
+                                           : kNoSample;
         }
         w[l] = (float)S.spectrum[2 * l + 1];
     }

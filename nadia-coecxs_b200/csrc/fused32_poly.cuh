@@ -66,11 +66,17 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_col_fwd(const Slot *con
 
 constexpr int kExpandThreads = 256;
 constexpr int kExpandBlocks = 1184; // 8 per SM
+constexpr int kNoSample = -(1 << 30); // offset of a sample outside the padded grid
 
 // One thread per pixel of the detector window in the panel layout (lanes
 // cover 4 columns x 8 rows, so the gathered q addresses of a warp are nearly
-// contiguous).  ratio = sqrt(I)/sqrt(I_calc) (0 when I_calc = 0) for measured
-// pixels, 1 elsewhere; partials[block] = sum of (sqrt(I) - sqrt(I_calc))^2.
+// contiguous).  S.gx[l][i] and S.gy[l][j] hold the parts of q's panel
+// address of the sample that wavelength l takes for row i and column j
+// (row part 4 ga, column part (gb/4) 4 mx + gb%4, kNoSample when outside the
+// grid), so a sample's address is their sum and it exists when that sum is
+// not negative.  ratio = sqrt(I)/sqrt(I_calc) (0 when I_calc = 0) for
+// measured pixels, 1 elsewhere; partials[block] = sum of (sqrt(I) -
+// sqrt(I_calc))^2.
 __global__ void __launch_bounds__(kExpandThreads) k_poly_expand(const Slot *const *slots)
 {
     const Slot &S = *slots[blockIdx.y];
@@ -96,19 +102,19 @@ __global__ void __launch_bounds__(kExpandThreads) k_poly_expand(const Slot *cons
             float acc = 0.f;
             int l = 0;
             for (; l + 4 <= nl; l += 4) {
-                float qv[4], w[4];
+                int off[4];
+                float qv[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int ga = __ldg(&gx[(l + u) * nx + i]), gb = __ldg(&gy[(l + u) * ny + j]);
-                    w[u] = (ga >= 0 && gb >= 0) ? __ldg(&wl[l + u]) : 0.f;
-                    qv[u] = (ga >= 0 && gb >= 0) ? __ldg(&q[paddr(ga, gb, mx)]) : 0.f;
-                }
+                for (int u = 0; u < 4; ++u)
+                    off[u] = __ldg(&gx[(l + u) * nx + i]) + __ldg(&gy[(l + u) * ny + j]);
 #pragma unroll
-                for (int u = 0; u < 4; ++u) acc += w[u] * qv[u];
+                for (int u = 0; u < 4; ++u) qv[u] = off[u] >= 0 ? __ldg(&q[off[u]]) : 0.f;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc += __ldg(&wl[l + u]) * qv[u];
             }
             for (; l < nl; ++l) {
-                const int ga = __ldg(&gx[l * nx + i]), gb = __ldg(&gy[l * ny + j]);
-                if (ga >= 0 && gb >= 0) acc += __ldg(&wl[l]) * __ldg(&q[paddr(ga, gb, mx)]);
+                const int o = __ldg(&gx[l * nx + i]) + __ldg(&gy[l * ny + j]);
+                acc += __ldg(&wl[l]) * (o >= 0 ? __ldg(&q[o]) : 0.f);
             }
             const float calc = sqrtf(acc);
             r = calc == 0.f ? 0.f : m / calc;

@@ -22,10 +22,11 @@ pytestmark = pytest.mark.gpu
 # below sqrt(I) (up to 1e5 times in the first iterations) that ratio
 # amplifies FP32 rounding by as much.  Each pixel's difference is therefore
 # divided by max(1, sqrt(I)/|c9|) (c9 from the FP64 form's single
-# operators) before it is compared with the largest value; without that the
-# first step differs by 3.4e-4 at the worst pixel, 1.6e-5 in the L2 norm.
+# operators) before it is compared with the largest value (and in the L2
+# norm); without that the first step at 256^2 differs by 3.4e-4 at the worst
+# pixel and 1.6e-5 in the L2 norm, with it by 1.8e-7.
 STEP_TOL = 2e-6
-L2_TOL = 5e-5
+L2_TOL = 2e-6
 ERR_TOL = 2e-5
 
 
@@ -35,7 +36,8 @@ def rel(a, b):
 
 def step(d, s, x0, isqrt, measured):
     """Both forms iterate once from x0; returns the amplification-normalised
-    and the L2 difference of the estimates."""
+    difference of the estimates, its largest value and its L2 norm, each
+    relative to the estimate's."""
     c9 = d.propagate_to_detector(d.apply_support(d.propagate_from_detector(x0)))
     for h in (d, s):
         h.set_exit_surface_wave(x0)
@@ -44,9 +46,8 @@ def step(d, s, x0, isqrt, measured):
     with np.errstate(divide="ignore"):
         amp = np.where(measured, isqrt / np.abs(c9), 1.0)
     amp = np.maximum(np.nan_to_num(amp, posinf=np.inf), 1.0)
-    norm = float((np.abs(xs - xd) / amp).max() / np.abs(xd).max())
-    l2 = float(np.linalg.norm(xs - xd) / np.linalg.norm(xd))
-    return norm, l2
+    dn = np.abs(xs - xd) / amp
+    return float(dn.max() / np.abs(xd).max()), float(np.linalg.norm(dn) / np.linalg.norm(xd))
 
 
 def make(prec, f, nx, ny=None):
