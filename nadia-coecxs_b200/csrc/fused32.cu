@@ -532,14 +532,15 @@ float time_launches(const std::function<void(cudaStream_t)> &f, cudaStream_t st,
 
 } // namespace
 
-const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
+const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows, bool wf)
 {
     static std::mutex mu;
     static std::map<TuneKey, Choice> cache;
     int dev = 0;
     NADIA_CUDA(cudaGetDevice(&dev));
     const int batch = nslots > 1 ? 4 : 1;
-    TuneKey key{dev, nx, ny, fresnel ? 1 : 0, batch, plain_rows ? 1 : 0};
+    const int kind = wf ? 2 : (fresnel ? 1 : 0);
+    TuneKey key{dev, nx, ny, kind, batch, plain_rows ? 1 : 0};
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
@@ -556,9 +557,11 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
     // pick the first variant whose tiles divide the grid (and tune among those)
     std::vector<const TileVariant *> cols, rows;
     for (const auto &v : cv)
-        if (v.col && ny % v.L == 0) cols.push_back(&v);
+        if ((wf ? v.wf_col != nullptr : v.col != nullptr) && ny % v.L == 0) cols.push_back(&v);
     for (const auto &v : rv)
-        if (v.row && nx % v.L == 0 && !(plain_rows && v.persistent)) rows.push_back(&v);
+        if ((wf ? v.wf_row != nullptr : v.row != nullptr) && nx % v.L == 0 &&
+            !(plain_rows && v.persistent))
+            rows.push_back(&v);
     NADIA_REQUIRE(!cols.empty() && !rows.empty(), NADIA_ERR_UNSUPPORTED,
                   "grid shape does not divide into the FP32 tiles");
     ch.col = cols[0];
@@ -568,9 +571,11 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
         if (FILE *f = fopen(tfile, "r")) {
             int a, b, c, d, ci, ri;
             while (fscanf(f, "%d %d %d %d %d %d", &a, &b, &c, &d, &ci, &ri) == 6)
-                if (a == nx && b == ny && c == (fresnel ? 1 : 0) && d == batch && ci >= 0 &&
-                    ci < (int)cv.size() && ri >= 0 && ri < (int)rv.size() && cv[ci].col &&
-                    rv[ri].row && ny % cv[ci].L == 0 && nx % rv[ri].L == 0) {
+                if (a == nx && b == ny && c == kind && d == batch && ci >= 0 &&
+                    ci < (int)cv.size() && ri >= 0 && ri < (int)rv.size() &&
+                    (wf ? cv[ci].wf_col != nullptr : cv[ci].col != nullptr) &&
+                    (wf ? rv[ri].wf_row != nullptr : rv[ri].row != nullptr) &&
+                    ny % cv[ci].L == 0 && nx % rv[ri].L == 0) {
                     ch.col = &cv[ci];
                     ch.row = &rv[ri];
                     fclose(f);
@@ -587,8 +592,9 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
         std::vector<DevBuf<float2>> P(ns), X(ns);
         std::vector<DevBuf<float>> sup(ns), mI(ns);
         DevBuf<float2> W(n), tx(nx), ty(ny);
-        int maxcol = 0;
+        int maxcol = 0; // error partials: one per column tile (per row tile for FresnelCDI_WF)
         for (auto *v : cols) maxcol = std::max(maxcol, ny / v->L);
+        for (auto *v : rows) maxcol = std::max(maxcol, nx / v->L);
         DevBuf<double> part((size_t)maxcol * ns), err(ns), ring(ns * 4);
         DevBuf<long long> iter(ns);
         DevBuf<int> flag(1);
@@ -607,7 +613,9 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
             Slot &s = hs[i];
             s = Slot{};
             s.P = P[i].p; s.x = X[i].p; s.sup = sup[i].p; s.mI = mI[i].p;
-            s.W = fresnel ? W.p : nullptr; s.tx = fresnel ? tx.p : nullptr; s.ty = fresnel ? ty.p : nullptr;
+            s.W = fresnel ? W.p : nullptr;
+            s.tx = (fresnel || wf) ? tx.p : nullptr; // FresnelCDI_WF: the zone-plate factors
+            s.ty = (fresnel || wf) ? ty.p : nullptr;
             s.partials = part.p + (size_t)i * maxcol; s.err = err.p + i; s.ring = ring.p + 4 * i;
             s.ring_len = 4; s.iter = iter.p + i; s.ncol = 1; s.w_id = 1; s.w_pf = -0.9f;
             s.w_ps = -1; s.w_psf = 1.9f; s.project = 1; s.s0 = 1.f; s.inv_norm2 = 1.0;
@@ -623,16 +631,20 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
         NADIA_CUDA(cudaStreamSynchronize(st));
         const float2 *twx = twiddle_table(nx), *twy = twiddle_table(ny);
         // bring the clocks up before timing anything
-        for (int i = 0; i < 20; ++i) cols[0]->col(fresnel, dptrs.p, ns, nx, ny, twx, st);
+        auto run_col = [&](const TileVariant *v, cudaStream_t s) {
+            if (wf)
+                v->wf_col(dptrs.p, ns, nx, ny, twx, s);
+            else
+                v->col(fresnel, dptrs.p, ns, nx, ny, twx, s);
+        };
+        for (int i = 0; i < 20; ++i) run_col(cols[0], st);
         NADIA_CUDA(cudaStreamSynchronize(st));
         float best = 1e30f;
         for (auto *v : cols) {
-            float us = time_launches([&](cudaStream_t s) {
-                v->col(fresnel, dptrs.p, ns, nx, ny, twx, s);
-            }, st, 5);
+            float us = time_launches([&](cudaStream_t s) { run_col(v, s); }, st, 5);
             if (verbose)
-                fprintf(stderr, "nadia tune: col n=%d NT=%d L=%d radices=%s%s batch=%d: %.2f us\n",
-                        nx, v->nt, v->L, v->radices,
+                fprintf(stderr, "nadia tune: %scol n=%d NT=%d L=%d radices=%s%s batch=%d: %.2f us\n",
+                        wf ? "FresnelCDI_WF " : "", nx, v->nt, v->L, v->radices,
                         v->single ? " persistent-1stage" : (v->persistent ? " persistent" : (v->ping ? " ping" : "")),
                         ns, us);
             if (us < best) { best = us; ch.col = v; ch.col_us = us; }
@@ -640,11 +652,14 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
         best = 1e30f;
         for (auto *v : rows) {
             float us = time_launches([&](cudaStream_t s) {
-                v->row(kRowFull, dptrs.p, ns, nx, ny, twy, s);
+                if (wf)
+                    v->wf_row(kRowFull, dptrs.p, ns, nx, ny, twy, s);
+                else
+                    v->row(kRowFull, dptrs.p, ns, nx, ny, twy, s);
             }, st, 5);
             if (verbose)
-                fprintf(stderr, "nadia tune: row n=%d NT=%d L=%d G=%d radices=%s%s batch=%d: %.2f us\n",
-                        ny, v->nt, v->L, v->groups, v->radices,
+                fprintf(stderr, "nadia tune: %srow n=%d NT=%d L=%d G=%d radices=%s%s batch=%d: %.2f us\n",
+                        wf ? "FresnelCDI_WF " : "", ny, v->nt, v->L, v->groups, v->radices,
                         v->persistent ? " persistent" : (v->ping ? " ping" : ""), ns, us);
             if (us < best) { best = us; ch.row = v; ch.row_us = us; }
         }
@@ -657,7 +672,7 @@ const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows)
     }
     if (tfile) {
         if (FILE *f = fopen(tfile, "a")) {
-            fprintf(f, "%d %d %d %d %d %d\n", nx, ny, fresnel ? 1 : 0, batch,
+            fprintf(f, "%d %d %d %d %d %d\n", nx, ny, kind, batch,
                     (int)(ch.col - cv.data()), (int)(ch.row - rv.data()));
             fclose(f);
         }
@@ -690,14 +705,9 @@ Fused32::Impl::Impl(Solver &s) : S(s)
                       "the FP32 form supports grid sizes 256, 512, 768, 1024, 1536, 2048 and "
                       "4096 per axis; use NADIA_FP64 for other sizes");
         if (wf) {
-            // the first tile shape of each length that has FresnelCDI_WF passes
-            for (const auto &v : variants(nx))
-                if (!wfc && v.wf_col) wfc = &v;
-            for (const auto &v : variants(ny))
-                if (!wfr && v.wf_row) wfr = &v;
-            NADIA_REQUIRE(wfc && wfr, NADIA_ERR_UNSUPPORTED, "no FresnelCDI_WF tile shape");
-            wfc->prepare();
-            wfr->prepare();
+            const Choice &c = choose(nx, ny, false, 1, false, true);
+            wfc = c.col;
+            wfr = c.row;
         } else {
             choice = &choose(nx, ny, s.kind == NADIA_FRESNEL, 1);
         }

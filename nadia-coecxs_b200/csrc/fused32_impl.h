@@ -185,7 +185,10 @@ struct Choice {
 };
 // plain_rows: only row variants that are not persistent (the ones that
 // carry the transmission constraint)
-const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows = false);
+// wf: the FresnelCDI_WF passes of the plain variants (the tune file marks
+// those choices with 2 in its kind column)
+const Choice &choose(int nx, int ny, bool fresnel, int nslots, bool plain_rows = false,
+                     bool wf = false);
 
 // Mixed-length persistent passes (fused32_mixed.cu): one launch per pass over
 // a work list of items (reconstruction index into the slot list, its column

@@ -89,6 +89,24 @@ __device__ __forceinline__ double block_sum(double v)
     return t;
 }
 
+// FP64 block sum in the order of the persistent column pass (warp sums by
+// shuffles, then warp 0's ... warp NT/32-1's added in turn); result valid in
+// thread 0
+template <int NT>
+__device__ __forceinline__ double block_sum_seq(double v)
+{
+    __shared__ double red[NT / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int w = 0; w < NT / 32; ++w) t += red[w];
+    return t;
+}
+
 // -------------------------------------------------------------- column pass
 
 template <class C, bool FRESNEL>

@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(F::NT, 1)
                 }
                 v[e] = X;
             });
-            const double tot = block_sum<C::NT>(diff);
+            const double tot = block_sum_seq<C::NT>(diff); // the order of kp_col
             if (threadIdx.x == 0) S.partials[m.tile] = tot;
             transform<C, false>(v, Pb, tw);
             for_each_slot<C, false, false>([&](int e, int s, int pos) { Pb[raw_col<C>(s, pos)] = v[e]; });

@@ -76,6 +76,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     constexpr bool MDIRECT = MMODE == 1;
     constexpr bool MSTAGE = MMODE == 2;
     extern __shared__ __align__(1024) unsigned char smraw[];
+    __shared__ double wsum[C::NT / 32];
     constexpr int TW = C::N * C::L;
     float2 *Pb0 = reinterpret_cast<float2 *>(smraw);
     float2 *Pb1 = Pb0 + TW * (STAGES - 1);
@@ -187,13 +188,21 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             }
             v[e] = X;
         });
-        const double tot = block_sum<C::NT>(diff); // every thread has read sqrt(I)
-        if (threadIdx.x == 0) {
-            S.partials[t % tps] = tot;
-            if (MSTAGE && tn < ntiles) {
-                tma::fence_async_shared();
-                issue_m(tn);
+        if (MSTAGE) {
+            const double tot = block_sum<C::NT>(diff); // every thread has read sqrt(I)
+            if (threadIdx.x == 0) {
+                S.partials[t % tps] = tot;
+                if (tn < ntiles) {
+                    tma::fence_async_shared();
+                    issue_m(tn);
+                }
             }
+        } else {
+            // warp sums now; thread 0 adds them up after the barrier that
+            // precedes the tile's store (no barrier of its own)
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) diff += __shfl_down_sync(0xffffffffu, diff, off);
+            if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = diff;
         }
 
         transform_h<C, false>(v, Pb, Xb, tw, [] {});
@@ -203,6 +212,14 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         if (threadIdx.x == 0) {
             tma::bulk_store(S.P + (size_t)(t % tps) * C::L * nx, Pb, TW * 8);
             tma::bulk_commit();
+            if (!MSTAGE) {
+                // the warps' sums in a fixed order; the next tile's writes
+                // come after its first barrier, which thread 0 reaches later
+                double tot = 0.0;
+#pragma unroll
+                for (int w = 0; w < C::NT / 32; ++w) tot += wsum[w];
+                S.partials[t % tps] = tot;
+            }
         }
     }
     if (threadIdx.x == 0) tma::bulk_wait_all();
