@@ -139,6 +139,12 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             }
         }
         const bool ok = tma::mbar_wait(&bar[b], par, polls);
+        float2 v[C::E];
+        float m[C::E];
+        // (where the wait gave up these are stale values; the tile is dropped)
+        for_each_slot<C, true, true>([&](int e, int s, int pos) { v[e] = Pb[raw_col<C>(s, pos)]; });
+        // one barrier: the stage has been read (the first exchange writes it)
+        // and every thread knows whether the wait gave up
         if (__syncthreads_or(!ok)) {
             // every copy issued so far lands before the CTA leaves
             if (threadIdx.x == 0) {
@@ -150,10 +156,6 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             }
             break;
         }
-        float2 v[C::E];
-        float m[C::E];
-        for_each_slot<C, true, true>([&](int e, int s, int pos) { v[e] = Pb[raw_col<C>(s, pos)]; });
-        __syncthreads();
         const float *mg = S.mI + (size_t)(t % tps) * C::L * nx;
         transform_h<C, true>(v, Pb, Xb, tw, [&] {
             if (MDIRECT)
@@ -301,7 +303,12 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             issue_xs(t);
             if (tn < ntiles) issue_p(tn, b ^ 1, false);
         }
-        bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
+        const bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
+        float2 v[C::E];
+        // (where the wait gave up these are stale values; the tile is dropped)
+        for_each_slot<C, false, true>([&](int e, int s, int pos) { v[e] = Pb[raw_row<C>(s, pos)]; });
+        // one barrier: the stage has been read (the first exchange writes it)
+        // and every thread knows whether the wait gave up
         if (__syncthreads_or(!ok)) {
             // every copy issued so far lands before the CTA leaves
             if (threadIdx.x == 0) {
@@ -312,20 +319,11 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             }
             break;
         }
-        float2 v[C::E];
-        for_each_slot<C, false, true>([&](int e, int s, int pos) { v[e] = Pb[raw_row<C>(s, pos)]; });
-        __syncthreads();
         transform<C, false>(v, Pb, tw);
 
-        ok = tma::mbar_wait(&bar[2], it & 1, polls);
-        if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) {
-                raise_flag(S);
-                tma::mbar_wait(&bar[2], it & 1, polls);
-                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
-            }
-            break;
-        }
+        // x and the support; a wait that gave up is acted on at the barrier
+        // before the store (the tile's values are dropped there)
+        const bool okx = tma::mbar_wait(&bar[2], it & 1, polls);
         const float wid = S.w_id, wpf = S.w_pf, wps = S.w_ps, wpsf = S.w_psf;
         const bool er = S.er;
         for_each_slot<C, false, false>([&](int e, int s, int pos) {
@@ -345,7 +343,14 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         transform<C, true>(v, Pb, tw);
         for_each_slot<C, true, false>([&](int e, int s, int pos) { Pb[raw_row<C>(s, pos)] = v[e]; });
         tma::fence_async_shared();
-        __syncthreads();
+        if (__syncthreads_or(!okx)) {
+            if (threadIdx.x == 0) {
+                raise_flag(S);
+                tma::mbar_wait(&bar[2], it & 1, polls);
+                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+            }
+            break;
+        }
         if (threadIdx.x == 0) {
             for (int c = 0; c < npan; c += boxp) {
                 tma::tensor_store_3d(&S.tm[TM][0], 0, i0, c, Pb + (size_t)c * C::L * kPanel);
@@ -457,7 +462,12 @@ __global__ void __launch_bounds__(C::NT * C::GROUPS, 1)
             issue_xs(t);
             if (tn < ntiles) issue_p(tn, b ^ 1, false);
         }
-        bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
+        const bool ok = tma::mbar_wait(&bar[b], (it >> 1) & 1, polls);
+        float2 v[C::E];
+        // (where the wait gave up these are stale values; the tile is dropped)
+        for_each_slot<C, false, true>([&](int e, int s, int pos) { v[e] = Pb[raw_row<C>(s, pos)]; });
+        // one group barrier: the stage has been read (the first exchange
+        // writes it) and the group knows whether the wait gave up
         if (group_or<C>(!ok)) {
             // every copy issued so far lands before the group leaves
             if (u == 0) {
@@ -468,20 +478,11 @@ __global__ void __launch_bounds__(C::NT * C::GROUPS, 1)
             }
             break;
         }
-        float2 v[C::E];
-        for_each_slot<C, false, true>([&](int e, int s, int pos) { v[e] = Pb[raw_row<C>(s, pos)]; });
-        C::sync();
         transform<C, false>(v, Pb, tw);
 
-        ok = tma::mbar_wait(&bar[2], it & 1, polls);
-        if (group_or<C>(!ok)) {
-            if (u == 0) {
-                raise_flag(S);
-                tma::mbar_wait(&bar[2], it & 1, polls);
-                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
-            }
-            break;
-        }
+        // x and the support; a wait that gave up is acted on at the barrier
+        // before the store (the tile's values are dropped there)
+        const bool okx = tma::mbar_wait(&bar[2], it & 1, polls);
         const float wid = S.w_id, wpf = S.w_pf, wps = S.w_ps, wpsf = S.w_psf;
         const bool er = S.er;
         for_each_slot<C, false, false>([&](int e, int s, int pos) {
@@ -501,7 +502,14 @@ __global__ void __launch_bounds__(C::NT * C::GROUPS, 1)
         transform<C, true>(v, Pb, tw);
         for_each_slot<C, true, false>([&](int e, int s, int pos) { Pb[raw_row<C>(s, pos)] = v[e]; });
         tma::fence_async_shared();
-        C::sync();
+        if (group_or<C>(!okx)) {
+            if (u == 0) {
+                raise_flag(S);
+                tma::mbar_wait(&bar[2], it & 1, polls);
+                if (tn < ntiles) tma::mbar_wait(&bar[b ^ 1], ((it + 1) >> 1) & 1, polls);
+            }
+            break;
+        }
         if (u == 0) {
             for (int c = 0; c < npan; c += boxp) {
                 tma::tensor_store_3d(&S.tm[TM][0], 0, i0, c, Pb + (size_t)c * C::L * kPanel);
