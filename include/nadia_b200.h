@@ -88,8 +88,9 @@ int nadia_poly_create(int nx, int ny, int precision, double beta, int n_best,
  * focal_detector_length, pixel_size, n_best) -- NADIA/src/FresnelCDI_WF.c++:17-79:
  * recovery of the white field (the detector-plane illumination that
  * FresnelCDI consumes) from a white-field measurement; the estimate is the
- * detector-plane field.  FP64 form only (NADIA_FP32 returns
- * NADIA_ERR_UNSUPPORTED).  Its algorithm is fixed (FresnelCDI_WF.c++:155-162):
+ * detector-plane field.  Both forms; NADIA_FP32 on grids of 256 ... 4096 per
+ * axis (one column and one row pass per iteration; NADIA_ERR_UNSUPPORTED on
+ * other sizes).  Its algorithm is fixed (FresnelCDI_WF.c++:155-162):
  * set_algorithm, set_custom_algorithm and set_relaxation_parameter return
  * NADIA_ERR_UNSUPPORTED, where the reference prints a warning. */
 int nadia_fresnel_wf_create(int nx, int ny, int precision, double beam_wavelength,
