@@ -70,13 +70,13 @@ constexpr int kNoSample = -(1 << 30); // offset of a sample outside the padded g
 
 // One thread per pixel of the detector window in the panel layout (lanes
 // cover 4 columns x 8 rows, so the gathered q addresses of a warp are nearly
-// contiguous).  S.gx[l][i] and S.gy[l][j] hold the parts of q's panel
-// address of the sample that wavelength l takes for row i and column j
-// (row part 4 ga, column part (gb/4) 4 mx + gb%4, kNoSample when outside the
-// grid), so a sample's address is their sum and it exists when that sum is
-// not negative.  ratio = sqrt(I)/sqrt(I_calc) (0 when I_calc = 0) for
-// measured pixels, 1 elsewhere; partials[block] = sum of (sqrt(I) -
-// sqrt(I_calc))^2.
+// contiguous; 32-bit index arithmetic, one division per pixel).  S.gx[l][i]
+// and S.gy[l][j] hold the parts of q's panel address of the sample that
+// wavelength l takes for row i and column j (row part 4 ga, column part
+// (gb/4) 4 mx + gb%4, kNoSample when outside the grid), so a sample's address
+// is their sum and it exists when that sum is not negative.
+// ratio = sqrt(I)/sqrt(I_calc) (0 when I_calc = 0) for measured pixels, 1
+// elsewhere; partials[block] = sum of (sqrt(I) - sqrt(I_calc))^2.
 __global__ void __launch_bounds__(kExpandThreads) k_poly_expand(const Slot *const *slots)
 {
     const Slot &S = *slots[blockIdx.y];
@@ -89,16 +89,17 @@ __global__ void __launch_bounds__(kExpandThreads) k_poly_expand(const Slot *cons
     const int *__restrict__ gy = S.gy;
     const float *__restrict__ wl = S.wl;
     float *__restrict__ ratio = S.ratio;
-    const size_t n = (size_t)nx * ny;
+    const unsigned n = (unsigned)nx * (unsigned)ny;
     double diff = 0.0;
-    for (size_t a = blockIdx.x * (size_t)kExpandThreads + threadIdx.x; a < n;
-         a += (size_t)gridDim.x * kExpandThreads) {
-        const size_t t = a / kPanel;
-        const int i = (int)(t % nx), j = (int)(t / nx) * kPanel + (int)(a % kPanel);
+    for (unsigned a = blockIdx.x * kExpandThreads + threadIdx.x; a < n;
+         a += gridDim.x * kExpandThreads) {
+        const unsigned t = a / kPanel, jp = t / (unsigned)nx;
+        const int i = (int)(t - jp * (unsigned)nx), j = (int)(jp * kPanel + a % kPanel);
         const float m = __ldg(&mI[a]);
         float r = 1.f;
         if (!(m < 0.f)) {
-            // groups of four wavelengths: their loads issue together
+            // groups of four wavelengths: their loads issue together (a whole
+            // spectrum's loads at once measured slower)
             float acc = 0.f;
             int l = 0;
             for (; l + 4 <= nl; l += 4) {

@@ -12,6 +12,7 @@ continuous batching, and results that are the same alone and in the mix.
   metrics before the first shrinkwrap stay within 1e-4 of the oracle's.
 * Errors: invalid requests are refused at submit, a request that fails on
   the device side fails alone, and destroying a busy server ends cleanly."""
+import gc
 import time
 
 import numpy as np
@@ -55,6 +56,9 @@ def run_alone(request):
                                          ("poly", pynadia.FP64, 96),
                                          ("poly", pynadia.FP32, 240)])
 def test_admission_charge_covers_device_bytes(kind, prec, n):
+    # handles of earlier tests that are still unreferenced release their
+    # buffers when collected; collect them before the count is taken
+    gc.collect()
     before = pynadia.device_bytes()
     kw = {}
     if kind == "fresnel":
