@@ -785,6 +785,7 @@ void Fused32::Impl::push_slot()
 // stop the host from queueing further iterations while the device runs.
 bool Fused32::Impl::push_slot_async(cudaStream_t st)
 {
+    flush_intensity();
     const double *w = S.w;
     h_slot.er = (S.algorithm == NADIA_ER);
     h_slot.w_id = (float)(1 + w[PI]);
@@ -847,9 +848,12 @@ void Fused32::Impl::prepare_pfs()
 // device arrays in the panel layout.  The host converts, so uploads and
 // readbacks are plain copies: they run on the copy engines and never wait
 // for SMs held by other reconstructions' passes.
-void Fused32::Impl::put_panel_f(const float *h, int stride, void *dst, bool fold)
+namespace {
+// host array (x*ny + y order, stride values per element, of type T) to the
+// panel layout in FP32, converted in the same pass
+template <class T>
+void to_panel(const T *h, int stride, float *p, int nx, int ny, bool fold)
 {
-    std::vector<float> p(n * stride);
     // x outer, y inner: the source is read in order, and the panel rows a
     // column writes (16 bytes each) are the next column's neighbours
     for (int kx = 0; kx < nx; ++kx) {
@@ -858,7 +862,7 @@ void Fused32::Impl::put_panel_f(const float *h, int stride, void *dst, bool fold
             dx = kx + nx / 2;
             dx = dx >= nx ? dx - nx : dx;
         }
-        const float *src = h + (size_t)dx * ny * stride;
+        const T *src = h + (size_t)dx * ny * stride;
         for (int ky = 0; ky < ny; ++ky) {
             int dy = ky;
             if (fold) {
@@ -866,9 +870,16 @@ void Fused32::Impl::put_panel_f(const float *h, int stride, void *dst, bool fold
                 dy = dy >= ny ? dy - ny : dy;
             }
             const size_t a = panel_index_dev(kx, ky, nx);
-            for (int c = 0; c < stride; ++c) p[a * stride + c] = src[(size_t)dy * stride + c];
+            for (int c = 0; c < stride; ++c) p[a * stride + c] = (float)src[(size_t)dy * stride + c];
         }
     }
+}
+} // namespace
+
+void Fused32::Impl::put_panel_f(const float *h, int stride, void *dst, bool fold)
+{
+    std::vector<float> p(n * stride);
+    to_panel(h, stride, p.data(), nx, ny, fold);
     NADIA_CUDA(cudaMemcpyAsync(dst, p.data(), n * stride * sizeof(float), cudaMemcpyHostToDevice,
                                S.st));
     NADIA_CUDA(cudaStreamSynchronize(S.st));
@@ -876,9 +887,11 @@ void Fused32::Impl::put_panel_f(const float *h, int stride, void *dst, bool fold
 
 void Fused32::Impl::put_panel(const double *h, int stride, void *dst, bool fold)
 {
-    std::vector<float> f(n * stride);
-    for (size_t k = 0; k < f.size(); ++k) f[k] = (float)h[k];
-    put_panel_f(f.data(), stride, dst, fold);
+    std::vector<float> p(n * stride);
+    to_panel(h, stride, p.data(), nx, ny, fold);
+    NADIA_CUDA(cudaMemcpyAsync(dst, p.data(), n * stride * sizeof(float), cudaMemcpyHostToDevice,
+                               S.st));
+    NADIA_CUDA(cudaStreamSynchronize(S.st));
 }
 
 void Fused32::Impl::get_panel_f(const void *src, int stride, float *h)
@@ -901,10 +914,17 @@ void Fused32::Impl::get_panel(const void *src, int stride, double *h)
     for (size_t k = 0; k < f.size(); ++k) h[k] = f[k];
 }
 
+// set_intensity and set_beam_stop mark sqrt(I) for conversion; it is formed
+// once, when the reconstruction's estimate is set or before its descriptor
+// goes to the device (every launch path pushes the descriptor first)
+void Fused32::Impl::upload_intensity() { mI_dirty = true; }
+
 // sqrt(I) in transform order with the unmeasured pixels marked -1; the
 // normalisation sum of BaseCDI::scale_intensity over the measured pixels
-void Fused32::Impl::upload_intensity()
+void Fused32::Impl::flush_intensity()
 {
+    if (!mI_dirty) return;
+    mI_dirty = false;
     std::vector<float> m(n);
     double norm2 = 0;
     for (size_t d = 0; d < n; ++d) {
@@ -1128,6 +1148,7 @@ void Fused32::set_x(const double *h)
 {
     impl->put_panel(h, 2, impl->x.p, false);
     impl->p_valid = false;
+    impl->flush_intensity();
 }
 
 void Fused32::get_x(double *h) { impl->get_panel(impl->x.p, 2, h); }
@@ -1136,6 +1157,7 @@ void Fused32::set_x_f32(const float *h)
 {
     impl->put_panel_f(h, 2, impl->x.p, false);
     impl->p_valid = false;
+    impl->flush_intensity();
 }
 
 void Fused32::get_x_f32(float *h) { impl->get_panel_f(impl->x.p, 2, h); }

@@ -277,7 +277,9 @@ struct Fused32::Impl {
     void put_panel_f(const float *h, int stride, void *dst, bool fold);
     void get_panel(const void *src, int stride, double *h);
     void get_panel_f(const void *src, int stride, float *h);
-    void upload_intensity();
+    void upload_intensity(); // marks sqrt(I) for conversion (flush_intensity)
+    void flush_intensity();
+    bool mI_dirty = false;
     void blur(bool cplx, const void *in, double gauss_width, int cut);
     int blur_blocks() const;
     void check_algorithm() const;
