@@ -645,7 +645,8 @@ def constraint_report(pynadia, synth, n=2048, iters=50, modes=("none", "pixel", 
     """TransmissionConstraint (charge flipping, unit magnitude, and three
     complex-constraint regions) on a PlanarCDI HIO reconstruction of 2048^2 in
     the FP64 form (without, with the per-pixel part, with regions) and the
-    FP32 form (without, with the per-pixel part inside its fused row pass):
+    FP32 form (without, with the per-pixel part inside its fused row pass,
+    with regions around its split row pass):
     device time per iteration, CUDA events on the handle's stream.  The
     constraint runs in each support projection, twice per HIO iteration.
     The reference's float build is timed for one iteration of each on one
@@ -680,9 +681,10 @@ def constraint_report(pynadia, synth, n=2048, iters=50, modes=("none", "pixel", 
         ms[mode] = a.elapsed_time(b) / iters
         s.close()
     out["gpu_fp64_ms_per_iteration"] = ms
-    # the per-pixel part inside the FP32 fused row pass
+    # the per-pixel part inside the FP32 fused row pass; regions in its row
+    # pass split around the region sums
     ms32 = {}
-    for mode in ("none", "pixel"):
+    for mode in ("none", "pixel", "regions"):
         if mode not in modes:
             continue
         s = pynadia.Solver("planar", n, n, precision=pynadia.FP32)

@@ -15,10 +15,10 @@
 //     print_algorithm are virtual, so FresnelCDI_WF's versions (a warning:
 //     its algorithm is fixed) answer calls through a BaseCDI pointer too;
 //   - a TransmissionConstraint's per-pixel part (charge flipping, unit
-//     magnitude) runs inside the FP32 form's fused passes; complex-constraint
-//     regions and custom functions run in the FP64 form, to which an FP32
-//     reconstruction moves when it gets them (as does an FP32 PolyCDI given
-//     any constraint).  The constraint is read when iterate() or
+//     magnitude) runs inside the FP32 form's fused passes, its
+//     complex-constraint regions in the FP32 form's split row pass; custom
+//     functions run in the FP64 form, to which an FP32 reconstruction moves
+//     when it gets one (as does an FP32 PolyCDI given any constraint).  The constraint is read when iterate() or
 //     apply_support() next runs (changes to it after that are picked up at
 //     the following call).
 #ifndef NADIA_DROPIN_BASECDI_H

@@ -1,7 +1,7 @@
 // TransmissionConstraint.h -- drop-in for the reference's ComplexConstraint and
 // TransmissionConstraint (NADIA/include/TransmissionConstraint.h): the
 // constraint object a caller builds and hands to set_complex_constraint.  The
-// reconstruction applies it on the GPU (FP64 form) after every support
+// reconstruction applies it on the GPU (FP32 or FP64 form) after every support
 // projection; apply_constraint here is the same operation on the host for
 // callers that apply it to a field of their own.
 #ifndef NADIA_DROPIN_TRANSMISSIONCONSTRAINT_H
@@ -152,9 +152,9 @@ public:
             alpha[2 * r + 1] = c->get_alpha2();
             fixed[r] = c->is_c_fixed() ? c->get_c_mean() : NAN;
         }
-        // regions and custom functions run in the FP64 form (the per-pixel
-        // part also runs inside the FP32 form's fused passes)
-        if (R > 0 || custom_constraint) nadia_cxx::check(nadia_convert_to_fp64(h));
+        // custom functions run in the FP64 form (the per-pixel part and the
+        // regions also run in the FP32 form)
+        if (custom_constraint) nadia_cxx::check(nadia_convert_to_fp64(h));
         int rc = nadia_set_transmission_constraint(
             h, do_enforce_unity, do_charge_flip, flip_sign, R, R ? regions.data() : nullptr,
             R ? alpha.data() : nullptr, R ? fixed.data() : nullptr);

@@ -285,6 +285,80 @@ __global__ void k_fresnel_set_t(const float2 *t, const float2 *ill, float2 *esw,
 
 // the constraint's per-pixel part over a whole panel-layout array (the
 // transmission function FresnelCDI::get_transmission_function returns)
+// per block and region: the sums of |ln|t|| and |arg t| over the region's
+// pixels (FP64, each thread in pixel order, then the block's fixed tree);
+// the region map streams as int4 (four pixels of a panel row)
+__global__ void __launch_bounds__(kTcThreads) k_tc32_sums(const Slot *slot, int field,
+                                                          const float2 *arr, size_t n)
+{
+    const Slot &S = *slot;
+    const int R = S.tc_R;
+    double lnA[kTcMaxRegions], ph[kTcMaxRegions];
+#pragma unroll
+    for (int r = 0; r < kTcMaxRegions; ++r) lnA[r] = ph[r] = 0.0;
+    const int4 *reg4 = reinterpret_cast<const int4 *>(S.tc_region);
+    for (size_t q = blockIdx.x * (size_t)kTcThreads + threadIdx.x; q < n / 4;
+         q += (size_t)gridDim.x * kTcThreads) {
+        const int4 rr = __ldg(&reg4[q]);
+        const int rv[4] = {rr.x, rr.y, rr.z, rr.w};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int r = rv[c];
+            if (r > 0) {
+                const float2 t = tc_field(S, 4 * q + c, field, arr);
+#pragma unroll
+                for (int k = 0; k < kTcMaxRegions; ++k)
+                    if (k == r - 1) {
+                        ph[k] += fabs((double)atan2f(t.y, t.x));
+                        lnA[k] += fabs((double)logf(sqrtf(t.x * t.x + t.y * t.y)));
+                    }
+            }
+        }
+    }
+    for (int r = 0; r < R; ++r) {
+        const double a = block_sum<kTcThreads>(lnA[r]);
+        __syncthreads();
+        const double b = block_sum<kTcThreads>(ph[r]);
+        if (threadIdx.x == 0) {
+            S.tc_part[2 * ((size_t)blockIdx.x * R + r)] = a;
+            S.tc_part[2 * ((size_t)blockIdx.x * R + r) + 1] = b;
+        }
+        __syncthreads();
+    }
+}
+
+// one block per region: the blocks' partials in a fixed order, then c_mean
+// (the region's fixed value where one was set)
+__global__ void __launch_bounds__(kTcThreads) k_tc32_cmean(const Slot *slot, int field, int nblocks)
+{
+    const Slot &S = *slot;
+    const int R = S.tc_R, r = blockIdx.x;
+    double a = 0.0, b = 0.0;
+    for (int blk = threadIdx.x; blk < nblocks; blk += kTcThreads) {
+        a += S.tc_part[2 * ((size_t)blk * R + r)];
+        b += S.tc_part[2 * ((size_t)blk * R + r) + 1];
+    }
+    a = block_sum<kTcThreads>(a);
+    __syncthreads();
+    b = block_sum<kTcThreads>(b);
+    if (threadIdx.x == 0)
+        S.tc_cm[field * R + r] = S.tc_par[4 * r + 2] != 0.f ? S.tc_par[4 * r + 3] : (float)(a / b);
+}
+
+// the whole constraint on an array of transmission functions (or estimates)
+// whose c_mean is field 2's (get_transmission_function, FresnelCDI.c++:352-353)
+__global__ void k_tc32_apply_array(float2 *t, size_t n, const Slot *slot)
+{
+    const Slot &S = *slot;
+    for (size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x; a < n;
+         a += (size_t)gridDim.x * blockDim.x) {
+        float2 v = t[a];
+        const int r = S.tc_R > 0 ? S.tc_region[a] : 0;
+        if (r > 0) v = tc_region_update(v, S.tc_par + 4 * (r - 1), S.tc_cm[2 * S.tc_R + r - 1]);
+        t[a] = tc_pixel(v, S);
+    }
+}
+
 __global__ void k_tc_pixels(float2 *t, size_t n, const Slot *slot)
 {
     const Slot &S = *slot;
@@ -1080,11 +1154,38 @@ void Fused32::fresnel_set_transmission(const double *t)
     I.S.sync();
 }
 
-void Fused32::set_constraint(bool on, bool unity, bool flip, int flip_sign)
+void Fused32::set_constraint(bool on, bool unity, bool flip, int flip_sign, int nregions,
+                             const int *map, const double *prm)
 {
     Impl &I = *impl;
     NADIA_REQUIRE(!on || I.S.kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
                   "a transmission constraint on PolyCDI runs in the FP64 form");
+    NADIA_REQUIRE(nregions >= 0 && nregions <= kTcMaxRegions && (nregions == 0 || (map && prm)),
+                  NADIA_ERR_INVALID, "between 0 and 16 complex-constraint regions");
+    NADIA_CUDA(cudaStreamSynchronize(I.S.st)); // buffers of an earlier constraint may be replaced
+    const int R = on ? nregions : 0;
+    if (R > 0) {
+        // the region map in the panel layout, the parameters as floats
+        std::vector<int> pm(I.n);
+        for (int kx = 0; kx < I.nx; ++kx)
+            for (int ky = 0; ky < I.ny; ++ky)
+                pm[panel_index_dev(kx, ky, I.nx)] = map[(size_t)kx * I.ny + ky];
+        std::vector<float> pf(4 * (size_t)R);
+        for (size_t k = 0; k < pf.size(); ++k) pf[k] = (float)prm[k];
+        I.tc_region.alloc(I.n);
+        I.tc_par.alloc(pf.size());
+        I.tc_cm.alloc(3 * (size_t)R);
+        I.tc_part.alloc(2 * (size_t)kTcBlocks * R);
+        if (!I.Y) I.Y.alloc(I.n);
+        upload_now(I.tc_region.p, pm.data(), I.n * sizeof(int));
+        upload_now(I.tc_par.p, pf.data(), pf.size() * sizeof(float));
+    }
+    I.h_slot.tc_R = R;
+    I.h_slot.tc_region = R > 0 ? I.tc_region.p : nullptr;
+    I.h_slot.tc_par = R > 0 ? I.tc_par.p : nullptr;
+    I.h_slot.tc_cm = R > 0 ? I.tc_cm.p : nullptr;
+    I.h_slot.tc_part = R > 0 ? I.tc_part.p : nullptr;
+    I.h_slot.Y = R > 0 ? I.Y.p : nullptr;
     I.h_slot.tc_on = on ? 1 : 0;
     I.h_slot.tc_unity = on && unity ? 1 : 0;
     I.h_slot.tc_flip = on && flip ? 1 : 0;
@@ -1104,6 +1205,20 @@ void Fused32::set_constraint(bool on, bool unity, bool flip, int flip_sign)
 
 bool Fused32::constrained() const { return impl->h_slot.tc_on != 0; }
 
+// TransmissionConstraint::apply_constraint on a whole array (FresnelCDI's
+// transmission function when it is read, FresnelCDI.c++:352-353): region
+// sums and c_mean as field 2, then the update of every pixel
+void Fused32::Impl::constrain_array(float2 *t)
+{
+    if (h_slot.tc_R > 0) {
+        k_tc32_sums<<<kTcBlocks, kTcThreads, 0, S.st>>>(slot.p, 2, t, n);
+        k_tc32_cmean<<<h_slot.tc_R, kTcThreads, 0, S.st>>>(slot.p, 2, kTcBlocks);
+        k_tc32_apply_array<<<grid1(n), 256, 0, S.st>>>(t, n, slot.p);
+    } else {
+        k_tc_pixels<<<grid1(n), 256, 0, S.st>>>(t, n, slot.p);
+    }
+}
+
 void Fused32::transmission_to_device(double2 *dst)
 {
     Impl &I = *impl;
@@ -1112,7 +1227,7 @@ void Fused32::transmission_to_device(double2 *dst)
         I.p_valid = false; // T is formed in the work array
         I.push_slot();
         k_fresnel_get_t<<<grid1(I.n), 256, 0, I.S.st>>>(I.x.p, I.ill.p, I.P.p, I.n);
-        if (I.h_slot.tc_on) k_tc_pixels<<<grid1(I.n), 256, 0, I.S.st>>>(I.P.p, I.n, I.slot.p);
+        if (I.h_slot.tc_on) I.constrain_array(I.P.p);
         src = I.P.p;
     }
     k_panel_widen<<<grid1(I.n), 256, 0, I.S.st>>>(src, dst, I.nx, I.ny);
@@ -1138,7 +1253,7 @@ void Fused32::fresnel_get_transmission(double *t)
     I.p_valid = false; // T is formed in the work array
     I.push_slot();
     k_fresnel_get_t<<<grid1(I.n), 256, 0, I.S.st>>>(I.x.p, I.ill.p, I.P.p, I.n);
-    if (I.h_slot.tc_on) k_tc_pixels<<<grid1(I.n), 256, 0, I.S.st>>>(I.P.p, I.n, I.slot.p);
+    if (I.h_slot.tc_on) I.constrain_array(I.P.p);
     I.get_panel(I.P.p, 2, t);
 }
 
@@ -1219,6 +1334,19 @@ void Fused32::Impl::launch_iteration_wf(cudaStream_t st)
 void Fused32::Impl::launch_iteration(cudaStream_t st)
 {
     const Slot *const *sl = slot_ptr.p;
+    if (h_slot.tc_R > 0) {
+        // complex-constraint regions: the row pass in two halves around the
+        // region sums of both projected fields (Ps x is summed for ER too,
+        // so one captured graph serves every algorithm)
+        choice->col->col(S.kind == NADIA_FRESNEL, sl, 1, nx, ny, twx, st);
+        choice->row->tc_row(1, sl, 1, nx, ny, twy, st);
+        for (int field = 0; field < 2; ++field) {
+            k_tc32_sums<<<kTcBlocks, kTcThreads, 0, st>>>(slot.p, field, nullptr, n);
+            k_tc32_cmean<<<h_slot.tc_R, kTcThreads, 0, st>>>(slot.p, field, kTcBlocks);
+        }
+        choice->row->tc_row(2, sl, 1, nx, ny, twy, st);
+        return;
+    }
     choice->col->col(S.kind == NADIA_FRESNEL, sl, 1, nx, ny, twx, st);
     choice->row->row(kRowFull, sl, 1, nx, ny, twy, st);
 }
@@ -1257,7 +1385,7 @@ void Fused32::iterate(int count)
     I.push_slot();
     cudaStream_t st = I.S.st;
     if (!I.p_valid || (pfs && !I.q_valid)) I.prime(st);
-    const int per_iter = (pfs || wf) ? 3 : 2;
+    const int per_iter = (pfs || wf) ? 3 : (I.h_slot.tc_R > 0 ? 7 : 2);
     auto one = [&] {
         if (wf)
             I.launch_iteration_wf(st);

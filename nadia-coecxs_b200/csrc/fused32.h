@@ -27,7 +27,11 @@ public:
     void fresnel_get_transmission(double *t);
     // TransmissionConstraint's per-pixel part (charge flipping, unit
     // magnitude) inside the row pass's support projections
-    void set_constraint(bool on, bool unity, bool flip, int flip_sign);
+    // and its complex-constraint regions: map[k] = the region (1-based, 0:
+    // none) of pixel k in the reference's order, prm = alpha1, alpha2, fixed
+    // flag, fixed c_mean per region
+    void set_constraint(bool on, bool unity, bool flip, int flip_sign, int nregions = 0,
+                        const int *map = nullptr, const double *prm = nullptr);
     bool constrained() const;
     // the result a PhaseDiverseCDI exchanges (Fresnel: the transmission
     // function; else the estimate), natural order, double, on the device

@@ -64,6 +64,18 @@ struct alignas(64) Slot {
     int tc_on, tc_unity, tc_flip;
     float tc_sign;
     const float2 *tc_ill;
+    // complex-constraint regions (TransmissionConstraint.c++:76-172), when
+    // tc_R > 0: each pixel's region (0: none; panel layout), per region
+    // alpha1, alpha2, fixed flag, fixed c_mean; c_mean per field and region
+    // (field 0: Ps x, 1: Ps of the projection, 2: a whole array), the FP64
+    // region partials, and Y, the row pass's inverse transforms, kept between
+    // its two halves while the region sums are formed
+    int tc_R;
+    const int *tc_region;
+    const float *tc_par;
+    float *tc_cm;
+    double *tc_part;
+    float2 *Y;
     // PolyCDI: P is the padded mx x my grid (the estimate sits at rows
     // px..px+nx-1, columns py..py+ny-1); q holds |Psi|^2 of the padded
     // detector field in centred coordinates (panel layout over mx rows);
@@ -154,6 +166,10 @@ struct TileVariant {
     // FresnelCDI_WF passes in this tile shape (plain variants only)
     WfColLaunch wf_col = nullptr;
     RowLaunch wf_row = nullptr;
+    // the row pass's two halves around complex-constraint region sums
+    // (mode 1: inverse transforms into Y; 2: the constrained combine and the
+    // forward transforms; plain variants only)
+    RowLaunch tc_row = nullptr;
 };
 
 // PolyCDI passes of one tile shape: forward column transform of the padded
@@ -228,6 +244,12 @@ struct Fused32::Impl {
     int nx = 0, ny = 0, ncol = 0;
     size_t n = 0;
     DevBuf<float2> P, x, W, ill, tx, ty;
+    // complex-constraint regions (Slot::tc_*)
+    DevBuf<int> tc_region;
+    DevBuf<float> tc_par, tc_cm;
+    DevBuf<double> tc_part;
+    DevBuf<float2> Y;
+    void constrain_array(float2 *t); // the whole constraint on an array (field 2)
     DevBuf<float> sup, mI, tmp1, tmp2, maxpart;
     DevBuf<double> partials;
     DevBuf<long long> iter;

@@ -154,28 +154,6 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_col(const Slot *const *slots
 
 // ----------------------------------------------------------------- row pass
 
-// the constraint on a support-projected value z at panel address a, column
-// yy: on z itself, or for FresnelCDI on its transmission function
-// T = (z + L) / L (FresnelCDI::apply_support, FresnelCDI.c++:203-215), written
-// back as L T - L for columns below nx (set_transmission_function's bound)
-__device__ __forceinline__ float2 tc_apply(float2 z, const Slot &S, size_t a, int yy, int nx,
-                                           int ny)
-{
-    if (!S.tc_ill) return tc_pixel(z, S);
-    if (ny >= nx && yy >= nx) return z;
-    const float2 l = S.tc_ill[a];
-    const float denom = l.x * l.x + l.y * l.y;
-    float2 t = make_float2(1.f, 0.f);
-    if (denom != 0.f) {
-        const float rn = l.x * (z.x + l.x) + l.y * (z.y + l.y);
-        const float in = l.x * (z.y + l.y) - l.y * (z.x + l.x);
-        t = make_float2(rn / denom, in / denom);
-    }
-    t = tc_pixel(t, S);
-    return make_float2(l.x * t.x - l.y * t.y - l.x, l.x * t.y + l.y * t.x - l.y);
-}
-
-
 // finish the error metric of the column pass that just ran (block 0 of a
 // slot's row pass): from x's projection, or -- algorithms whose only
 // projection is of Ps x (a PfPs term alone) -- from Q's
@@ -200,6 +178,14 @@ __device__ __forceinline__ void finish_error_row(const Slot &S)
         *S.iter = it + 1;
     }
 }
+
+} // namespace f32
+} // namespace nadia
+
+#include "fused32_tc.cuh"
+
+namespace nadia {
+namespace f32 {
 
 template <class C, int MODE>
 __global__ void __launch_bounds__(C::NT, C::MINB) k_row(const Slot *const *slots, int nx, int ny,
@@ -229,13 +215,13 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_row(const Slot *const *slots
             float2 xn;
             if (er) {
                 xn = cscale(y, f);
-                if (tc) xn = tc_apply(xn, S, a, pos, nx, ny);
+                if (tc) xn = tc_apply(xn, S, a, pos, nx, ny, 1);
             } else {
                 const float2 xk = x[a];
                 float2 ps = make_float2(f * xk.x, f * xk.y), psf = make_float2(f * y.x, f * y.y);
                 if (tc) {
-                    ps = tc_apply(ps, S, a, pos, nx, ny);
-                    psf = tc_apply(psf, S, a, pos, nx, ny);
+                    ps = tc_apply(ps, S, a, pos, nx, ny, 0);
+                    psf = tc_apply(psf, S, a, pos, nx, ny, 1);
                 }
                 xn = make_float2(wid * xk.x + wpf * y.x + wps * ps.x + wpsf * psf.x,
                                  wid * xk.y + wpf * y.y + wps * ps.y + wpsf * psf.y);
@@ -336,6 +322,19 @@ void prepare_variant()
     set_smem<CC>(k_wf_col<CC>);
     set_smem<CR>(k_wf_row<CR, kRowFull>);
     set_smem<CR>(k_wf_row<CR, kRowPrime>);
+    set_smem<CR>(k_row_tc<CR, 1>);
+    set_smem<CR>(k_row_tc<CR, 2>);
+}
+
+template <class C>
+void launch_row_tc(int half, const Slot *const *slots, int nslots, int nx, int ny, const float2 *tw,
+                   cudaStream_t st)
+{
+    const dim3 grid(nx / C::L, nslots);
+    if (half == 1)
+        k_row_tc<C, 1><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
+    else
+        k_row_tc<C, 2><<<grid, C::NT, smem_bytes<C>(), st>>>(slots, nx, ny, tw);
 }
 
 template <class C>
@@ -492,6 +491,7 @@ TileVariant make_variant(const char *radices)
     t.row = &launch_row<CR>;
     t.wf_col = &launch_wf_col<CC>;
     t.wf_row = &launch_wf_row<CR>;
+    t.tc_row = &launch_row_tc<CR>;
     return t;
 }
 
@@ -511,6 +511,7 @@ TileVariant make_ping(const char *radices)
     t.prepare = &prepare_variant<CC, CR>;
     t.col = &launch_col<CC>;
     t.row = &launch_row<CR>;
+    t.tc_row = &launch_row_tc<CR>;
     return t;
 }
 

@@ -386,17 +386,31 @@ void Solver::set_transmission_constraint(int unity, int flip, int flip_sign, int
     NADIA_REQUIRE(nregions == 0 || n % 4 == 0, NADIA_ERR_UNSUPPORTED,
                   "complex-constraint regions need a pixel count divisible by 4");
     if (prec == NADIA_FP32) {
-        // the per-pixel part runs inside the fused row pass; regions need
-        // whole-image sums between the projection and its update
-        NADIA_REQUIRE(nregions == 0 && kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
-                      "complex-constraint regions (and PolyCDI constraints) run in the FP64 "
-                      "form: convert the reconstruction first");
-        f32->set_constraint(true, unity != 0, flip != 0, flip_sign);
+        // the per-pixel part runs inside the fused row pass; regions split
+        // the row pass around their sums (fused32_tc.cuh)
+        NADIA_REQUIRE(kind != NADIA_POLY, NADIA_ERR_UNSUPPORTED,
+                      "PolyCDI constraints run in the FP64 form: convert the reconstruction "
+                      "first");
+        NADIA_REQUIRE(nregions == 0 || (regions && alpha), NADIA_ERR_INVALID,
+                      "complex-constraint regions need their masks and alphas");
+        std::vector<int> map(nregions > 0 ? n : 0, 0);
+        std::vector<double> prm(4 * (size_t)nregions, 0.0);
+        for (int r = 0; r < nregions; ++r) {
+            for (size_t k = 0; k < n; ++k)
+                if (regions[(size_t)r * n + k] > 0 && map[k] == 0) map[k] = r + 1;
+            prm[4 * r] = alpha[2 * r];
+            prm[4 * r + 1] = alpha[2 * r + 1];
+            const bool fixed = fixed_c && fixed_c[r] == fixed_c[r];
+            prm[4 * r + 2] = fixed ? 1.0 : 0.0;
+            prm[4 * r + 3] = fixed ? fixed_c[r] : 0.0;
+        }
+        f32->set_constraint(true, unity != 0, flip != 0, flip_sign, nregions, map.data(),
+                            prm.data());
         tc.active = true;
         tc.unity = unity ? 1 : 0;
         tc.flip = flip ? 1 : 0;
         tc.flip_sign = flip_sign > 0 ? 1 : -1;
-        tc.nregions = 0;
+        tc.nregions = nregions;
         tc.custom = nullptr;
         tc.user = nullptr;
         return;

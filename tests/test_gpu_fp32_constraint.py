@@ -1,7 +1,8 @@
-"""The transmission constraint's per-pixel part (unit magnitude, charge
-flipping) inside the FP32 form's fused row pass, and FP32 phase-diverse
-frames: each step matches the FP64 form (itself bit-identical to the oracle)
-to the FP32 per-step bar, 2e-5 relative; short runs follow it."""
+"""The transmission constraint in the FP32 form -- its per-pixel part (unit
+magnitude, charge flipping) inside the fused row pass, its complex-constraint
+regions in the row pass split around the region sums -- and FP32
+phase-diverse frames: each step matches the FP64 form (itself the oracle's
+arithmetic) to the FP32 per-step bar, 2e-5 relative; short runs follow it."""
 import numpy as np
 import pytest
 
@@ -87,12 +88,55 @@ def test_constraint_changes_the_iterate():
     assert l2rel(b.get_exit_surface_wave(), a.get_exit_surface_wave()) <= STEP_TOL
 
 
-def test_refusals_and_conversion():
+@pytest.mark.parametrize("kind", ["planar", "fresnel"])
+@pytest.mark.parametrize("alg", ["ER", "HIO"])
+def test_regions_teacher_forced_steps(kind, alg):
+    """Three complex-constraint regions (one with a fixed c_mean, one
+    overlapping another) with charge flipping and unit magnitude: the FP32
+    row pass in two halves around the region sums against the FP64 form."""
+    n = 256
+    a, b = planar_pair(n) if kind == "planar" else fresnel_pair(n)
+    regions, alphas, fixed = synth.constraint_regions(n)
+    for s in (a, b):
+        s.set_algorithm(alg)
+        s.set_transmission_constraint(True, True, 1, regions, alphas, fixed)
+    assert b.get_precision() == pynadia.FP32
+    # FresnelCDI's initial transmission function is real (1 - 0.2 rand), so
+    # sum |arg T| over a region is a sum of rounding errors and c_mean their
+    # ratio to sum |ln|T||: any two arithmetics disagree there (the FP32 step
+    # from it differs by 0.47, the next one by 1e-6).  The comparison starts
+    # after two FP64 iterations have given T its phase.
+    if kind == "fresnel":
+        a.iterate(2)
+    for _ in range(4):
+        b.set_exit_surface_wave(a.get_exit_surface_wave())
+        a.iterate(1)
+        b.iterate(1)
+        assert abs(b.get_error() - a.get_error()) <= STEP_TOL * a.get_error()
+        assert l2rel(b.get_exit_surface_wave(), a.get_exit_surface_wave()) <= STEP_TOL
+    if kind == "fresnel":  # get_transmission applies the constraint, regions included
+        assert l2rel(b.get_transmission(), a.get_transmission()) <= STEP_TOL
+
+
+def test_regions_change_the_iterate():
+    """The regions are really applied: with them the FP32 step differs from
+    the step with the per-pixel part alone by far more than the FP32 bar."""
     n = 256
     a, b = planar_pair(n)
     regions, alphas, fixed = synth.constraint_regions(n)
-    with pytest.raises(pynadia.NadiaError):
-        b.set_transmission_constraint(True, True, 1, regions, alphas, fixed)
+    for s in (a, b):
+        s.set_algorithm("HIO")
+    a.set_transmission_constraint(True, True, 1)
+    b.set_transmission_constraint(True, True, 1, regions, alphas, fixed)
+    b.set_exit_surface_wave(a.get_exit_surface_wave())
+    a.iterate(1)
+    b.iterate(1)
+    assert l2rel(b.get_exit_surface_wave(), a.get_exit_surface_wave()) > 1e-3
+
+
+def test_refusals_and_conversion():
+    n = 256
+    a, b = planar_pair(n)
     b.set_transmission_constraint(True, True, -1)
     with pytest.raises(pynadia.NadiaError):
         b.set_transmission_custom(lambda t, nx, ny: None)
