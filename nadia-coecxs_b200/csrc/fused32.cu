@@ -950,42 +950,57 @@ void to_panel(const T *h, int stride, float *p, int nx, int ny, bool fold)
 }
 } // namespace
 
+// the host staging array of the conversions, kept between calls (a fresh
+// one would be page-faulted in again on every upload and readback)
+float *Fused32::Impl::staging(size_t count)
+{
+    if (stage.size() < count) stage.resize(count);
+    return stage.data();
+}
+
 void Fused32::Impl::put_panel_f(const float *h, int stride, void *dst, bool fold)
 {
-    std::vector<float> p(n * stride);
-    to_panel(h, stride, p.data(), nx, ny, fold);
-    NADIA_CUDA(cudaMemcpyAsync(dst, p.data(), n * stride * sizeof(float), cudaMemcpyHostToDevice,
-                               S.st));
+    float *p = staging(n * stride);
+    to_panel(h, stride, p, nx, ny, fold);
+    NADIA_CUDA(cudaMemcpyAsync(dst, p, n * stride * sizeof(float), cudaMemcpyHostToDevice, S.st));
     NADIA_CUDA(cudaStreamSynchronize(S.st));
 }
 
 void Fused32::Impl::put_panel(const double *h, int stride, void *dst, bool fold)
 {
-    std::vector<float> p(n * stride);
-    to_panel(h, stride, p.data(), nx, ny, fold);
-    NADIA_CUDA(cudaMemcpyAsync(dst, p.data(), n * stride * sizeof(float), cudaMemcpyHostToDevice,
-                               S.st));
+    float *p = staging(n * stride);
+    to_panel(h, stride, p, nx, ny, fold);
+    NADIA_CUDA(cudaMemcpyAsync(dst, p, n * stride * sizeof(float), cudaMemcpyHostToDevice, S.st));
     NADIA_CUDA(cudaStreamSynchronize(S.st));
 }
 
-void Fused32::Impl::get_panel_f(const void *src, int stride, float *h)
+namespace {
+// panel layout (FP32) to the reference's order, converted to T in the pass
+template <class T>
+void from_panel(const float *p, int stride, T *h, int nx, int ny)
 {
-    std::vector<float> p(n * stride);
-    NADIA_CUDA(cudaMemcpyAsync(p.data(), src, n * stride * sizeof(float), cudaMemcpyDeviceToHost,
-                               S.st));
-    NADIA_CUDA(cudaStreamSynchronize(S.st));
     for (int xx = 0; xx < nx; ++xx)
         for (int yy = 0; yy < ny; ++yy) {
             const size_t a = panel_index_dev(xx, yy, nx), d = (size_t)xx * ny + yy;
-            for (int c = 0; c < stride; ++c) h[d * stride + c] = p[a * stride + c];
+            for (int c = 0; c < stride; ++c) h[d * stride + c] = (T)p[a * stride + c];
         }
+}
+} // namespace
+
+void Fused32::Impl::get_panel_f(const void *src, int stride, float *h)
+{
+    float *p = staging(n * stride);
+    NADIA_CUDA(cudaMemcpyAsync(p, src, n * stride * sizeof(float), cudaMemcpyDeviceToHost, S.st));
+    NADIA_CUDA(cudaStreamSynchronize(S.st));
+    from_panel(p, stride, h, nx, ny);
 }
 
 void Fused32::Impl::get_panel(const void *src, int stride, double *h)
 {
-    std::vector<float> f(n * stride);
-    get_panel_f(src, stride, f.data());
-    for (size_t k = 0; k < f.size(); ++k) h[k] = f[k];
+    float *p = staging(n * stride);
+    NADIA_CUDA(cudaMemcpyAsync(p, src, n * stride * sizeof(float), cudaMemcpyDeviceToHost, S.st));
+    NADIA_CUDA(cudaStreamSynchronize(S.st));
+    from_panel(p, stride, h, nx, ny);
 }
 
 // set_intensity and set_beam_stop mark sqrt(I) for conversion; it is formed
@@ -999,7 +1014,8 @@ void Fused32::Impl::flush_intensity()
 {
     if (!mI_dirty) return;
     mI_dirty = false;
-    std::vector<float> m(n);
+    std::vector<float> &m = mstage; // kept between calls, like the staging array
+    m.resize(n);
     double norm2 = 0;
     for (size_t d = 0; d < n; ++d) {
         const bool measured = !S.has_beam_stop || h_bs[d] > 0;

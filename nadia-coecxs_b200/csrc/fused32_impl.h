@@ -295,6 +295,8 @@ struct Fused32::Impl {
     // host arrays in the reference's order <-> device arrays in the panel
     // layout (stride 1: real, 2: complex; fold: PlanarCDI's centred detector
     // to transform order), converted on the host: plain copies on the device
+    std::vector<float> stage, mstage; // host staging arrays, kept between calls
+    float *staging(size_t count);
     void put_panel(const double *h, int stride, void *dst, bool fold);
     void put_panel_f(const float *h, int stride, void *dst, bool fold);
     void get_panel(const void *src, int stride, double *h);
