@@ -35,7 +35,7 @@ size_t footprint_bytes(int kind, int nx, int ny, int prec, int n_best, int pad_n
     size_t b = 8 + 8 * (size_t)Solver::kRing + 8 * (2 * (size_t)plain::kRedBlocks + 64) + 16;
     if (prec == NADIA_FP64) {
         b += n * (16 + 8 + 8 + 8 + 8); // x, support, sqrt(I), blur result, scratch
-        b += 4 * 16 * n;               // the combine's four projection terms at most
+        if (kind != NADIA_FRESNEL_WF) b += 4 * 16 * n; // the combine's projection terms at most
         b += 8 * n;                    // beam stop
         b += 16 * (size_t)(nx + ny);   // transform twiddles
         if ((nx | ny) & 1) b += 16 * n; // odd grids: the quadrant swap's gather target
@@ -48,12 +48,15 @@ size_t footprint_bytes(int kind, int nx, int ny, int prec, int n_best, int pad_n
                  16 * (size_t)(pad_nx + pad_ny);
     } else {
         b += n * (8 + 8 + 4 + 4);                     // P, x, support, sqrt(I)
-        b += 8 * (size_t)(ny / 2) + 8 + 4 + 2 * 8;    // partials, counter, flag, slot pointer
+        // partials (one per column tile; FresnelCDI_WF one per row tile),
+        // counter, flag, slot pointer
+        b += 8 * (size_t)(kind == NADIA_FRESNEL_WF ? std::max(nx, ny / 2) : ny / 2) + 8 + 4 + 2 * 8;
         b += sizeof(f32::Slot);
         const size_t tiles = ((size_t)(nx + 31) / 32) * ((ny + 31) / 32);
         b += 2 * 4 * n + 4 * (std::max<size_t>(tiles, 592) + 2); // shrinkwrap scratch
         b += (size_t)n_best * 8 * n;
         if (kind == NADIA_FRESNEL) b += 8 * n + 8 * n + 8 * (size_t)(nx + ny);
+        if (kind == NADIA_FRESNEL_WF) b += 8 * (size_t)(nx + ny); // per-axis zone-plate factors
         if (kind == NADIA_POLY) {
             const size_t m = (size_t)pad_nx * pad_ny;
             b += 8 * m + 4 * m;                                  // padded work array, |Psi|^2

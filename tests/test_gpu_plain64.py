@@ -126,12 +126,16 @@ def test_transmission_custom_function():
 
 
 def test_transmission_constraint_refusals():
-    # the FP32 form takes the per-pixel part only: regions need the FP64 form
+    # the FP32 form takes regions but not a custom host function
     s = pynadia.Solver("planar", 256, 256, precision=pynadia.FP32)
     regions, alphas, fixed = sc.constraint_regions(256)
+    s.set_transmission_constraint(True, True, 1, regions, alphas, fixed)
     with pytest.raises(pynadia.NadiaError) as e:
-        s.set_transmission_constraint(True, True, 1, regions, alphas, fixed)
+        s.set_transmission_custom(lambda t: None)
     assert e.value.code == 3
+    with pytest.raises(pynadia.NadiaError) as e:   # at most 16 regions
+        s.set_transmission_constraint(True, True, 1, [regions[0]] * 17, [alphas[0]] * 17)
+    assert e.value.code == 2
     s = gpu("planar", 32, 32)
     with pytest.raises(pynadia.NadiaError) as e:   # a custom function needs a constraint
         s.set_transmission_custom(lambda t: None)

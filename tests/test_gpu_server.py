@@ -54,7 +54,9 @@ def run_alone(request):
                                          ("fresnel", pynadia.FP64, 128),
                                          ("fresnel", pynadia.FP32, 256),
                                          ("poly", pynadia.FP64, 96),
-                                         ("poly", pynadia.FP32, 240)])
+                                         ("poly", pynadia.FP32, 240),
+                                         ("fresnel_wf", pynadia.FP64, 128),
+                                         ("fresnel_wf", pynadia.FP32, 256)])
 def test_admission_charge_covers_device_bytes(kind, prec, n):
     # handles of earlier tests that are still unreferenced release their
     # buffers when collected; collect them before the count is taken
@@ -69,11 +71,19 @@ def test_admission_charge_covers_device_bytes(kind, prec, n):
     elif kind == "poly":
         p = synth.PolyCase(n, seed=3, padding=8 if prec == pynadia.FP32 else 4, photons=1e7)
         inten, sup = p.intensity, p.support
+    elif kind == "fresnel_wf":
+        w = synth.FresnelWFCase(n, seed=3)
+        kw = dict(wavelength=w.wavelength, zone_focal_length=w.z12, focal_detector_length=w.z23,
+                  pixel_size=w.pixel)
+        inten, sup = w.intensity, None
     else:
         c = planar(n, 3)
         inten, sup = c.intensity, c.support
     s = pynadia.Solver(kind, n, n, precision=prec, **kw)
-    s.set_support(sup, True)
+    if kind == "fresnel_wf":
+        s.set_wf_support(w.z_diameter)
+    else:
+        s.set_support(sup, True)
     s.set_intensity(inten)
     s.set_beam_stop(np.ones((n, n)))
     pad = (0, 0)
@@ -84,7 +94,8 @@ def test_admission_charge_covers_device_bytes(kind, prec, n):
         nl = p.spectrum.shape[0]
     s.initialise_estimate(1)
     for alg in ("HIO", "RAAR", "ER"):
-        s.set_algorithm(alg)
+        if kind != "fresnel_wf":  # its algorithm is fixed
+            s.set_algorithm(alg)
         s.iterate(3)
     s.apply_shrinkwrap(1.5, 0.1)
     s.get_exit_surface_wave()
