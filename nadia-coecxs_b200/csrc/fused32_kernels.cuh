@@ -72,17 +72,27 @@ __device__ __forceinline__ float2 combine2(float2 xk, float2 y, float f, float w
 }
 
 // FP64 block sum; result valid in thread 0
+// (NT that is not a multiple of 32: the last warp holds NT % 32 threads, a
+// power of two, and sums over those lanes alone)
 template <int NT>
 __device__ __forceinline__ double block_sum(double v)
 {
-    __shared__ double red[NT / 32];
+    constexpr int NW = (NT + 31) / 32, TAIL = NT % 32;
+    static_assert(NT >= 32 && (TAIL & (TAIL - 1)) == 0, "last warp: a power of two of lanes");
+    __shared__ double red[NW];
+    if (TAIL == 0 || (int)(threadIdx.x >> 5) < NW - 1) {
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    } else {
+#pragma unroll
+        for (int off = TAIL / 2; off > 0; off >>= 1)
+            v += __shfl_down_sync((1u << TAIL) - 1u, v, off);
+    }
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
     __syncthreads();
     double t = 0;
     if (threadIdx.x < 32) {
-        t = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.0;
+        t = threadIdx.x < NW ? red[threadIdx.x] : 0.0;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
     }

@@ -1,7 +1,9 @@
 // fused32_poly.cu -- the FP32 PolyCDI form: tile shapes of the padded grid
 // sizes, the set-up done by set_spectrum, and the iteration (the kernels and
 // their design are in fused32_poly.cuh).
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <map>
 
 #include "batch.h"
@@ -14,15 +16,22 @@ namespace f32 {
 
 // Padded sizes with PolyCDI tiles: 256 and 512 (small cases) and 1080, the
 // 1024 x 1024 detector padded by 28 on each side (1080 = 6*6*6*5, so every
-// radix divides the 30 values a thread holds).  Swizzles from
-// tests/swizzle_search.py.
+// radix divides the 30 values a thread holds).  A 1080-point tile needs
+// about 168 registers a thread, so an SM holds 288 such threads: as one CTA
+// of 8 signals, or as two independent CTAs of 4 signals and 144 threads
+// (four and a half warps), whose global loads and barriers overlap each
+// other's arithmetic.  Swizzles from tests/swizzle_search.py.
 const std::vector<PolyVariant> &poly_variants(int n)
 {
     static const std::map<int, std::vector<PolyVariant>> reg = [] {
         std::map<int, std::vector<PolyVariant>> r;
         r[256].push_back(make_poly<256, 256, 8, 3, Swizzle<4, 6, 3, 2>, 8, 8, 4>("8.8.4"));
         r[512].push_back(make_poly<512, 256, 8, 2, Swizzle<4, 6, 3, 2>, 16, 8, 4>("16.8.4"));
-        r[1080].push_back(make_poly<1080, 288, 8, 1, Swizzle<4, 0, 1, 2>, 6, 6, 6, 5>("6.6.6.5"));
+        r[1080].push_back(make_poly<1080, 144, 4, 2, Swizzle<7, 0, 7, 1>, 6, 6, 6, 5>("6.6.6.5"));
+        r[1080].push_back(
+            make_poly<1080, 144, 4, 2, Swizzle<7, 0, 7, 1>, 6, 6, 6, 5>("6.6.6.5 direct", false));
+        r[1080].push_back(
+            make_poly<1080, 288, 8, 1, Swizzle<4, 0, 1, 2>, 6, 6, 6, 5>("6.6.6.5 direct", false));
         return r;
     }();
     static const std::vector<PolyVariant> none;
@@ -37,11 +46,15 @@ using namespace f32;
 namespace {
 
 // the first variant whose tiles divide `tiles_of` (column tiles run over the
-// padded columns, row tiles over the estimate's rows)
+// padded columns, row tiles over the estimate's rows); NADIA_POLY_TILE=k
+// starts the search at the k-th registered shape of the size
 const PolyVariant *pick(int n, int tiles_of)
 {
-    for (const auto &v : poly_variants(n))
-        if (tiles_of % v.L == 0) return &v;
+    const auto &vs = poly_variants(n);
+    const char *e = std::getenv("NADIA_POLY_TILE");
+    const size_t first = e ? (size_t)std::max(0, std::atoi(e)) : 0;
+    for (size_t k = first < vs.size() ? first : 0; k < vs.size(); ++k)
+        if (tiles_of % vs[k].L == 0) return &vs[k];
     return nullptr;
 }
 

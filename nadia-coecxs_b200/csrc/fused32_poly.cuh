@@ -91,6 +91,63 @@ __global__ void __launch_bounds__(kExpandThreads) k_poly_expand(const Slot *cons
     float *__restrict__ ratio = S.ratio;
     const unsigned n = (unsigned)nx * (unsigned)ny;
     double diff = 0.0;
+    if ((ny & 3) == 0) {
+        // whole panels: a thread takes the four pixels (i, 4 jp .. 4 jp + 3),
+        // sixteen contiguous bytes of sqrt(I) and of the ratio, and reads each
+        // wavelength's row part once and its four column parts as one vector
+        // (lanes run along i, so the column parts are one broadcast); each
+        // pixel's sum runs over the wavelengths in the same order as below
+        const float4 *__restrict__ mI4 = reinterpret_cast<const float4 *>(mI);
+        float4 *__restrict__ ratio4 = reinterpret_cast<float4 *>(ratio);
+        const unsigned cells = n / kPanel;
+        for (unsigned u = blockIdx.x * kExpandThreads + threadIdx.x; u < cells;
+             u += gridDim.x * kExpandThreads) {
+            const unsigned jp = u / (unsigned)nx;
+            const int i = (int)(u - jp * (unsigned)nx);
+            const float4 m4 = __ldg(&mI4[u]);
+            const float m[4] = {m4.x, m4.y, m4.z, m4.w};
+            float r[4] = {1.f, 1.f, 1.f, 1.f};
+            if (!(m[0] < 0.f) || !(m[1] < 0.f) || !(m[2] < 0.f) || !(m[3] < 0.f)) {
+                const int4 *__restrict__ gy4 = reinterpret_cast<const int4 *>(gy + jp * kPanel);
+                float acc[4] = {0.f, 0.f, 0.f, 0.f};
+                int l = 0;
+                for (; l + 2 <= nl; l += 2) {
+                    float qv[2][4];
+#pragma unroll
+                    for (int u2 = 0; u2 < 2; ++u2) {
+                        const int ox = __ldg(&gx[(l + u2) * nx + i]);
+                        const int4 oy = __ldg(&gy4[(l + u2) * (ny / kPanel)]);
+                        const int o[4] = {ox + oy.x, ox + oy.y, ox + oy.z, ox + oy.w};
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) qv[u2][k] = o[k] >= 0 ? __ldg(&q[o[k]]) : 0.f;
+                    }
+#pragma unroll
+                    for (int u2 = 0; u2 < 2; ++u2) {
+                        const float w = __ldg(&wl[l + u2]);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) acc[k] += w * qv[u2][k];
+                    }
+                }
+                for (; l < nl; ++l) {
+                    const int ox = __ldg(&gx[l * nx + i]);
+                    const int4 oy = __ldg(&gy4[l * (ny / kPanel)]);
+                    const int o[4] = {ox + oy.x, ox + oy.y, ox + oy.z, ox + oy.w};
+                    const float w = __ldg(&wl[l]);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) acc[k] += w * (o[k] >= 0 ? __ldg(&q[o[k]]) : 0.f);
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (m[k] < 0.f) continue;
+                    const float calc = sqrtf(acc[k]);
+                    r[k] = calc == 0.f ? 0.f : m[k] / calc;
+                    const double d = (double)m[k] - (double)calc;
+                    diff += d * d;
+                }
+            }
+            ratio4[u] = make_float4(r[0], r[1], r[2], r[3]);
+        }
+    } else {
     for (unsigned a = blockIdx.x * kExpandThreads + threadIdx.x; a < n;
          a += gridDim.x * kExpandThreads) {
         const unsigned t = a / kPanel, jp = t / (unsigned)nx;
@@ -124,6 +181,7 @@ __global__ void __launch_bounds__(kExpandThreads) k_poly_expand(const Slot *cons
         }
         ratio[a] = r;
     }
+    }
     const double tot = block_sum<kExpandThreads>(diff);
     if (threadIdx.x == 0) S.partials[blockIdx.x] = tot;
 }
@@ -154,7 +212,31 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_col_inv(const Slot *con
     });
 }
 
-template <class C, int MODE>
+// 16-byte asynchronous copies global -> shared (completion: cp_async_wait_all)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
+
+// Shared memory of the row pass: the exchange tile, then (PREF) the tile's
+// rows of x and of the support, staged in their panel order [ny/4][L][4]
+template <class C, bool PREF>
+constexpr size_t poly_row_smem()
+{
+    return (size_t)C::smem_words() * sizeof(float2) + (PREF ? (size_t)C::N * C::L * 12 : 0);
+}
+
+// PREF: when the window's width is a multiple of the panel (always for the
+// padded grids in use), the tile's rows of x and of the support are copied
+// into shared memory by cp.async at the start, so those loads run during the
+// inverse row transform instead of stalling the combine after it.  The tile's
+// rows of a panel are one contiguous run of L*4 elements.
+template <class C, int MODE, bool PREF>
 __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_row(const Slot *const *slots,
                                                                const float2 *__restrict__ tw)
 {
@@ -166,6 +248,26 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_row(const Slot *const *
     const int nx = mx - 2 * px, ny = my - 2 * py;
     const int i0 = blockIdx.x * C::L; // unpadded row of the tile's first signal
     float2 v[C::E];
+    float2 *xs = sm + C::smem_words();
+    float *ss = reinterpret_cast<float *>(xs + C::N * C::L);
+    const bool staged = PREF && MODE == kRowFull && (ny & 3) == 0;
+    if (staged) {
+        constexpr int SEG = C::L * kPanel; // elements of one panel's run
+        const int nseg = ny / kPanel;
+        const bool need_x = !S.er;
+        const float2 *__restrict__ xg = x + (size_t)i0 * kPanel;
+        const float *__restrict__ sg = S.sup + (size_t)i0 * kPanel;
+        // x: SEG/2 chunks of 16 bytes a run; the support: SEG/4
+        for (int c = threadIdx.x; c < nseg * (SEG / 2); c += C::NT) {
+            if (!need_x) break;
+            const int jp = c / (SEG / 2), k = c % (SEG / 2);
+            cp_async16(xs + jp * SEG + 2 * k, xg + (size_t)jp * nx * kPanel + 2 * k);
+        }
+        for (int c = threadIdx.x; c < nseg * (SEG / 4); c += C::NT) {
+            const int jp = c / (SEG / 4), k = c % (SEG / 4);
+            cp_async16(ss + jp * SEG + 4 * k, sg + (size_t)jp * nx * kPanel + 4 * k);
+        }
+    }
 
     if (MODE == kRowFull) {
         if (blockIdx.x == 0 && S.project) {
@@ -188,6 +290,10 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_row(const Slot *const *
             v[e] = P[paddr(px + i0 + s, pos, mx)];
         });
         transform<C, false>(v, sm, tw);
+        if (staged) {
+            cp_async_wait_all();
+            __syncthreads();
+        }
         const float *__restrict__ sup = S.sup;
         const float wid = S.w_id, wpf = S.w_pf, wps = S.w_ps, wpsf = S.w_psf;
         const bool er = S.er;
@@ -196,12 +302,13 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_row(const Slot *const *
             float2 xn = make_float2(0.f, 0.f);
             if (j >= 0 && j < ny) {
                 const size_t a = paddr(i0 + s, j, nx);
-                const float f = support_factor(__ldg(&sup[a]));
+                const int b = ((j / kPanel) * C::L + s) * kPanel + j % kPanel; // staged index
+                const float f = support_factor(staged ? ss[b] : __ldg(&sup[a]));
                 const float2 y = v[e];
                 if (er) {
                     xn = cscale(y, f);
                 } else {
-                    const float2 xk = x[a];
+                    const float2 xk = staged ? xs[b] : x[a];
                     xn = combine2(xk, y, f, wid, wpf, wps, wpsf);
                 }
                 x[a] = xn;
@@ -220,13 +327,15 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_row(const Slot *const *
     });
 }
 
-template <class CC, class CR>
+template <class CC, class CR, bool PREF>
 void prepare_poly()
 {
     set_smem<CC>(k_poly_col_fwd<CC>);
     set_smem<CC>(k_poly_col_inv<CC>);
-    set_smem<CR>(k_poly_row<CR, kRowFull>);
-    set_smem<CR>(k_poly_row<CR, kRowPrime>);
+    NADIA_CUDA(cudaFuncSetAttribute(k_poly_row<CR, kRowFull, PREF>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)poly_row_smem<CR, PREF>()));
+    set_smem<CR>(k_poly_row<CR, kRowPrime, PREF>);
 }
 
 // column passes: tiles = my / L column tiles; row pass: tiles = nx / L row tiles
@@ -245,18 +354,19 @@ void launch_poly_col_inv(const Slot *const *slots, int nslots, int tiles, cudaSt
     k_poly_col_inv<C><<<dim3(tiles, nslots), C::NT, smem_bytes<C>(), st>>>(slots, tw);
 }
 
-template <class C>
+template <class C, bool PREF>
 void launch_poly_row(int mode, const Slot *const *slots, int nslots, int tiles, cudaStream_t st,
                      const float2 *tw)
 {
     if (mode == kRowFull)
-        k_poly_row<C, kRowFull><<<dim3(tiles, nslots), C::NT, smem_bytes<C>(), st>>>(slots, tw);
+        k_poly_row<C, kRowFull, PREF>
+            <<<dim3(tiles, nslots), C::NT, poly_row_smem<C, PREF>(), st>>>(slots, tw);
     else
-        k_poly_row<C, kRowPrime><<<dim3(tiles, nslots), C::NT, smem_bytes<C>(), st>>>(slots, tw);
+        k_poly_row<C, kRowPrime, PREF><<<dim3(tiles, nslots), C::NT, smem_bytes<C>(), st>>>(slots, tw);
 }
 
 template <int N, int NT, int L, int MINB, class SW, int... Rs>
-PolyVariant make_poly(const char *radices)
+PolyVariant make_poly(const char *radices, bool prefetch = true)
 {
     using CC = TileCfg<N, NT, L, kColMap, Radices<Rs...>, SW, MINB>;
     using CR = TileCfg<N, NT, L, kRowMap, Radices<Rs...>, SW, MINB>;
@@ -265,10 +375,10 @@ PolyVariant make_poly(const char *radices)
     t.nt = NT;
     t.L = L;
     t.radices = radices;
-    t.prepare = &prepare_poly<CC, CR>;
+    t.prepare = prefetch ? &prepare_poly<CC, CR, true> : &prepare_poly<CC, CR, false>;
     t.col_fwd = &launch_poly_col_fwd<CC>;
     t.col_inv = &launch_poly_col_inv<CC>;
-    t.row = &launch_poly_row<CR>;
+    t.row = prefetch ? &launch_poly_row<CR, true> : &launch_poly_row<CR, false>;
     return t;
 }
 

@@ -42,6 +42,8 @@ def rowmap(beta, NR, L):
 def wavefronts(addrs):
     total = 0
     for half in (addrs[:16], addrs[16:]):
+        if not half:   # the last warp of a tile whose thread count is not a multiple of 32
+            continue
         banks = {}
         for a in half:
             banks.setdefault((2 * a) % 32, set()).add(a)
@@ -58,25 +60,25 @@ def count(N, NT, L, radices, mapf, sw):
         NR, B = N // R, E // R
         for q in range(B):
             for r in range(R):
-                for w in range(NT // 32):
+                for w in range((NT + 31) // 32):
                     addrs = []
-                    for lane in range(32):
+                    for lane in range(min(32, NT - 32 * w)):
                         s, j = mapf(w * 32 + lane + q * NT, NR, L)
                         base = (j // Ns) * Ns * R + j % Ns
                         addrs.append(sw((base + r * Ns) * L + s))
                     tot += wavefronts(addrs)
-                    ideal += 2
+                    ideal += (len(addrs) + 15) // 16
         R2 = order[p + 1]
         NR2, B2 = N // R2, E // R2
         for q in range(B2):
             for r in range(R2):
-                for w in range(NT // 32):
+                for w in range((NT + 31) // 32):
                     addrs = []
-                    for lane in range(32):
+                    for lane in range(min(32, NT - 32 * w)):
                         s, j = mapf(w * 32 + lane + q * NT, NR2, L)
                         addrs.append(sw((j + r * NR2) * L + s))
                     tot += wavefronts(addrs)
-                    ideal += 2
+                    ideal += (len(addrs) + 15) // 16
         Ns *= R
     return tot, max(ideal, 1)
 

@@ -135,7 +135,7 @@ def test_transmission_constraint_refusals():
     assert e.value.code == 3
     with pytest.raises(pynadia.NadiaError) as e:   # at most 16 regions
         s.set_transmission_constraint(True, True, 1, [regions[0]] * 17, [alphas[0]] * 17)
-    assert e.value.code == 2
+    assert e.value.code == 1   # NADIA_ERR_INVALID: a bad argument
     s = gpu("planar", 32, 32)
     with pytest.raises(pynadia.NadiaError) as e:   # a custom function needs a constraint
         s.set_transmission_custom(lambda t: None)

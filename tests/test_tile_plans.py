@@ -202,7 +202,9 @@ def test_registry_found():
 def test_tile_shape_constraints(v):
     N, NT, L, rad = v["N"], v["NT"], v["L"], v["rad"]
     assert np.prod(rad) == N
-    assert N * L % NT == 0 and NT % 32 == 0
+    # whole warps, or (PolyCDI's two-CTA 1080-point tiles) a last half warp,
+    # which the block reductions sum over on its own
+    assert N * L % NT == 0 and (NT % 32 == 0 or (v["kind"] == "poly" and NT % 32 == 16))
     E = N * L // NT
     assert E % reduce(lambda a, b: a * b // gcd(a, b), rad) == 0
     assert all((N // r) % K == 0 for r in rad), "row tiles need N/R divisible by the panel"
