@@ -271,11 +271,14 @@ constexpr int kPanel = 4; // panel width K
 // pattern of each warp).
 template <int S1_, int S2_, int M_, int SH_>
 struct Swizzle {
-    static __host__ __device__ __forceinline__ int apply(int a)
+    static constexpr __host__ __device__ __forceinline__ int apply(int a)
     {
         const int t = (a >> S1_) ^ (S2_ ? (a >> S2_) : 0);
         return a ^ ((t & M_) << SH_);
     }
+    // apply() is linear over GF(2) (shifts, masks and exclusive ors), so
+    // where two addends have no bit in common, apply(a + b) =
+    // apply(a) ^ apply(b).
     // Adding a multiple of 2^B, B above every bit the swizzle reads
     // (S1..S1+2, S2..S2+2) and writes (SH..SH+2), commutes with it:
     // apply(a + r*c) = apply(a) + r*c.
@@ -348,6 +351,16 @@ struct TileCfg {
         }
     }
 };
+
+constexpr bool pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
+
+// An exchange address (p + r*Nr)*L + s with p < Nr, s < L and r < R splits
+// into addends with no common bit (p*L + s below Nr*L, r*Nr*L at and above
+// it, below Nr*L*R) when Nr*L and R are powers of two; the swizzled address
+// is then the swizzle of the first addend, once per butterfly, XOR the
+// swizzle of the second, a constant.
+template <int R, int STRIDE>
+constexpr bool xor_split() { return pow2(R) && pow2(STRIDE); }
 
 constexpr int hibit(int r)
 {
@@ -435,6 +448,12 @@ __device__ __forceinline__ void pass_exchange(float2 (&v)[C::E], float2 *sm0, fl
             const int a0 = C::sidx(s, base);
 #pragma unroll
             for (int r = 0; r < R; ++r) sm[a0 + r * WSTRIDE] = v[q * R + r];
+        } else if constexpr (xor_split<R, WSTRIDE>()) {
+            // base = (j/Ns)*Ns*R + j%Ns: (base*L + s) has no bit in common
+            // with r*Ns*L (j%Ns*L + s < Ns*L; (j/Ns)*Ns*R*L a multiple of Ns*L*R)
+            const int a0 = C::sidx(s, base);
+#pragma unroll
+            for (int r = 0; r < R; ++r) sm[a0 ^ C::Swz::apply(r * WSTRIDE)] = v[q * R + r];
         } else {
 #pragma unroll
             for (int r = 0; r < R; ++r) sm[C::sidx(s, base + r * Ns)] = v[q * R + r];
@@ -453,6 +472,10 @@ __device__ __forceinline__ void pass_exchange(float2 (&v)[C::E], float2 *sm0, fl
             const int a0 = C::sidx(s, j);
 #pragma unroll
             for (int r = 0; r < R2; ++r) v[q * R2 + r] = sm[a0 + r * RSTRIDE];
+        } else if constexpr (xor_split<R2, RSTRIDE>()) {
+            const int a0 = C::sidx(s, j); // j < NR2: j*L + s < NR2*L
+#pragma unroll
+            for (int r = 0; r < R2; ++r) v[q * R2 + r] = sm[a0 ^ C::Swz::apply(r * RSTRIDE)];
         } else {
 #pragma unroll
             for (int r = 0; r < R2; ++r) v[q * R2 + r] = sm[C::sidx(s, j + r * NR2)];

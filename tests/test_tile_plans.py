@@ -86,6 +86,10 @@ def stride_commutes(sw, c):
     return c > 0 and c % (1 << hi) == 0 and sh + 3 <= hi
 
 
+def pow2(x):
+    return x > 0 and (x & (x - 1)) == 0
+
+
 def colmap(beta, NR, L):
     lo = beta % K
     rest = beta // K
@@ -144,6 +148,8 @@ def emulate(v, mapf, fwd, x):
                 a = np.array([sw(int(b + r * Ns) * L + int(ss)) for b, ss in zip(base, s)])
                 if stride_commutes(v["sw"], wstride):
                     assert (a == a0 + r * wstride).all(), "swizzle does not commute"
+                elif pow2(R) and pow2(wstride):   # fft32.cuh's xor_split form
+                    assert (a == (a0 ^ sw(r * wstride))).all(), "xor split of a write"
                 assert (a >= 0).all() and (a < N * L).all()
                 assert not used[a].any() and len(set(a.tolist())) == NT, "exchange overwrites"
                 used[a] = True
@@ -151,10 +157,14 @@ def emulate(v, mapf, fwd, x):
         assert used.all()
         R2 = radix(p + 1)
         NR2 = N // R2
+        rstride = NR2 * L
         for q in range(E // R2):
             s, j = mapf(t + q * NT, NR2, L)
+            a0 = np.array([sw(int(jj) * L + int(ss)) for jj, ss in zip(j, s)])
             for r in range(R2):
                 a = np.array([sw(int(jj + r * NR2) * L + int(ss)) for jj, ss in zip(j, s)])
+                if not stride_commutes(v["sw"], rstride) and pow2(R2) and pow2(rstride):
+                    assert (a == (a0 ^ sw(r * rstride))).all(), "xor split of a read"
                 vals[:, q * R2 + r] = sm[a]
     R = radix(P - 1)
     NR = N // R
