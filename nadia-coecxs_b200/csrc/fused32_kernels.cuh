@@ -117,9 +117,30 @@ __device__ __forceinline__ double block_sum_seq(double v)
     return t;
 }
 
+// 16-byte asynchronous copies global -> shared (completion: cp_async_wait_all)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
+
 // -------------------------------------------------------------- column pass
 
+// STAGE: the tile's sqrt(I) (and, for FresnelCDI, white field) -- one
+// contiguous run of N*L elements in the panel layout, like P's -- is copied
+// into shared memory by cp.async when the tile starts, so those loads land
+// during the forward transform instead of stalling the modulus after it.
 template <class C, bool FRESNEL>
+constexpr size_t col_stage_bytes()
+{
+    return (size_t)C::N * C::L * (FRESNEL ? 12 : 4);
+}
+
+template <class C, bool FRESNEL, bool STAGE = false>
 __global__ void __launch_bounds__(C::NT, C::MINB) k_col(const Slot *const *slots, int nx, int ny,
                                                const float2 *__restrict__ tw)
 {
@@ -130,24 +151,38 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_col(const Slot *const *slots
     const float s0 = S.s0;
     const int c0 = blockIdx.x * (C::L / kPanel);
     float2 v[C::E];
+    constexpr int TW = C::N * C::L;
+    float *ms = reinterpret_cast<float *>(sm + C::smem_words());
+    float2 *ws = reinterpret_cast<float2 *>(ms + TW);
+    if constexpr (STAGE) {
+        const size_t off = (size_t)c0 * kPanel * nx; // the tile's run (nx = N)
+        for (int c = threadIdx.x; c < TW / 4; c += C::NT) cp_async16(ms + 4 * c, mI + off + 4 * c);
+        if constexpr (FRESNEL)
+            for (int c = threadIdx.x; c < TW / 2; c += C::NT) cp_async16(ws + 2 * c, S.W + off + 2 * c);
+    }
 
     for_each_slot<C, true, true>([&](int e, int s, int pos) {
         v[e] = P[paddr(pos, c0 * kPanel + s, nx)];
     });
     transform<C, true>(v, sm, tw);
+    if constexpr (STAGE) {
+        cp_async_wait_all();
+        __syncthreads();
+    }
 
     double diff = 0.0;
     for_each_slot<C, true, false>([&](int e, int s, int kx) {
         const int ky = c0 * kPanel + s;
         const size_t a = paddr(kx, ky, nx);
-        const float m = __ldg(&mI[a]);
+        const int b = ((s / kPanel) * C::N + kx) * kPanel + s % kPanel; // staged index
+        const float m = STAGE ? ms[b] : __ldg(&mI[a]);
         float2 X = v[e];
         if (!FRESNEL) {
             // Planar: Psi = X s0; back-propagated value = projected Psi * s0
             X = planar_modulus(X, m, s0, diff);
         } else {
             const float2 cf = cmul(__ldg(&S.tx[kx]), __ldg(&S.ty[ky]));
-            const float2 w = S.W[a];
+            const float2 w = STAGE ? ws[b] : S.W[a];
             const float2 u = modulus(cadd(cscale(cmul(cf, X), s0), w), m, diff);
             X = cscale(cmulc(csub(u, w), cf), s0);
         }
@@ -308,7 +343,7 @@ namespace f32 {
 // --------------------------------------------------------------- variants
 
 template <class C>
-size_t smem_bytes()
+constexpr size_t smem_bytes()
 {
     return (size_t)C::smem_words() * sizeof(float2);
 }
@@ -503,6 +538,57 @@ TileVariant make_variant(const char *radices)
     t.wf_row = &launch_wf_row<CR>;
     t.tc_row = &launch_row_tc<CR>;
     return t;
+}
+
+// Column-pass-only variants whose tiles stage sqrt(I) (and the white field)
+// by cp.async at the start (k_col's STAGE), plain or with ping-pong exchanges.
+template <class C>
+void prepare_staged()
+{
+    NADIA_CUDA(cudaFuncSetAttribute(k_col<C, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(smem_bytes<C>() + col_stage_bytes<C, false>())));
+    NADIA_CUDA(cudaFuncSetAttribute(k_col<C, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(smem_bytes<C>() + col_stage_bytes<C, true>())));
+}
+
+template <class C>
+void launch_col_staged(bool fresnel, const Slot *const *slots, int nslots, int nx, int ny,
+                       const float2 *tw, cudaStream_t st)
+{
+    dim3 grid(ny / C::L, nslots);
+    if (fresnel)
+        k_col<C, true, true><<<grid, C::NT, smem_bytes<C>() + col_stage_bytes<C, true>(), st>>>(
+            slots, nx, ny, tw);
+    else
+        k_col<C, false, true><<<grid, C::NT, smem_bytes<C>() + col_stage_bytes<C, false>(), st>>>(
+            slots, nx, ny, tw);
+}
+
+template <int N, int NT, int L, int MINB, class SW, bool PING, int... Rs>
+TileVariant make_staged_col(const char *radices)
+{
+    using CC = TileCfg<N, NT, L, kColMap, Radices<Rs...>, SW, MINB, PING>;
+    static_assert(smem_bytes<CC>() + col_stage_bytes<CC, true>() <= 227 * 1024, "stage too large");
+    TileVariant t;
+    t.n = N;
+    t.nt = NT;
+    t.L = L;
+    t.minb = MINB;
+    t.ping = PING;
+    t.radices = radices;
+    t.prepare = &prepare_staged<CC>;
+    t.col = &launch_col_staged<CC>; // column pass only (no row, FresnelCDI_WF or constraint pass)
+    return t;
+}
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_staged(const char *radices)
+{
+    return make_staged_col<N, NT, L, MINB, SW, false, Rs...>(radices);
+}
+template <int N, int NT, int L, int MINB, class SW, int... Rs>
+TileVariant make_staged_ping(const char *radices)
+{
+    return make_staged_col<N, NT, L, MINB, SW, true, Rs...>(radices);
 }
 
 // The same tile shape with ping-pong exchange buffers (twice the shared memory).

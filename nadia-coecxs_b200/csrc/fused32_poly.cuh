@@ -212,17 +212,6 @@ __global__ void __launch_bounds__(C::NT, C::MINB) k_poly_col_inv(const Slot *con
     });
 }
 
-// 16-byte asynchronous copies global -> shared (completion: cp_async_wait_all)
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
-{
-    const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all()
-{
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
-}
-
 // Shared memory of the row pass: the exchange tile, then (PREF) the tile's
 // rows of x and of the support, staged in their panel order [ny/4][L][4]
 template <class C, bool PREF>

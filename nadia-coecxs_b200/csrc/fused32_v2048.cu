@@ -46,6 +46,9 @@ void add_variants_2048(std::vector<TileVariant> &v)
     // the best column and row shapes with every twiddle loaded from the table
     v.push_back(make_persistent_tw<2048, 512, 4, 1, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16 tw"));
     v.push_back(make_grouped_row_tw<2048, 128, 1, 4, Swizzle<4, 5, 7, 1>, 8, 16, 16>("8.16.16 tw"));
+    // column passes that stage sqrt(I) (and the white field) by cp.async
+    v.push_back(make_staged_ping<2048, 1024, 4, 1, Swizzle<4, 5, 3, 2>, 8, 8, 8, 4>("8.8.8.4 staged"));
+    v.push_back(make_staged<2048, 1024, 4, 1, Swizzle<4, 5, 3, 2>, 8, 8, 8, 4>("8.8.8.4 staged"));
 }
 
 } // namespace f32

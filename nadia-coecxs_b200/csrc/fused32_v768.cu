@@ -16,6 +16,9 @@ void add_variants_768(std::vector<TileVariant> &v)
     v.push_back(make_ping<768, 256, 8, 2, Swizzle<4, 6, 3, 2>, 8, 8, 4, 3>("8.8.4.3"));
     // the tile configuration of this length's class in the mixed-length passes
     v.push_back(make_persistent<768, 512, 8, 1, Swizzle<4, 5, 3, 2>, 12, 4, 4, 4>("12.4.4.4"));
+    // column passes that stage sqrt(I) (and the white field) by cp.async
+    v.push_back(make_staged<768, 128, 4, 4, Swizzle<4, 0, 7, 1>, 8, 8, 4, 3>("8.8.4.3 staged"));
+    v.push_back(make_staged<768, 256, 8, 2, Swizzle<4, 6, 3, 2>, 8, 8, 4, 3>("8.8.4.3 staged"));
 }
 
 } // namespace f32

@@ -115,3 +115,29 @@ def test_batched_equals_alone_and_pass_times():
         assert np.array_equal(a.get_exit_surface_wave(), b.get_exit_surface_wave())
     c1, c2, r = pynadia.pass_times(batch, reps=3)
     assert c1 > 0 and c2 > 0 and r > 0
+
+
+@pytest.mark.parametrize("alg", ["ER", "HIO"])
+def test_1080_tile_shapes_agree(alg, monkeypatch):
+    """The three 1080-point tile shapes (two 144-thread CTAs per SM with the
+    row pass's x and support staged by cp.async, the same without staging,
+    one 288-thread CTA; NADIA_POLY_TILE selects the first shape tried) run
+    the same radix passes; the compiler may contract their multiply-adds
+    differently, so after five iterations they agree to FP32 rounding (the
+    per-step bar), not bit for bit."""
+    p = synth.PolyCase(1024, seed=3, padding=28, photons=1e8)
+    out = []
+    for k in ("0", "1", "2"):
+        monkeypatch.setenv("NADIA_POLY_TILE", k)
+        s = pynadia.Solver("poly", 1024, 1024, precision=pynadia.FP32)
+        s.set_support(p.support)
+        s.set_intensity(p.intensity)
+        s.set_spectrum(p.spectrum)
+        s.initialise_estimate(7)
+        s.set_algorithm(alg)
+        s.iterate(5)
+        out.append((s.get_error_history(5), s.get_exit_surface_wave()))
+        s.close()
+    for h, x in out[1:]:
+        assert np.allclose(h, out[0][0], rtol=STEP_TOL, atol=0)
+        assert l2rel(x, out[0][1]) <= STEP_TOL

@@ -33,7 +33,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "nadia-coecxs_b200", "csrc")
 K = 4  # panel width
 
-PAT = re.compile(r"make_(variant|ping|persistent_single|persistent_direct|persistent_ping|persistent_mstage|"
+PAT = re.compile(r"make_(variant|ping|staged_ping|staged|persistent_single|persistent_direct|persistent_ping|persistent_mstage|"
                  r"persistent_row|grouped_row_tw|grouped_row|grouped_col|persistent_tw|persistent|poly)<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+),\s*"
                  r"Swizzle<\s*(\d+),\s*(\d+),\s*(\d+),\s*(\d+)>\s*,\s*([\d,\s]+)>")
 
@@ -190,7 +190,8 @@ def out_positions(v, mapf, first_radix):
     return np.array(pos)
 
 
-COLUMN_ONLY = ("persistent_single", "persistent_direct", "persistent_ping", "persistent_mstage")
+COLUMN_ONLY = ("persistent_single", "persistent_direct", "persistent_ping", "persistent_mstage",
+               "staged", "staged_ping")
 
 
 def maps_of(v):
@@ -237,6 +238,8 @@ def test_tile_shape_constraints(v):
         assert v["minb"] * (N * L * 24 + 24 + 1024) <= 228 * 1024
     if v["kind"] == "persistent_mstage":
         assert N * L * 28 + 24 <= 227 * 1024
+    if v["kind"] in ("staged", "staged_ping"):   # exchange tile(s) + sqrt(I) + white field
+        assert N * L * (8 * (2 if v["kind"] == "staged_ping" else 1) + 12) <= 227 * 1024
 
 
 @pytest.mark.parametrize("v", VARIANTS, ids=vid)
