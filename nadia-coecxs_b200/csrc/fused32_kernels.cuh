@@ -19,6 +19,17 @@ __device__ __forceinline__ float support_factor(float s)
     return s == 0.f ? 0.f : (s < 1.f ? s : 1.f);
 }
 
+// 1/sqrt(a) for the magnitude ratios: PTX's approximate reciprocal square
+// root (relative error below 2^-22.9) in its flush-to-zero form, on a raised
+// to the smallest normal float, so no subnormal handling is emitted around
+// it; a = 0 gives 2^63, finite, so a * rsqrt_normal(a) is 0.
+__device__ __forceinline__ float rsqrt_normal(float a)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(fmaxf(a, 1.17549435e-38f)));
+    return r;
+}
+
 // Modulus projection of one transform value (BaseCDI::scale_intensity,
 // BaseCDI.c++:163-189, with Complex_2D::set_mag, Complex_2D.h:205-215):
 // u is the detector-plane value, m its sqrt(I) (-1 = unmeasured).  Returns
@@ -29,8 +40,8 @@ __device__ __forceinline__ float2 modulus(float2 u, float m, double &diff)
     const float a2 = u.x * u.x + u.y * u.y;
     const bool measured = !(m < 0.f);
     const bool zero = !(a2 > 0.f);
-    const float inv = rsqrtf(zero ? 1.f : a2);
-    const float mag = zero ? 0.f : a2 * inv;
+    const float inv = rsqrt_normal(a2);
+    const float mag = a2 * inv;
     const float sc = measured ? m * inv : 1.f;
     float2 r = make_float2(u.x * sc, u.y * sc);
     if (measured && zero) r = make_float2(m, 0.f);
@@ -51,12 +62,12 @@ __device__ __forceinline__ float2 planar_modulus(float2 X, float m, float s0, do
     const float a2 = X.x * X.x + X.y * X.y;
     const bool measured = !(m < 0.f);
     const bool zero = !(a2 > 0.f);
-    const float inv = rsqrtf(zero ? 1.f : a2);
+    const float inv = rsqrt_normal(a2);
     const float sm = s0 * m;
     const float sc = measured ? sm * inv : s0 * s0; // unmeasured: Psi kept, s0 Psi = s0^2 X
     float2 r = make_float2(X.x * sc, X.y * sc);
     if (measured && zero) r = make_float2(sm, 0.f);
-    const float mag = zero ? 0.f : a2 * inv;
+    const float mag = a2 * inv;
     const float d = measured ? fmaf(s0, mag, -m) : 0.f;
     diff = fma((double)d, (double)d, diff);
     return r;

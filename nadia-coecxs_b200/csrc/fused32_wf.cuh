@@ -50,8 +50,8 @@ __device__ __forceinline__ float2 wf_modulus(float2 c, float m, float sg, double
     if (m < 0.f) return c; // unmeasured: kept
     const float a2 = c.x * c.x + c.y * c.y;
     const bool zero = !(a2 > 0.f);
-    const float inv = rsqrtf(zero ? 1.f : a2);
-    const float mag = zero ? 0.f : a2 * inv;
+    const float inv = rsqrt_normal(a2);
+    const float mag = a2 * inv;
     const float d = mag - m;
     diff = fma((double)d, (double)d, diff);
     if (zero) return make_float2(sg * m, 0.f);
