@@ -139,8 +139,11 @@ __global__ void __launch_bounds__(kExpandThreads) k_poly_expand(const Slot *cons
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     if (m[k] < 0.f) continue;
-                    const float calc = sqrtf(acc[k]);
-                    r[k] = calc == 0.f ? 0.f : m[k] / calc;
+                    // sqrt(I_calc) and the ratio from one approximate reciprocal
+                    // square root (no IEEE square-root or division sequence)
+                    const float inv = rsqrt_normal(acc[k]);
+                    const float calc = acc[k] * inv;
+                    r[k] = calc == 0.f ? 0.f : m[k] * inv;
                     const double d = (double)m[k] - (double)calc;
                     diff += d * d;
                 }
